@@ -1,0 +1,342 @@
+#!/usr/bin/env python
+"""Benchmark: one bootstrap particle-filter step (LibBi BootstrapPF::step) on
+the Lorenz '96 workload, d = 40, N = 65536 FP32 particles, RK4 h = 0.01 with
+N(0, 0.1^2) noise every 0.05, all 40 components observed with N(0, 1) noise
+every 0.05, systematic resampling at ESS < 0.5 N.
+
+A step is resample-if-due + fused transition/observation/reduction of all N
+particles for one observation interval.  Metric: particle-steps/s.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank runs an independent replica (the single filter does
+not shard; replicas only) and rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "l96_d40_n65536"
+METRIC = "particle-steps/s/GPU"
+UNIT = "particle-steps/s"
+N_PARTICLES = 65536
+DIM = 40
+T_OBS = 200
+DT = 0.05
+ESS_REL = 0.5
+SEED = 2
+DATA_SEED = 102
+L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
+# our kernels per step with the systematic resampler: weight tile sums,
+# offspring, survivors, fill (launched every step, gated on the device) +
+# the fused transition
+LAUNCHES_PER_STEP = 5
+# algorithmic bytes of the fused transition per particle: state read + write
+# (2 * d * 4 B) and FP64 log-weight read + write (16 B); the ancestor index
+# (4 B) is read only on resample steps
+TRANSITION_BYTES_PER_PARTICLE = 2 * DIM * 4 + 16
+# FP32 operations per particle-step of the fused transition (FMA = 2):
+# RK4 5 sub-steps x 40 components x 31 + noise add 2 x 40 + observation 6 x 40
+TRANSITION_FLOP_PER_PARTICLE = 5 * DIM * 31 + 2 * DIM + 6 * DIM
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured", d.get("sm_max_mhz", 1965.0)
+    return 6650.0, "fallback", 1965.0
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", self.gpu_id, f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def observe(xs, sigma_y):
+    """Observations of a true trajectory xs (T_OBS x DIM): N(0, sigma_y^2) noise."""
+    import numpy as np
+
+    rng = np.random.default_rng(DATA_SEED)
+    return (xs + sigma_y * rng.standard_normal(xs.shape)).astype(np.float32)
+
+
+def synthetic_observations(model):
+    """One model run (the library's own transition with its process noise,
+    N = 1, no observations) from the data seed, observed with N(0, sigma_y^2)
+    noise: T_OBS x DIM values in FP32, on the host."""
+    import numpy as np
+    from libbi_b200 import BootstrapPF
+
+    truth = BootstrapPF(model, 1, seed=DATA_SEED)
+    xs = np.zeros((T_OBS, DIM), np.float32)
+    for k in range(T_OBS):
+        truth.step(k * DT, (k + 1) * DT, None)
+        x, _, _ = truth.state()
+        xs[k] = x[:, 0].cpu().numpy()
+    truth.close()
+    return observe(xs, model.sigma_y)
+
+
+def cpu_baseline(y, seconds: float = 12.0):
+    """The oracle's port of the reference's CPU filter (OpenMP over particles,
+    all host threads), on a bounded sample of the same workload."""
+    import numpy as np
+    from oracle.oracle import Oracle
+    from libbi_b200 import configs
+    from libbi_b200 import _native as N
+
+    O = Oracle()
+    model = configs.L96_D40_N65536["model"]
+    desc = model.desc()
+    cfg = N.Config()
+    cfg.nparticles = N_PARTICLES
+    cfg.resampler = N.BPF_RESAMPLER_SYSTEMATIC
+    cfg.ess_rel = ESS_REL
+    cfg.seed = SEED
+    t = time.perf_counter()
+    O.filter(desc, cfg, y[:2].reshape(-1), 2, 0.0, DT)
+    per = (time.perf_counter() - t) / 2
+    S = int(max(2, min(T_OBS, seconds / max(per, 1e-6))))
+    t = time.perf_counter()
+    O.filter(desc, cfg, y[:S].reshape(-1), S, 0.0, DT)
+    el = time.perf_counter() - t
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": N_PARTICLES * S / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"oracle port of the reference CPU filter, N={N_PARTICLES}, first {S} of {T_OBS} "
+                      f"observation steps (incl. initial draw), {threads} OpenMP threads, {el:.1f} s"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    from oracle.oracle import Oracle
+    from libbi_b200 import configs
+
+    # the same true trajectory as the GPU arm (same draws, same arithmetic),
+    # here from the oracle's model run, with the same observation noise
+    model = configs.L96_D40_N65536["model"]
+    _, xs = Oracle().simulate(model.desc(), DATA_SEED, T_OBS, 0.0, DT)
+    y = observe(xs, model.sigma_y)
+    cb = cpu_baseline(y, seconds=max(5.0, 2.0 * (args.steps + args.warmup)))
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "nparticles": N_PARTICLES, "dim": DIM, "resampler": "systematic",
+                       "ess_rel": ESS_REL},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    if args.warmup < 3:
+        args.warmup = 3
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+
+    import numpy as np
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from libbi_b200 import BootstrapPF, build, configs
+
+    build.build()
+    model = configs.L96_D40_N65536["model"]
+    y_host = synthetic_observations(model)
+    y_dev = torch.as_tensor(y_host, device="cuda")
+    pf = BootstrapPF(model, N_PARTICLES, resampler="systematic", ess_rel=ESS_REL, seed=SEED + 1000 * rank)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    k = 0
+
+    def next_k():
+        nonlocal k
+        if k >= T_OBS:
+            pf.init()
+            k = 0
+        k += 1
+        return k
+
+    # warm-up (untimed)
+    for _ in range(args.warmup):
+        kk = next_k()
+        pf.step_device((kk - 1) * DT, kk * DT, y_dev[kk - 1], sync=False)
+    torch.cuda.synchronize()
+
+    # timed: K steps, L2 flushed before each, CUDA events around each step
+    pf.timing(True)
+    pf.timing_read(reset=True)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    gpu_id = str(torch.cuda.get_device_properties(local).uuid)
+    gpu_id = gpu_id if gpu_id.startswith("GPU-") else "GPU-" + gpu_id
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(gpu_id) as clk:
+        wall0 = time.perf_counter()
+        for i in range(args.steps):
+            kk = next_k()
+            flush.zero_()
+            starts[i].record()
+            pf.step_device((kk - 1) * DT, kk * DT, y_dev[kk - 1], sync=False)
+            ends[i].record()
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - wall0
+    if dist:
+        dist.barrier()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = sum(step_ms)
+    res_ms, tr_ms, nst = pf.timing_read(reset=True)
+    pf.timing(False)
+    if dist:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = N_PARTICLES * args.steps * world / (total_ms / 1e3)
+
+    # end to end through the public API: pinned host observation copied in,
+    # step statistics read back, every step
+    y_pin = torch.empty((T_OBS, DIM), dtype=torch.float32).pin_memory()
+    y_pin.copy_(torch.as_tensor(y_host))
+    y_np = y_pin.numpy()
+    e2e_s = 0.0
+    for i in range(args.steps):
+        kk = next_k()
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        pf.step((kk - 1) * DT, kk * DT, y_np[kk - 1])
+        e2e_s += time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = N_PARTICLES * args.steps * world / e2e_s
+
+    hbm, how, sm_max = peaks()
+    clocks = clk.summary()
+    t_launch = tr_ms / max(nst, 1) / 1e3
+    bytes_launch = TRANSITION_BYTES_PER_PARTICLE * N_PARTICLES
+    achieved = bytes_launch / t_launch / 1e9
+    f_mhz = clocks["sm_mhz"] or sm_max
+    fp32_peak = 148 * 128 * 2 * f_mhz * 1e6 / 1e12
+    fp32_ach = TRANSITION_FLOP_PER_PARTICLE * N_PARTICLES / t_launch / 1e12
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "nparticles": N_PARTICLES, "dim": DIM, "obs_interval": DT,
+                   "rk4_h": 0.01, "resampler": "systematic", "ess_rel": ESS_REL,
+                   "parallelism": f"replicas{world}" if world > 1 else "single",
+                   "l2": "flushed before every timed step (256 MiB write)",
+                   "resampled_steps_timed": None},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": DIM * 4,
+                "d2h_bytes_per_step": 80, "timer": "host wall clock around bpf_step"},
+        "gpu_launches": LAUNCHES_PER_STEP * args.steps,
+        "roofline": {"kernel": "k_l96_transition<float,40>", "bound": "hbm", "achieved": achieved,
+                     "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_source": how,
+                     "traffic": None, "algorithmic_bytes_per_launch": bytes_launch,
+                     "launch_ms": t_launch * 1e3,
+                     "fp32": {"achieved_tflops": fp32_ach, "peak_tflops": fp32_peak,
+                              "frac": fp32_ach / fp32_peak,
+                              "peak_source": "148 SM x 128 FP32 lanes x 2 x sampled SM clock"}},
+        "kernel_ms_per_step": {"resample": res_ms / max(nst, 1), "transition": tr_ms / max(nst, 1)},
+        "wall_s": wall,
+        "clocks": clocks,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(y_host)
+    pf.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,245 @@
+/*
+ * libbi_b200 — B200-native bootstrap particle-filter step, C ABI.
+ *
+ * This is the drop-in boundary for LibBi's bootstrap particle filter hot
+ * path.  Each entry point names the reference interface it replaces
+ * (paths are relative to the LibBi source tree).  All functions are
+ * extern "C", take plain pointers and sizes, and return an int status
+ * (BPF_OK or one of the BPF_E_* codes).  Pointers documented as "device"
+ * are CUDA device pointers on the current device; "host" pointers are
+ * ordinary host memory.  Work is enqueued on the stream given at creation
+ * (or the legacy default stream when that is NULL); functions that return
+ * scalars to the host synchronise that stream.
+ *
+ * Threading: one handle per host thread.  Handles never share buffers.
+ */
+#ifndef LIBBI_B200_H
+#define LIBBI_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+  BPF_OK = 0,
+  /* all weights zero or not finite when a resample was due; the reference
+   * throws ParticleFilterDegeneratedException here
+   * (share/src/bi/resampler/SystematicResampler.hpp:127-129,
+   *  share/src/bi/misc/exception.hpp:47) */
+  BPF_E_DEGENERATE = 1,
+  BPF_E_INVALID = 2,   /* bad argument (size, kind, null pointer) */
+  BPF_E_CUDA = 3,      /* a CUDA runtime call failed */
+  BPF_E_TIMEOUT = 4,   /* a bounded device-side wait gave up */
+  BPF_E_NOMEM = 5      /* device allocation failed */
+};
+
+/* ---- model description ------------------------------------------------ */
+/* The two models of the hot path.  LibBi compiles each .bi model into a
+ * Model<Name> class (share/tt/cpp/model.hpp.tt:95-510); here the model's
+ * transition and observation blocks are built into the library and chosen
+ * by kind, with the .bi model's constants passed in theta. */
+enum {
+  /* Lorenz '96, d components (docs/src/users.tex:354-358):
+   *   transition(delta) { eta[i] ~ gaussian(0, sigma_eta);
+   *                       ode(alg='RK4', h) { dx[i]/dt = (x[i+1]-x[i-2])*x[i-1] - x[i] + F }
+   *                       x[i] <- x[i] + eta[i] }
+   *   observation       { y[i] ~ gaussian(x[i], sigma_y) }
+   *   initial           { x[i] ~ gaussian(x0_mean, x0_std) }
+   * theta = { F, sigma_eta, sigma_y, x0_mean, x0_std } */
+  BPF_MODEL_L96 = 1,
+  /* Phytoplankton-zooplankton (docs/src/users.tex:40-84):
+   *   transition(delta) { alpha ~ log_normal(mu, sigma);
+   *                       ode(alg='RK4(3)', h, atoler, rtoler) {
+   *                         dP/dt = alpha*P - c*P*Z
+   *                         dZ/dt = e*c*P*Z - m*Z - q*Z*Z } }
+   *   observation       { y ~ gaussian(log(P), sigma_y) }
+   *   initial           { P ~ log_normal(p0_mu, p0_sigma); Z ~ log_normal(z0_mu, z0_sigma) }
+   * theta = { c, e, m, q, mu, sigma, sigma_y, p0_mu, p0_sigma, z0_mu, z0_sigma } */
+  BPF_MODEL_PZ = 2
+};
+
+enum { BPF_ODE_RK4 = 0, BPF_ODE_RK43 = 1 };
+enum { BPF_F32 = 0, BPF_F64 = 1 };
+
+#define BPF_MAX_THETA 16
+
+typedef struct {
+  int kind;        /* BPF_MODEL_* */
+  int dim;         /* state components: d for L96 (1..64), 2 for PZ */
+  int precision;   /* BPF_F32 or BPF_F64: state, ODE and log-density arithmetic
+                      (L96: either; PZ: BPF_F64) */
+  int integrator;  /* BPF_ODE_RK4 or BPF_ODE_RK43 (ode block 'alg') */
+  double h;        /* ode block 'h' (RK4 step / RK4(3) initial step) */
+  double atoler;   /* ode block 'atoler' (RK4(3) only) */
+  double rtoler;   /* ode block 'rtoler' (RK4(3) only) */
+  double theta[BPF_MAX_THETA];
+} bpf_model_desc;
+
+/* ---- filter configuration --------------------------------------------- */
+/* Resampler kinds: share/src/bi/resampler/ResamplerFactory.cpp:8-39 */
+enum {
+  BPF_RESAMPLER_SYSTEMATIC = 0,
+  BPF_RESAMPLER_MULTINOMIAL = 1,
+  BPF_RESAMPLER_METROPOLIS = 2
+};
+
+typedef struct {
+  int nparticles;        /* N (--nparticles) */
+  int resampler;         /* BPF_RESAMPLER_* (--resampler) */
+  int metropolis_steps;  /* B (--C), Metropolis only */
+  double ess_rel;        /* resample when ESS < ess_rel*N (--ess-rel) */
+  uint64_t seed;         /* --seed */
+  void* stream;          /* cudaStream_t, or NULL for the default stream */
+} bpf_config;
+
+/* Output of one filter step: the fields of BootstrapPFState / FilterState
+ * that BootstrapPF::correct updates (share/src/bi/filter/BootstrapPF.hpp:171-181). */
+typedef struct {
+  double ess;             /* s.ess */
+  double log_weight_sum;  /* lW = max + log sum exp(lw - max) - log N */
+  double log_increment;   /* s.logIncrements(k) = lW - previous logLikelihood */
+  double log_likelihood;  /* s.logLikelihood */
+  int resampled;          /* Resampler::resample returned true before this step's predict */
+  int status;             /* device-side status (BPF_OK, BPF_E_DEGENERATE, BPF_E_TIMEOUT) */
+} bpf_step_out;
+
+typedef struct bpf_handle bpf_handle;
+
+/* Create a filter: State + BootstrapPFState + Resampler + RNG for one model.
+ * Replaces the construction in the generated filter client
+ * (share/tt/cpp/client/filter_cpu.cpp.tt:105-184): BootstrapPFState(N),
+ * ResamplerFactory::create*, Random(seed), BootstrapPF(m, in, obs, resam). */
+int bpf_create(const bpf_model_desc* model, const bpf_config* config, bpf_handle** out);
+
+/* Release all device memory of the handle. */
+int bpf_destroy(bpf_handle* h);
+
+/* Device pointers of the particle store.  x: structure of arrays, component j
+ * of particle p at x[j*ld + p] in the model precision (State Xdn, column-major,
+ * share/src/bi/state/State.hpp:73-462); lw: N log-weights in FP64
+ * (BootstrapPFState::logWeights); as: N ancestors (BootstrapPFState::ancestors).
+ * The pointers stay valid until the next bpf_step / bpf_gather, which
+ * alternate between two state buffers. */
+int bpf_state_ptrs(bpf_handle* h, void** x, double** lw, int** as, int* ld);
+
+/* Simulator::init for the filter: draw initial particles from the model's
+ * initial block, clear log-weights, logLikelihood and ess
+ * (share/src/bi/simulator/Simulator.hpp:255-332, Filter::filter
+ * share/src/bi/filter/Filter.hpp:58-70). */
+int bpf_init(bpf_handle* h);
+
+/* One BootstrapPF::step from t1 to the observation at t2
+ * (share/src/bi/filter/BootstrapPF.hpp:158-181): resample if the previous
+ * schedule element was observed and ESS < ess_rel*N (Resampler::resample,
+ * share/src/bi/resampler/Resampler.hpp:167-182), predict with
+ * Model::transitionSamples (share/tt/cpp/model.hpp.tt:566-573), then correct
+ * with Model::observationLogDensities (model.hpp.tt:757-765) and
+ * Resampler::reduce.  y: host pointer to the step's observations in the
+ * model precision (L96: dim values; PZ: 1 value), or NULL for an unobserved
+ * step.  out may be NULL (no sync). */
+int bpf_step(bpf_handle* h, double t1, double t2, const void* y, bpf_step_out* out);
+
+/* bpf_step with the observation already in device memory (or NULL): no
+ * host-to-device copy is enqueued. */
+int bpf_step_device(bpf_handle* h, double t1, double t2, const void* y_device, bpf_step_out* out);
+
+/* Filter<BootstrapPF>::filter over T observations at t0+dt, ..., t0+T*dt
+ * (share/src/bi/filter/Filter.hpp:58-70 with BootstrapPF::term :192-196).
+ * y: host, T observations (L96: dim values each; PZ: 1) in the model
+ * precision, observation-major.
+ * Outputs (host, may be NULL): log_increments[T], ess[T], and the final
+ * log-likelihood.  Calls bpf_init first. */
+int bpf_filter(bpf_handle* h, int T, double t0, double dt, const void* y,
+               double* log_increments, double* ess, double* log_likelihood);
+
+/* Resampler<R>::reduce over the handle's log-weights
+ * (share/src/bi/resampler/Resampler.hpp:156-163 -> ess_reduce,
+ *  share/src/bi/primitive/vector_primitive.hpp:960-974). */
+int bpf_reduce(bpf_handle* h, double* lW, double* ess);
+
+/* Force one resample of the handle's state now (the ancestors, gather and
+ * log-weight reset of Resampler::resample, Resampler.hpp:170-177), whatever
+ * the ESS.  uniforms: optional DEVICE pointer to the resampler's uniforms
+ * (systematic: 1; multinomial: N in the reference's draw order; Metropolis:
+ * 2*B*N, particle-major) to replace the handle's own draws.  ancestors_out:
+ * optional device pointer receiving the N permuted ancestors. */
+int bpf_resample(bpf_handle* h, const double* uniforms, int* ancestors_out);
+
+/* Device timing of the steps (the reference's TicToc around Filter::filter,
+ * share/src/bi/misc/TicToc.hpp:17-70, at kernel granularity): when enabled,
+ * every step records CUDA events before its resample kernels, between them
+ * and the fused transition, and after it.  bpf_timing_read synchronises the
+ * stream and returns the summed milliseconds and the number of steps since
+ * the last reset. */
+int bpf_timing_enable(bpf_handle* h, int enable);
+int bpf_timing_read(bpf_handle* h, int reset, double* resample_ms, double* transition_ms, int* steps);
+
+/* ---- stand-alone primitives (the Resampler<R> and gather APIs) -------- */
+
+typedef struct bpf_resampler bpf_resampler;
+
+/* Resampler<R>(essRel) with scratch for up to max_n particles
+ * (share/src/bi/resampler/Resampler.hpp:125-132; B as MetropolisResampler(B),
+ *  share/src/bi/resampler/MetropolisResampler.hpp:201-204). */
+int bpf_resampler_create(int kind, int max_n, int metropolis_steps, void* stream,
+                         bpf_resampler** out);
+int bpf_resampler_destroy(bpf_resampler* r);
+
+/* ess_reduce (vector_primitive.hpp:960-974): device lw[n] (FP64);
+ * returns ESS and lW = max + log sum exp(lw-max) - log n through host pointers. */
+int bpf_ess_reduce(bpf_resampler* r, const double* lw, int n, double* lW, double* ess);
+
+/* logsumexp_reduce (vector_primitive.hpp:933-943), used by BootstrapPF::term. */
+int bpf_logsumexp_reduce(bpf_resampler* r, const double* lw, int n, double* out);
+
+/* R::ancestors / R::ancestorsPermute on device lw[n]:
+ *  systematic  SystematicResampler.hpp:132-148 (+ ScanResampler::precompute,
+ *              ScanResampler.hpp:35-40; cumulativeOffspring :111-130);
+ *              uniforms: 1 value, the offset a;
+ *  multinomial MultinomialResamplerHost::ancestors (sorted, Bentley & Saxe),
+ *              share/src/bi/host/resampler/MultinomialResamplerHost.hpp:29-65;
+ *              uniforms: n values in the reference's draw order;
+ *  metropolis  MetropolisResamplerHost::ancestors,
+ *              share/src/bi/host/resampler/MetropolisResamplerHost.hpp:32-62;
+ *              uniforms: 2*B*n values, particle-major.
+ * uniforms and as are DEVICE pointers.  permute = 0 gives R::ancestors,
+ * permute = 1 gives the permuted form: every particle with offspring is its
+ * own first offspring (as[i] == i) and the remaining copies, ordered by
+ * ancestor, fill the childless slots in ascending order — the rule of
+ * ResamplerHost::cumulativeOffspringToAncestorsPermute
+ * (share/src/bi/host/resampler/ResamplerHost.hpp:134-168).
+ * Os (optional, device, n ints) receives the cumulative offspring counts.
+ * Returns BPF_E_DEGENERATE when the weights sum to zero or are not finite. */
+int bpf_resampler_ancestors(bpf_resampler* r, const double* lw, int n,
+                            const double* uniforms, int permute, int* as, int* Os);
+
+/* gather_rows (share/src/bi/primitive/matrix_primitive.hpp:630-638,
+ * share/src/bi/cuda/primitive/matrix_primitive_kernel.cuh:50-57), out of
+ * place on device SoA buffers: Y[j*ld + i] = X[j*ld + as[i]], j < d, i < n.
+ * elem_size is 4 or 8. */
+int bpf_gather_rows(const int* as, const void* X, void* Y, int n, int d, int ld,
+                    int elem_size, void* stream);
+
+/* ---- checkpoint (BootstrapPFState save/load,
+ *      share/src/bi/state/BootstrapPFState.hpp:216-231) ------------------- */
+
+/* Bytes needed by bpf_snapshot for this handle. */
+int bpf_snapshot_size(bpf_handle* h, uint64_t* bytes);
+/* Copy state, log-weights, ancestors, scalars and the RNG step counter into
+ * host memory buf (bpf_snapshot_size bytes); bpf_restore reads it back. */
+int bpf_snapshot(bpf_handle* h, void* buf, uint64_t bytes);
+int bpf_restore(bpf_handle* h, const void* buf, uint64_t bytes);
+
+/* Library version string. */
+const char* bpf_version(void);
+/* Human-readable message for a status code. */
+const char* bpf_status_string(int status);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,14 @@
+"""libbi_b200: B200-native bootstrap particle-filter step with LibBi's API.
+
+The product is the CUDA shared library (libbi_b200/_lib/libbi_b200.so, C ABI
+in include/libbi_b200.h); this package is its host-side mirror of the
+reference's filter/resampler classes.
+"""
+from ._native import (BpfError, ParticleFilterDegeneratedException, load_library,  # noqa: F401
+                      LIB_PATH, EXPORTS)
+from .filter import (BootstrapPF, ModelL96, ModelPZ, Resampler, SystematicResampler,  # noqa: F401
+                     MultinomialResampler, MetropolisResampler, gather_rows, StepResult)
+from . import configs  # noqa: F401
+
+__all__ = ["BootstrapPF", "ModelL96", "ModelPZ", "Resampler", "SystematicResampler", "MultinomialResampler",
+           "MetropolisResampler", "gather_rows", "BpfError", "ParticleFilterDegeneratedException", "configs"]

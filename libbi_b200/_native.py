@@ -1,0 +1,147 @@
+"""ctypes binding of the libbi_b200 C ABI (include/libbi_b200.h).
+
+The shared library is built in-tree (``libbi_b200/_lib/libbi_b200.so``) by
+``libbi_b200.build``.  There is no fallback: if the library is missing or a
+CUDA device is not available, :func:`lib` raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import POINTER, c_double, c_int, c_uint64, c_void_p, c_char_p
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libbi_b200.so")
+
+BPF_OK = 0
+BPF_E_DEGENERATE = 1
+BPF_E_INVALID = 2
+BPF_E_CUDA = 3
+BPF_E_TIMEOUT = 4
+BPF_E_NOMEM = 5
+
+BPF_MODEL_L96 = 1
+BPF_MODEL_PZ = 2
+BPF_ODE_RK4 = 0
+BPF_ODE_RK43 = 1
+BPF_F32 = 0
+BPF_F64 = 1
+BPF_RESAMPLER_SYSTEMATIC = 0
+BPF_RESAMPLER_MULTINOMIAL = 1
+BPF_RESAMPLER_METROPOLIS = 2
+BPF_MAX_THETA = 16
+
+# every symbol include/libbi_b200.h declares
+EXPORTS = (
+    "bpf_create", "bpf_destroy", "bpf_state_ptrs", "bpf_init", "bpf_step",
+    "bpf_step_device", "bpf_filter", "bpf_reduce", "bpf_resample",
+    "bpf_resampler_create", "bpf_resampler_destroy", "bpf_ess_reduce",
+    "bpf_logsumexp_reduce", "bpf_resampler_ancestors", "bpf_gather_rows",
+    "bpf_snapshot_size", "bpf_snapshot", "bpf_restore", "bpf_version",
+    "bpf_status_string", "bpf_timing_enable", "bpf_timing_read",
+)
+
+
+class ModelDesc(ctypes.Structure):
+    _fields_ = [
+        ("kind", c_int), ("dim", c_int), ("precision", c_int), ("integrator", c_int),
+        ("h", c_double), ("atoler", c_double), ("rtoler", c_double),
+        ("theta", c_double * BPF_MAX_THETA),
+    ]
+
+
+class Config(ctypes.Structure):
+    _fields_ = [
+        ("nparticles", c_int), ("resampler", c_int), ("metropolis_steps", c_int),
+        ("ess_rel", c_double), ("seed", c_uint64), ("stream", c_void_p),
+    ]
+
+
+class StepOut(ctypes.Structure):
+    _fields_ = [
+        ("ess", c_double), ("log_weight_sum", c_double), ("log_increment", c_double),
+        ("log_likelihood", c_double), ("resampled", c_int), ("status", c_int),
+    ]
+
+
+class BpfError(RuntimeError):
+    """A libbi_b200 call returned a non-zero status."""
+
+    def __init__(self, status: int, what: str):
+        self.status = status
+        super().__init__(f"{what}: {status_string(status)} (status {status})")
+
+
+class ParticleFilterDegeneratedException(BpfError):
+    """All weights zero or not finite when a resample was due; the name and
+    meaning of share/src/bi/misc/exception.hpp:47."""
+
+
+_lib = None
+
+
+def _declare(L):
+    H = c_void_p
+    sig = {
+        "bpf_create": (c_int, [POINTER(ModelDesc), POINTER(Config), POINTER(H)]),
+        "bpf_destroy": (c_int, [H]),
+        "bpf_state_ptrs": (c_int, [H, POINTER(c_void_p), POINTER(c_void_p), POINTER(c_void_p), POINTER(c_int)]),
+        "bpf_init": (c_int, [H]),
+        "bpf_step": (c_int, [H, c_double, c_double, c_void_p, POINTER(StepOut)]),
+        "bpf_step_device": (c_int, [H, c_double, c_double, c_void_p, POINTER(StepOut)]),
+        "bpf_filter": (c_int, [H, c_int, c_double, c_double, c_void_p, c_void_p, c_void_p, POINTER(c_double)]),
+        "bpf_reduce": (c_int, [H, POINTER(c_double), POINTER(c_double)]),
+        "bpf_resample": (c_int, [H, c_void_p, c_void_p]),
+        "bpf_resampler_create": (c_int, [c_int, c_int, c_int, c_void_p, POINTER(H)]),
+        "bpf_resampler_destroy": (c_int, [H]),
+        "bpf_ess_reduce": (c_int, [H, c_void_p, c_int, POINTER(c_double), POINTER(c_double)]),
+        "bpf_logsumexp_reduce": (c_int, [H, c_void_p, c_int, POINTER(c_double)]),
+        "bpf_resampler_ancestors": (c_int, [H, c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p]),
+        "bpf_gather_rows": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_int, c_void_p]),
+        "bpf_snapshot_size": (c_int, [H, POINTER(c_uint64)]),
+        "bpf_snapshot": (c_int, [H, c_void_p, c_uint64]),
+        "bpf_restore": (c_int, [H, c_void_p, c_uint64]),
+        "bpf_timing_enable": (c_int, [H, c_int]),
+        "bpf_timing_read": (c_int, [H, c_int, POINTER(c_double), POINTER(c_double), POINTER(c_int)]),
+        "bpf_version": (c_char_p, []),
+        "bpf_status_string": (c_char_p, [c_int]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    return L
+
+
+def load_library(path: str = LIB_PATH):
+    """Load the shared library without touching the GPU (CPU-safe)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(path):
+            raise OSError(f"libbi_b200 shared library not built: {path} (run libbi_b200.build.build())")
+        _lib = _declare(ctypes.CDLL(path))
+    return _lib
+
+
+def lib():
+    """The loaded library, for compute calls: requires a CUDA device."""
+    import torch
+
+    if not torch.cuda.is_available():
+        raise RuntimeError("libbi_b200 needs a CUDA device; there is no CPU fallback")
+    return load_library()
+
+
+def status_string(status: int) -> str:
+    try:
+        return load_library().bpf_status_string(status).decode()
+    except OSError:
+        return "library not loaded"
+
+
+def check(status: int, what: str) -> None:
+    if status == BPF_OK:
+        return
+    if status == BPF_E_DEGENERATE:
+        raise ParticleFilterDegeneratedException(status, what)
+    raise BpfError(status, what)

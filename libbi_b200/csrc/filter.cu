@@ -1,0 +1,612 @@
+// Filter handle and the C ABI (include/libbi_b200.h).
+//
+// The handle owns what LibBi's generated filter client builds
+// (share/tt/cpp/client/filter_cpu.cpp.tt:105-184): the particle State
+// (structure of arrays, two buffers so that the ancestor gather is fused into
+// the next transition's loads), the BootstrapPFState fields (log-weights,
+// ancestors, ess, logLikelihood, logIncrements), the resampler's scratch and
+// the counter-based RNG.  One BootstrapPF::step is a short, fixed sequence of
+// kernels on the handle's stream; nothing returns to the host unless asked.
+#include "internal.cuh"
+
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <cmath>
+#include <vector>
+
+static thread_local cudaError_t g_last_cuda_error = cudaSuccess;
+void bpf_set_last_cuda_error(cudaError_t e) { g_last_cuda_error = e; }
+
+struct bpf_handle {
+  bpf::ModelArgs model;
+  bpf_config cfg;
+  int n = 0, ld = 0, dim = 0, esz = 0;
+  void* x[2] = {nullptr, nullptr};
+  int cur = 0;
+  double* lw = nullptr;
+  int* as = nullptr;
+  void* y_dev = nullptr;
+  size_t y_cap = 0;
+  double* hist = nullptr;  // per-step (inc, ess, resampled) for bpf_filter
+  int hist_cap = 0;
+  bpf::ResampleScratch rs;
+  cudaStream_t stream = nullptr;
+  int step = 0;
+  // optional device timing: 3 events per step (before resample, before
+  // transition, after transition)
+  bool timing = false;
+  std::vector<cudaEvent_t> ev;
+  int ev_steps = 0;
+};
+
+struct bpf_resampler {
+  int kind = 0, B = 0;
+  cudaStream_t stream = nullptr;
+  bpf::ResampleScratch rs;
+};
+
+namespace {
+
+int check_model(const bpf_model_desc* m) {
+  if (!m) return BPF_E_INVALID;
+  if (m->precision != BPF_F32 && m->precision != BPF_F64) return BPF_E_INVALID;
+  if (m->kind == BPF_MODEL_L96) {
+    if (m->integrator != BPF_ODE_RK4) return BPF_E_INVALID;
+    const int ok_dims[] = {4, 8, 16, 32, 40, 64};
+    bool ok = false;
+    for (int d : ok_dims) ok |= (m->dim == d);
+    if (!ok) return BPF_E_INVALID;
+    if (!(m->h > 0.0) || !(m->theta[1] >= 0.0) || !(m->theta[2] > 0.0)) return BPF_E_INVALID;
+  } else if (m->kind == BPF_MODEL_PZ) {
+    if (m->integrator != BPF_ODE_RK43 || m->dim != 2 || m->precision != BPF_F64) return BPF_E_INVALID;
+    if (!(m->h > 0.0) || !(m->theta[5] >= 0.0) || !(m->theta[6] > 0.0)) return BPF_E_INVALID;
+    if (!(m->atoler > 0.0) || !(m->rtoler >= 0.0)) return BPF_E_INVALID;
+  } else {
+    return BPF_E_INVALID;
+  }
+  return BPF_OK;
+}
+
+// observed values per observation: every component for L96, log P for PZ
+int nobs(const bpf_handle* h) { return h->model.kind == BPF_MODEL_L96 ? h->dim : 1; }
+
+int ensure_y(bpf_handle* h, size_t bytes) {
+  if (bytes <= h->y_cap) return BPF_OK;
+  if (h->y_dev) cudaFree(h->y_dev);
+  h->y_dev = nullptr;
+  h->y_cap = 0;
+  if (cudaMalloc(&h->y_dev, bytes) != cudaSuccess) return BPF_E_NOMEM;
+  h->y_cap = bytes;
+  return BPF_OK;
+}
+
+int read_stats(bpf_handle* h, bpf::StepStats* out) {
+  BPF_TRY(cudaMemcpyAsync(out, h->rs.stats, sizeof(*out), cudaMemcpyDeviceToHost, h->stream));
+  BPF_TRY(cudaStreamSynchronize(h->stream));
+  return BPF_OK;
+}
+
+// Resample (gated on the device flag set by the previous correct), then the
+// fused transition + observation + reduction.  y_dev: device pointer or null.
+int timing_event(bpf_handle* h, int which) {
+  const size_t idx = (size_t)h->ev_steps * 3 + which;
+  while (h->ev.size() <= idx) {
+    cudaEvent_t e;
+    BPF_TRY(cudaEventCreate(&e));
+    h->ev.push_back(e);
+  }
+  BPF_TRY(cudaEventRecord(h->ev[idx], h->stream));
+  return BPF_OK;
+}
+
+int enqueue_step(bpf_handle* h, double t1, double t2, const void* y_dev) {
+  const int k = h->step + 1;
+  if (h->timing) {
+    int rc = timing_event(h, 0);
+    if (rc) return rc;
+  }
+  const int* gate = &h->rs.stats->resample;
+  bpf::ResampleArgs ra;
+  ra.kind = h->cfg.resampler;
+  ra.n = h->n;
+  ra.B = h->cfg.metropolis_steps;
+  ra.lw = h->lw;
+  ra.uniforms = nullptr;
+  ra.seed = h->cfg.seed;
+  ra.step = k;
+  ra.permute = 1;
+  ra.as = h->as;
+  ra.Os_out = nullptr;
+  ra.gate = gate;
+  ra.max_known = true;
+  int rc = bpf::launch_resample(ra, h->rs, h->stream);
+  if (rc) return rc;
+  if (h->timing) {
+    rc = timing_event(h, 1);
+    if (rc) return rc;
+  }
+  bpf::TransitionArgs ta;
+  ta.x_in = h->x[h->cur];
+  ta.x_out = h->x[h->cur ^ 1];
+  ta.ld = h->ld;
+  ta.n = h->n;
+  ta.as = h->as;
+  ta.lw = h->lw;
+  ta.y = y_dev;
+  ta.t1 = t1;
+  ta.t2 = t2;
+  ta.seed = h->cfg.seed;
+  ta.step = k;
+  ta.stats = h->rs.stats;
+  ta.partials = h->rs.partials;
+  ta.counter = h->rs.counters + 4;
+  rc = bpf::launch_transition(h->model, ta, h->stream);
+  if (rc) return rc;
+  if (h->timing) {
+    rc = timing_event(h, 2);
+    if (rc) return rc;
+    h->ev_steps += 1;
+  }
+  h->cur ^= 1;
+  h->step = k;
+  return BPF_OK;
+}
+
+__global__ void k_record(const bpf::StepStats* st, double* hist, int k) {
+  hist[3 * k + 0] = st->inc;
+  hist[3 * k + 1] = st->ess;
+  hist[3 * k + 2] = (double)st->resampled;
+}
+
+__global__ void k_set_status_ok(bpf::StepStats* st) { st->status = BPF_OK; }
+
+// set_elements(s.logWeights(), s.logLikelihood), Resampler.hpp:177
+__global__ void k_reset_lw(double* lw, int n, const bpf::StepStats* st) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) lw[i] = st->ll;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* bpf_version(void) { return "libbi_b200 0.1 (sm_100a)"; }
+
+const char* bpf_status_string(int s) {
+  switch (s) {
+    case BPF_OK: return "ok";
+    case BPF_E_DEGENERATE: return "particle filter degenerated (weights sum to zero or are not finite)";
+    case BPF_E_INVALID: return "invalid argument";
+    case BPF_E_CUDA: return cudaGetErrorString(g_last_cuda_error);
+    case BPF_E_TIMEOUT: return "bounded device wait gave up";
+    case BPF_E_NOMEM: return "device allocation failed";
+    default: return "unknown status";
+  }
+}
+
+int bpf_create(const bpf_model_desc* model, const bpf_config* config, bpf_handle** out) {
+  if (!out || !config) return BPF_E_INVALID;
+  *out = nullptr;
+  int rc = check_model(model);
+  if (rc) return rc;
+  if (config->nparticles <= 0) return BPF_E_INVALID;
+  if (config->resampler < BPF_RESAMPLER_SYSTEMATIC || config->resampler > BPF_RESAMPLER_METROPOLIS)
+    return BPF_E_INVALID;
+  if (config->resampler == BPF_RESAMPLER_METROPOLIS && config->metropolis_steps < 0) return BPF_E_INVALID;
+  // Resampler constructor pre-condition, share/src/bi/resampler/Resampler.hpp:129
+  if (!(config->ess_rel >= 0.0 && config->ess_rel <= 1.0)) return BPF_E_INVALID;
+  bpf_handle* h = new (std::nothrow) bpf_handle();
+  if (!h) return BPF_E_NOMEM;
+  h->model.kind = model->kind;
+  h->model.dim = model->dim;
+  h->model.precision = model->precision;
+  h->model.integrator = model->integrator;
+  h->model.h = model->h;
+  h->model.atoler = model->atoler;
+  h->model.rtoler = model->rtoler;
+  for (int i = 0; i < BPF_MAX_THETA; ++i) h->model.theta[i] = model->theta[i];
+  h->cfg = *config;
+  h->stream = (cudaStream_t)config->stream;
+  h->n = config->nparticles;
+  // leading dimension rounded up to 32 particles (State::roundup for CUDA,
+  // share/src/bi/state/State.hpp:40-57), so every component row is 128-byte aligned
+  h->ld = ((h->n + 31) / 32) * 32;
+  h->dim = model->dim;
+  h->esz = model->precision == BPF_F64 ? 8 : 4;
+  const size_t xb = (size_t)h->ld * h->dim * h->esz;
+  if (cudaMalloc(&h->x[0], xb) != cudaSuccess || cudaMalloc(&h->x[1], xb) != cudaSuccess ||
+      cudaMalloc((void**)&h->lw, (size_t)h->ld * sizeof(double)) != cudaSuccess ||
+      cudaMalloc((void**)&h->as, (size_t)h->ld * sizeof(int)) != cudaSuccess) {
+    bpf_destroy(h);
+    return BPF_E_NOMEM;
+  }
+  rc = bpf::scratch_alloc(h->rs, h->n);
+  if (rc) { bpf_destroy(h); return rc; }
+  rc = bpf_init(h);
+  if (rc) { bpf_destroy(h); return rc; }
+  *out = h;
+  return BPF_OK;
+}
+
+int bpf_destroy(bpf_handle* h) {
+  if (!h) return BPF_OK;
+  if (h->stream) cudaStreamSynchronize(h->stream); else cudaDeviceSynchronize();
+  if (h->x[0]) cudaFree(h->x[0]);
+  if (h->x[1]) cudaFree(h->x[1]);
+  if (h->lw) cudaFree(h->lw);
+  if (h->as) cudaFree(h->as);
+  if (h->y_dev) cudaFree(h->y_dev);
+  if (h->hist) cudaFree(h->hist);
+  for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
+  bpf::scratch_free(h->rs);
+  delete h;
+  return BPF_OK;
+}
+
+int bpf_state_ptrs(bpf_handle* h, void** x, double** lw, int** as, int* ld) {
+  if (!h) return BPF_E_INVALID;
+  if (x) *x = h->x[h->cur];
+  if (lw) *lw = h->lw;
+  if (as) *as = h->as;
+  if (ld) *ld = h->ld;
+  return BPF_OK;
+}
+
+int bpf_init(bpf_handle* h) {
+  if (!h) return BPF_E_INVALID;
+  h->cur = 0;
+  h->step = 0;
+  return bpf::launch_init(h->model, h->x[0], h->ld, h->n, h->lw, h->cfg.seed, h->rs.stats, h->cfg.ess_rel,
+                          h->stream);
+}
+
+static void fill_out(const bpf::StepStats& s, bpf_step_out* out) {
+  out->ess = s.ess;
+  out->log_weight_sum = s.lW;
+  out->log_increment = s.inc;
+  out->log_likelihood = s.ll;
+  out->resampled = s.resampled;
+  out->status = s.status;
+}
+
+int bpf_step(bpf_handle* h, double t1, double t2, const void* y, bpf_step_out* out) {
+  if (!h || !(t1 < t2)) return BPF_E_INVALID;
+  const void* yd = nullptr;
+  if (y) {
+    const size_t yb = (size_t)nobs(h) * h->esz;
+    int rc = ensure_y(h, yb);
+    if (rc) return rc;
+    BPF_TRY(cudaMemcpyAsync(h->y_dev, y, yb, cudaMemcpyHostToDevice, h->stream));
+    yd = h->y_dev;
+  }
+  int rc = enqueue_step(h, t1, t2, yd);
+  if (rc) return rc;
+  if (out) {
+    bpf::StepStats s;
+    rc = read_stats(h, &s);
+    if (rc) return rc;
+    fill_out(s, out);
+    return s.status;
+  }
+  return BPF_OK;
+}
+
+int bpf_step_device(bpf_handle* h, double t1, double t2, const void* y_dev, bpf_step_out* out) {
+  if (!h || !(t1 < t2)) return BPF_E_INVALID;
+  int rc = enqueue_step(h, t1, t2, y_dev);
+  if (rc) return rc;
+  if (out) {
+    bpf::StepStats s;
+    rc = read_stats(h, &s);
+    if (rc) return rc;
+    fill_out(s, out);
+    return s.status;
+  }
+  return BPF_OK;
+}
+
+int bpf_filter(bpf_handle* h, int T, double t0, double dt, const void* y, double* log_increments, double* ess,
+               double* log_likelihood) {
+  if (!h || T <= 0 || !(dt > 0.0) || !y) return BPF_E_INVALID;
+  int rc = bpf_init(h);
+  if (rc) return rc;
+  const size_t yb = (size_t)T * nobs(h) * h->esz;
+  rc = ensure_y(h, yb);
+  if (rc) return rc;
+  BPF_TRY(cudaMemcpyAsync(h->y_dev, y, yb, cudaMemcpyHostToDevice, h->stream));
+  if (T > h->hist_cap) {
+    if (h->hist) cudaFree(h->hist);
+    h->hist = nullptr;
+    h->hist_cap = 0;
+    if (cudaMalloc((void**)&h->hist, (size_t)3 * T * sizeof(double)) != cudaSuccess) return BPF_E_NOMEM;
+    h->hist_cap = T;
+  }
+  for (int k = 1; k <= T; ++k) {
+    const double t1 = t0 + (k - 1) * dt, t2 = t0 + k * dt;
+    rc = enqueue_step(h, t1, t2, (const char*)h->y_dev + (size_t)(k - 1) * nobs(h) * h->esz);
+    if (rc) return rc;
+    k_record<<<1, 1, 0, h->stream>>>(h->rs.stats, h->hist, k - 1);
+  }
+  BPF_TRY(cudaGetLastError());
+  // BootstrapPF::term: logLikelihood = logsumexp(lws) - log P
+  // (share/src/bi/filter/BootstrapPF.hpp:192-196); keep the step statistics
+  bpf::StepStats s;
+  rc = read_stats(h, &s);
+  if (rc) return rc;
+  if (s.status != BPF_OK) return s.status;
+  rc = bpf::launch_logsumexp(h->lw, h->n, h->rs, h->stream);
+  if (rc) return rc;
+  bpf::StepStats s2;
+  rc = read_stats(h, &s2);
+  if (rc) return rc;
+  if (log_likelihood) *log_likelihood = s2.lW - std::log((double)h->n);
+  // restore the step statistics the term reduction overwrote
+  BPF_TRY(cudaMemcpyAsync(h->rs.stats, &s, sizeof(s), cudaMemcpyHostToDevice, h->stream));
+  if (log_increments || ess) {
+    double* tmp = new (std::nothrow) double[(size_t)3 * T];
+    if (!tmp) return BPF_E_NOMEM;
+    cudaError_t e = cudaMemcpyAsync(tmp, h->hist, (size_t)3 * T * sizeof(double), cudaMemcpyDeviceToHost,
+                                    h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) { delete[] tmp; bpf_set_last_cuda_error(e); return BPF_E_CUDA; }
+    for (int k = 0; k < T; ++k) {
+      if (log_increments) log_increments[k] = tmp[3 * k];
+      if (ess) ess[k] = tmp[3 * k + 1];
+    }
+    delete[] tmp;
+  }
+  BPF_TRY(cudaStreamSynchronize(h->stream));
+  return BPF_OK;
+}
+
+int bpf_reduce(bpf_handle* h, double* lW, double* ess) {
+  if (!h) return BPF_E_INVALID;
+  bpf::StepStats keep;
+  int rc = read_stats(h, &keep);
+  if (rc) return rc;
+  rc = bpf::launch_lw_reduce(h->lw, h->n, h->rs, h->stream);
+  if (rc) return rc;
+  bpf::StepStats s;
+  rc = read_stats(h, &s);
+  if (rc) return rc;
+  if (lW) *lW = s.lW;
+  if (ess) *ess = s.ess;
+  // the reduction leaves mx/s1/s2/ess/lW of the current weights; keep the
+  // filter's likelihood bookkeeping
+  s.ll = keep.ll; s.inc = keep.inc; s.step = keep.step; s.resample = keep.resample;
+  s.resampled = keep.resampled; s.ess_rel = keep.ess_rel; s.n = keep.n;
+  BPF_TRY(cudaMemcpyAsync(h->rs.stats, &s, sizeof(s), cudaMemcpyHostToDevice, h->stream));
+  BPF_TRY(cudaStreamSynchronize(h->stream));
+  return BPF_OK;
+}
+
+int bpf_resample(bpf_handle* h, const double* uniforms, int* ancestors_out) {
+  if (!h) return BPF_E_INVALID;
+  // fresh max / reduction over the current log-weights
+  bpf::StepStats keep;
+  int rc = read_stats(h, &keep);
+  if (rc) return rc;
+  if (keep.status != BPF_OK) return keep.status;
+  rc = bpf::launch_lw_reduce(h->lw, h->n, h->rs, h->stream);
+  if (rc) return rc;
+  bpf::ResampleArgs ra;
+  ra.kind = h->cfg.resampler;
+  ra.n = h->n;
+  ra.B = h->cfg.metropolis_steps;
+  ra.lw = h->lw;
+  ra.uniforms = uniforms;
+  ra.seed = h->cfg.seed;
+  ra.step = h->step + 1;
+  ra.permute = 1;
+  ra.as = h->as;
+  ra.Os_out = nullptr;
+  ra.gate = nullptr;
+  ra.max_known = true;
+  rc = bpf::launch_resample(ra, h->rs, h->stream);
+  if (rc) return rc;
+  bpf::StepStats s;
+  rc = read_stats(h, &s);
+  if (rc) return rc;
+  if (s.status != BPF_OK) return s.status;
+  // gather (out of place into the other buffer) and reset log-weights to the
+  // log-likelihood (Resampler.hpp:176-177)
+  const void* X = h->x[h->cur];
+  void* Y = h->x[h->cur ^ 1];
+  rc = bpf::launch_gather(h->as, X, Y, h->n, h->dim, h->ld, h->esz, nullptr, h->stream);
+  if (rc) return rc;
+  h->cur ^= 1;
+  k_reset_lw<<<(h->n + 255) / 256, 256, 0, h->stream>>>(h->lw, h->n, h->rs.stats);
+  BPF_TRY(cudaGetLastError());
+  if (ancestors_out) {
+    BPF_TRY(cudaMemcpyAsync(ancestors_out, h->as, (size_t)h->n * sizeof(int), cudaMemcpyDeviceToDevice,
+                            h->stream));
+  }
+  keep.resample = 0;
+  keep.resampled = 1;
+  BPF_TRY(cudaMemcpyAsync(h->rs.stats, &keep, sizeof(keep), cudaMemcpyHostToDevice, h->stream));
+  BPF_TRY(cudaStreamSynchronize(h->stream));
+  return BPF_OK;
+}
+
+int bpf_timing_enable(bpf_handle* h, int enable) {
+  if (!h) return BPF_E_INVALID;
+  h->timing = enable != 0;
+  h->ev_steps = 0;
+  return BPF_OK;
+}
+
+int bpf_timing_read(bpf_handle* h, int reset, double* resample_ms, double* transition_ms, int* steps) {
+  if (!h) return BPF_E_INVALID;
+  BPF_TRY(cudaStreamSynchronize(h->stream));
+  double r = 0.0, t = 0.0;
+  for (int s = 0; s < h->ev_steps; ++s) {
+    float a = 0.f, b = 0.f;
+    BPF_TRY(cudaEventElapsedTime(&a, h->ev[3 * s], h->ev[3 * s + 1]));
+    BPF_TRY(cudaEventElapsedTime(&b, h->ev[3 * s + 1], h->ev[3 * s + 2]));
+    r += a;
+    t += b;
+  }
+  if (resample_ms) *resample_ms = r;
+  if (transition_ms) *transition_ms = t;
+  if (steps) *steps = h->ev_steps;
+  if (reset) h->ev_steps = 0;
+  return BPF_OK;
+}
+
+// ---- stand-alone resampler ------------------------------------------------
+
+int bpf_resampler_create(int kind, int max_n, int metropolis_steps, void* stream, bpf_resampler** out) {
+  if (!out) return BPF_E_INVALID;
+  *out = nullptr;
+  if (kind < BPF_RESAMPLER_SYSTEMATIC || kind > BPF_RESAMPLER_METROPOLIS || max_n <= 0 || metropolis_steps < 0)
+    return BPF_E_INVALID;
+  bpf_resampler* r = new (std::nothrow) bpf_resampler();
+  if (!r) return BPF_E_NOMEM;
+  r->kind = kind;
+  r->B = metropolis_steps;
+  r->stream = (cudaStream_t)stream;
+  int rc = bpf::scratch_alloc(r->rs, max_n);
+  if (rc) { delete r; return rc; }
+  *out = r;
+  return BPF_OK;
+}
+
+int bpf_resampler_destroy(bpf_resampler* r) {
+  if (!r) return BPF_OK;
+  if (r->stream) cudaStreamSynchronize(r->stream); else cudaDeviceSynchronize();
+  bpf::scratch_free(r->rs);
+  delete r;
+  return BPF_OK;
+}
+
+static int reset_status(bpf_resampler* r) {
+  k_set_status_ok<<<1, 1, 0, r->stream>>>(r->rs.stats);
+  BPF_TRY(cudaGetLastError());
+  return BPF_OK;
+}
+
+static int read_rs_stats(bpf_resampler* r, bpf::StepStats* s) {
+  BPF_TRY(cudaMemcpyAsync(s, r->rs.stats, sizeof(*s), cudaMemcpyDeviceToHost, r->stream));
+  BPF_TRY(cudaStreamSynchronize(r->stream));
+  return BPF_OK;
+}
+
+int bpf_ess_reduce(bpf_resampler* r, const double* lw, int n, double* lW, double* ess) {
+  if (!r || !lw || n <= 0 || n > r->rs.max_n) return BPF_E_INVALID;
+  int rc = reset_status(r);
+  if (rc) return rc;
+  rc = bpf::launch_lw_reduce(lw, n, r->rs, r->stream);
+  if (rc) return rc;
+  bpf::StepStats s;
+  rc = read_rs_stats(r, &s);
+  if (rc) return rc;
+  if (lW) *lW = s.lW;
+  if (ess) *ess = s.ess;
+  return BPF_OK;
+}
+
+int bpf_logsumexp_reduce(bpf_resampler* r, const double* lw, int n, double* out) {
+  if (!r || !lw || n <= 0 || n > r->rs.max_n) return BPF_E_INVALID;
+  int rc = reset_status(r);
+  if (rc) return rc;
+  rc = bpf::launch_logsumexp(lw, n, r->rs, r->stream);
+  if (rc) return rc;
+  bpf::StepStats s;
+  rc = read_rs_stats(r, &s);
+  if (rc) return rc;
+  if (out) *out = s.lW;
+  return BPF_OK;
+}
+
+int bpf_resampler_ancestors(bpf_resampler* r, const double* lw, int n, const double* uniforms, int permute,
+                            int* as, int* Os) {
+  if (!r || !lw || !as || n <= 0 || n > r->rs.max_n) return BPF_E_INVALID;
+  int rc = reset_status(r);
+  if (rc) return rc;
+  bpf::ResampleArgs ra;
+  ra.kind = r->kind;
+  ra.n = n;
+  ra.B = r->B;
+  ra.lw = lw;
+  ra.uniforms = uniforms;
+  ra.seed = 0;
+  ra.step = 0;
+  ra.permute = permute;
+  ra.as = as;
+  ra.Os_out = Os;
+  ra.gate = nullptr;
+  ra.max_known = false;
+  rc = bpf::launch_resample(ra, r->rs, r->stream);
+  if (rc) return rc;
+  bpf::StepStats s;
+  rc = read_rs_stats(r, &s);
+  if (rc) return rc;
+  return s.status;
+}
+
+int bpf_gather_rows(const int* as, const void* X, void* Y, int n, int d, int ld, int elem_size, void* stream) {
+  if (!as || !X || !Y || X == Y) return BPF_E_INVALID;
+  return bpf::launch_gather(as, X, Y, n, d, ld, elem_size, nullptr, (cudaStream_t)stream);
+}
+
+// ---- checkpoint ------------------------------------------------------------
+
+struct SnapHeader {
+  uint64_t magic;
+  int n, ld, dim, esz, step, pad;
+  bpf::StepStats stats;
+};
+
+static const uint64_t kSnapMagic = 0x3130304250464253ull;  // "SBFPB001"
+
+int bpf_snapshot_size(bpf_handle* h, uint64_t* bytes) {
+  if (!h || !bytes) return BPF_E_INVALID;
+  *bytes = sizeof(SnapHeader) + (uint64_t)h->ld * h->dim * h->esz + (uint64_t)h->n * (sizeof(double) + sizeof(int));
+  return BPF_OK;
+}
+
+int bpf_snapshot(bpf_handle* h, void* buf, uint64_t bytes) {
+  uint64_t need;
+  if (bpf_snapshot_size(h, &need) || !buf || bytes < need) return BPF_E_INVALID;
+  SnapHeader hd;
+  std::memset(&hd, 0, sizeof(hd));
+  hd.magic = kSnapMagic;
+  hd.n = h->n; hd.ld = h->ld; hd.dim = h->dim; hd.esz = h->esz; hd.step = h->step;
+  int rc = read_stats(h, &hd.stats);
+  if (rc) return rc;
+  char* p = (char*)buf;
+  std::memcpy(p, &hd, sizeof(hd));
+  p += sizeof(hd);
+  const size_t xb = (size_t)h->ld * h->dim * h->esz;
+  BPF_TRY(cudaMemcpyAsync(p, h->x[h->cur], xb, cudaMemcpyDeviceToHost, h->stream));
+  p += xb;
+  BPF_TRY(cudaMemcpyAsync(p, h->lw, (size_t)h->n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  p += (size_t)h->n * sizeof(double);
+  BPF_TRY(cudaMemcpyAsync(p, h->as, (size_t)h->n * sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  BPF_TRY(cudaStreamSynchronize(h->stream));
+  return BPF_OK;
+}
+
+int bpf_restore(bpf_handle* h, const void* buf, uint64_t bytes) {
+  uint64_t need;
+  if (bpf_snapshot_size(h, &need) || !buf || bytes < need) return BPF_E_INVALID;
+  SnapHeader hd;
+  std::memcpy(&hd, buf, sizeof(hd));
+  if (hd.magic != kSnapMagic || hd.n != h->n || hd.ld != h->ld || hd.dim != h->dim || hd.esz != h->esz)
+    return BPF_E_INVALID;
+  const char* p = (const char*)buf + sizeof(hd);
+  const size_t xb = (size_t)h->ld * h->dim * h->esz;
+  h->cur = 0;
+  BPF_TRY(cudaMemcpyAsync(h->x[0], p, xb, cudaMemcpyHostToDevice, h->stream));
+  p += xb;
+  BPF_TRY(cudaMemcpyAsync(h->lw, p, (size_t)h->n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  p += (size_t)h->n * sizeof(double);
+  BPF_TRY(cudaMemcpyAsync(h->as, p, (size_t)h->n * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  BPF_TRY(cudaMemcpyAsync(h->rs.stats, &hd.stats, sizeof(hd.stats), cudaMemcpyHostToDevice, h->stream));
+  BPF_TRY(cudaStreamSynchronize(h->stream));
+  h->step = hd.step;
+  return BPF_OK;
+}
+
+}  // extern "C"

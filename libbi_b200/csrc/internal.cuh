@@ -1,0 +1,265 @@
+// Internal declarations shared by the libbi_b200 CUDA sources.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "../../include/libbi_b200.h"
+#include "../../include/bpf_philox.h"
+
+#define BPF_TRY(call)                                          \
+  do {                                                         \
+    cudaError_t e_ = (call);                                   \
+    if (e_ != cudaSuccess) { bpf_set_last_cuda_error(e_); return BPF_E_CUDA; } \
+  } while (0)
+
+void bpf_set_last_cuda_error(cudaError_t e);
+
+namespace bpf {
+
+// Resampler tile: 256 threads x 8 items.
+constexpr int kBlock = 256;
+constexpr int kItems = 8;
+constexpr int kTile = kBlock * kItems;
+
+inline int ntiles(int n) { return (n + kTile - 1) / kTile; }
+
+// ---------------------------------------------------------------------------
+// Exact 128-bit fixed-point sums.
+//
+// Normalised weights w = exp(lw - max) lie in [0, 1].  Each is rounded once
+// to a multiple of 2^-63 (q = rint(w * 2^63), at most 2^63) and all prefix
+// sums are formed exactly in 128-bit integers.  Integer addition is
+// associative, so every tile order, look-back path and thread count gives the
+// same sums: the prefix sum is deterministic and at least as accurate as a
+// sequential FP64 sum.  A sum is rounded to FP64 once, by u128_to_weight().
+// ---------------------------------------------------------------------------
+struct u128 {
+  unsigned long long lo, hi;
+};
+
+__host__ __device__ __forceinline__ u128 u128_zero() { u128 r; r.lo = 0; r.hi = 0; return r; }
+
+__host__ __device__ __forceinline__ u128 u128_add(u128 a, u128 b) {
+  u128 r;
+  r.lo = a.lo + b.lo;
+  r.hi = a.hi + b.hi + (r.lo < a.lo ? 1ull : 0ull);
+  return r;
+}
+
+__host__ __device__ __forceinline__ u128 u128_sub(u128 a, u128 b) {
+  u128 r;
+  r.lo = a.lo - b.lo;
+  r.hi = a.hi - b.hi - (a.lo < b.lo ? 1ull : 0ull);
+  return r;
+}
+
+// weight in [0,1] -> fixed point q = rint(w * 2^63)
+__device__ __forceinline__ unsigned long long weight_to_fixed(double w) {
+  return __double2ull_rn(__dmul_rn(w, 9223372036854775808.0));
+}
+
+// fixed-point weight sum -> FP64 value of the sum (unscaled): hi*2 + lo*2^-63
+__device__ __forceinline__ double u128_to_weight(u128 q) {
+  return __dadd_rn(__dmul_rn((double)q.hi, 2.0),
+                   __dmul_rn(__ull2double_rn(q.lo), 1.0842021724855044e-19 /* 2^-63 */));
+}
+
+// non-negative double -> fixed point with 64 fraction bits: (floor(v), frac(v)*2^64 truncated)
+__device__ __forceinline__ u128 spacing_to_fixed(double v) {
+  double f = floor(v);
+  u128 r;
+  r.hi = (unsigned long long)f;
+  r.lo = __double2ull_rz(__dmul_rn(__dsub_rn(v, f), 18446744073709551616.0));
+  return r;
+}
+
+// fixed point with 64 fraction bits -> double: hi + lo*2^-64
+__device__ __forceinline__ double fixed_to_spacing(u128 q) {
+  return __dadd_rn((double)q.hi, __dmul_rn(__ull2double_rn(q.lo), 5.421010862427522e-20 /* 2^-64 */));
+}
+
+__device__ __forceinline__ u128 shfl_up_u128(u128 v, int d) {
+  u128 r;
+  r.lo = __shfl_up_sync(0xffffffffu, v.lo, d);
+  r.hi = __shfl_up_sync(0xffffffffu, v.hi, d);
+  return r;
+}
+
+__device__ __forceinline__ u128 shfl_u128(u128 v, int src) {
+  u128 r;
+  r.lo = __shfl_sync(0xffffffffu, v.lo, src);
+  r.hi = __shfl_sync(0xffffffffu, v.hi, src);
+  return r;
+}
+
+// Block-wide exclusive scan of one u128 per thread (blockDim.x == kBlock).
+// Returns the exclusive prefix; *total receives the block sum.
+__device__ __forceinline__ u128 block_exclusive_scan_u128(u128 v, u128* total) {
+  __shared__ u128 warp_tot[kBlock / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  u128 inc = v;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    u128 o = shfl_up_u128(inc, d);
+    if (lane >= d) inc = u128_add(inc, o);
+  }
+  if (lane == 31) warp_tot[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    u128 t = lane < kBlock / 32 ? warp_tot[lane] : u128_zero();
+#pragma unroll
+    for (int d = 1; d < kBlock / 32; d <<= 1) {
+      u128 o = shfl_up_u128(t, d);
+      if (lane >= d) t = u128_add(t, o);
+    }
+    if (lane < kBlock / 32) warp_tot[lane] = t;  // inclusive warp prefixes
+  }
+  __syncthreads();
+  u128 warp_excl = warp > 0 ? warp_tot[warp - 1] : u128_zero();
+  *total = warp_tot[kBlock / 32 - 1];
+  u128 excl = u128_sub(inc, v);
+  __syncthreads();
+  return u128_add(warp_excl, excl);
+}
+
+// Block-wide exclusive scan of one int per thread.
+__device__ __forceinline__ int block_exclusive_scan_int(int v, int* total) {
+  __shared__ int wt[kBlock / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int inc = v;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    int o = __shfl_up_sync(0xffffffffu, inc, d);
+    if (lane >= d) inc += o;
+  }
+  if (lane == 31) wt[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    int t = lane < kBlock / 32 ? wt[lane] : 0;
+#pragma unroll
+    for (int d = 1; d < kBlock / 32; d <<= 1) {
+      int o = __shfl_up_sync(0xffffffffu, t, d);
+      if (lane >= d) t += o;
+    }
+    if (lane < kBlock / 32) wt[lane] = t;
+  }
+  __syncthreads();
+  int r = (warp > 0 ? wt[warp - 1] : 0) + inc - v;
+  *total = wt[kBlock / 32 - 1];
+  __syncthreads();
+  return r;
+}
+
+// nanexp: share/src/bi/math/function.hpp:158-164 (NaN gives zero)
+__device__ __forceinline__ double nanexp(double x) { return isnan(x) ? 0.0 : exp(x); }
+
+// nan_less max: share/src/bi/primitive/functor.hpp:43-53 (NaN orders first)
+__device__ __forceinline__ double nan_max(double a, double b) {
+  if (isnan(a)) return b;
+  if (isnan(b)) return a;
+  return a < b ? b : a;
+}
+
+// ---------------------------------------------------------------------------
+// Log-weight reduction (max, sum e, sum e^2) with e = nanexp(lw - max).
+// ---------------------------------------------------------------------------
+struct LwPartial {
+  double mx, s1, s2;
+};
+
+// Device-side results of a reduction / filter step.
+struct StepStats {
+  double mx;        // max log-weight
+  double s1, s2;    // sum e, sum e^2 with e = nanexp(lw - mx)
+  double ess;       // s1^2 / s2
+  double lW;        // mx + log s1 - log N
+  double ll;        // logLikelihood
+  double inc;       // logIncrement of the latest correct
+  int resample;     // next step resamples (ESS < essRel*N after an observed step)
+  int resampled;    // this step resampled
+  int status;       // BPF_OK / BPF_E_DEGENERATE / BPF_E_TIMEOUT
+  int step;         // schedule index of the latest correct (0 = initial)
+  double ess_rel;
+  int n;
+  int pad;
+};
+
+// Scratch of the resampler pipeline for up to max_n particles.
+struct ResampleScratch {
+  int max_n = 0;
+  int max_tiles = 0;
+  u128* tile_sum = nullptr;     // per-tile weight sums
+  u128* tile_prefix = nullptr;  // exclusive prefixes (+1 entry: total)
+  u128* vtile_sum = nullptr;    // per-tile spacing sums (multinomial)
+  u128* vtile_prefix = nullptr;
+  int* zcount = nullptr;        // per-tile childless counts
+  int* zprefix = nullptr;       // exclusive prefixes (+1 entry: total)
+  int* icount = nullptr;        // per-tile integer sums (offspring counts)
+  int* iprefix = nullptr;
+  int* Os = nullptr;            // cumulative offspring
+  int* E = nullptr;             // cumulative extra copies
+  int* o = nullptr;             // offspring counts (Metropolis)
+  double* Ws = nullptr;         // FP64 cumulative weights (multinomial search)
+  double* lu = nullptr;         // log sorted uniforms (multinomial)
+  unsigned* counters = nullptr; // last-block tickets
+  StepStats* stats = nullptr;   // reduction results
+  LwPartial* partials = nullptr;
+  int max_partials = 0;
+};
+
+int scratch_alloc(ResampleScratch& s, int max_n);
+void scratch_free(ResampleScratch& s);
+
+// Reduction of lw[0..n) into s.stats (mx, s1, s2, ess, lW); stats->ll/inc untouched.
+int launch_lw_reduce(const double* lw, int n, ResampleScratch& s, cudaStream_t st);
+int launch_logsumexp(const double* lw, int n, ResampleScratch& s, cudaStream_t st);
+
+// Resampler pipelines.  uniforms: device pointer or null (then drawn from
+// Philox with (seed, step)).  gate: device int or null; when non-null the
+// kernels do nothing unless *gate != 0.  mx from s.stats->mx when
+// use_stats_max, else computed first.
+struct ResampleArgs {
+  int kind;
+  int n;
+  int B;
+  const double* lw;
+  const double* uniforms;
+  uint64_t seed;
+  int step;
+  int permute;
+  int* as;
+  int* Os_out;
+  const int* gate;
+  bool max_known;  // s.stats->mx already holds max(lw)
+};
+int launch_resample(const ResampleArgs& a, ResampleScratch& s, cudaStream_t st);
+
+int launch_gather(const int* as, const void* X, void* Y, int n, int d, int ld, int esz,
+                  const int* gate, cudaStream_t st);
+
+// Models
+struct ModelArgs {
+  int kind, dim, precision, integrator;
+  double h, atoler, rtoler;
+  double theta[BPF_MAX_THETA];
+};
+
+struct TransitionArgs {
+  const void* x_in;   // state before the step (model precision, SoA)
+  void* x_out;        // state after the step
+  int ld, n;
+  const int* as;      // ancestors, read when *resampled_flag
+  double* lw;         // FP64 log-weights, updated in place
+  const void* y;      // device observation (dim values) or null
+  double t1, t2;
+  uint64_t seed;
+  int step;
+  StepStats* stats;   // reads resample flag / ll; finalised by the last block
+  LwPartial* partials;
+  unsigned* counter;
+};
+int launch_transition(const ModelArgs& m, const TransitionArgs& a, cudaStream_t st);
+int launch_init(const ModelArgs& m, void* x, int ld, int n, double* lw, uint64_t seed,
+                StepStats* stats, double ess_rel, cudaStream_t st);
+
+}  // namespace bpf

@@ -1,0 +1,662 @@
+// Resamplers of the bootstrap particle filter, B200-native.
+//
+// Reference path (LibBi): Resampler<R>::resample
+// (share/src/bi/resampler/Resampler.hpp:167-182) runs R::precompute
+// (ScanResampler::precompute, share/src/bi/resampler/ScanResampler.hpp:35-40:
+// a Thrust max pass and a Thrust transform_inclusive_scan of nanexp(lw - max))
+// and R::ancestorsPermute, then gathers the state.  The reference's CUDA
+// variants use Thrust for the scan and search and atomics for the
+// permutation (share/src/bi/cuda/resampler/ResamplerKernel.cuh:78-165).
+//
+// Here every pass is a hand-written kernel over tiles of kTile = 2048
+// log-weights (256 threads x 8):
+//   weight tile sums   exact 128-bit fixed-point sums of the weights; the
+//                      last block to finish scans the tile sums (no waiting)
+//   offspring          per tile: exact prefix -> FP64 cumulative weight ->
+//                      cumulative offspring, childless counts
+//   permute            survivors in place; copies fill childless slots by a
+//                      search over the cumulative extra-copy counts
+// The FP64 cumulative weight of element i is the exact sum rounded once, so
+// ancestors are independent of tile order, thread count and timing.
+#include "internal.cuh"
+#include "reduce.cuh"
+
+namespace bpf {
+
+// ---------------------------------------------------------------------------
+// helpers
+// ---------------------------------------------------------------------------
+
+// Signal "this block is done" and return true in every thread of the last
+// block of the grid to finish.  The caller's global writes must precede it.
+__device__ __forceinline__ bool last_block_arrive(unsigned* counter) {
+  __shared__ bool am_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned ticket = atomicAdd(counter, 1u);
+    am_last = (ticket == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (am_last) __threadfence();
+  return am_last;
+}
+
+__device__ __forceinline__ u128 ldcg_u128(const u128* p) {
+  u128 r;
+  r.lo = __ldcg(&p->lo);
+  r.hi = __ldcg(&p->hi);
+  return r;
+}
+
+// Exclusive scan of in[0..T) into out[0..T] (out[T] = total), run by one block.
+__device__ void block_scan_tiles_u128(const u128* in, u128* out, int T) {
+  u128 carry = u128_zero();
+  for (int base = 0; base < T; base += kTile) {
+    u128 v[kItems];
+    u128 loc = u128_zero();
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+      int i = base + threadIdx.x * kItems + k;
+      v[k] = i < T ? ldcg_u128(&in[i]) : u128_zero();
+      loc = u128_add(loc, v[k]);
+    }
+    u128 tot;
+    u128 ex = u128_add(carry, block_exclusive_scan_u128(loc, &tot));
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+      int i = base + threadIdx.x * kItems + k;
+      if (i < T) out[i] = ex;
+      ex = u128_add(ex, v[k]);
+    }
+    carry = u128_add(carry, tot);
+  }
+  if (threadIdx.x == 0) out[T] = carry;
+}
+
+__device__ void block_scan_tiles_int(const int* in, int* out, int T) {
+  int carry = 0;
+  for (int base = 0; base < T; base += kTile) {
+    int v[kItems];
+    int loc = 0;
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+      int i = base + threadIdx.x * kItems + k;
+      v[k] = i < T ? __ldcg(&in[i]) : 0;
+      loc += v[k];
+    }
+    int tot;
+    int ex = carry + block_exclusive_scan_int(loc, &tot);
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+      int i = base + threadIdx.x * kItems + k;
+      if (i < T) out[i] = ex;
+      ex += v[k];
+    }
+    carry += tot;
+  }
+  if (threadIdx.x == 0) out[T] = carry;
+}
+
+// Load the 8 consecutive log-weights of this thread (blocked layout).
+__device__ __forceinline__ void load_blocked(const double* __restrict__ lw, int i0, int n, double v[kItems]) {
+  if (i0 + kItems <= n && ((reinterpret_cast<uintptr_t>(lw + i0) & 15) == 0)) {
+    const double2* p = reinterpret_cast<const double2*>(lw + i0);
+#pragma unroll
+    for (int k = 0; k < kItems / 2; ++k) {
+      double2 t = __ldg(p + k);
+      v[2 * k] = t.x;
+      v[2 * k + 1] = t.y;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) v[k] = (i0 + k < n) ? __ldg(lw + i0 + k) : NAN;
+  }
+}
+
+__device__ __forceinline__ bool gate_closed(const int* gate, const StepStats* st) {
+  if (gate != nullptr && *gate == 0) return true;
+  return st->status != BPF_OK;
+}
+
+// uniform for the multinomial draw consumed at position t (t = 0 first)
+__device__ __forceinline__ double multinomial_uniform(const double* u, int t, uint64_t seed, int step) {
+  if (u) return u[t];
+  bpf_u32x4 r = bpf_draw(seed, (uint32_t)t, (uint32_t)step, 0u, BPF_RNG_MULTINOMIAL);
+  return bpf_u01d(r.v[0], r.v[1]);
+}
+
+// Bentley & Saxe spacing of output slot s: the reference accumulates
+// lMax += log(u)/i for i = n, n-1, ..., 1 and writes slot i-1
+// (share/src/bi/host/resampler/MultinomialResamplerHost.hpp:239-249);
+// slot s = i-1 consumes draw t = n-1-s.  Returns -log(u)/i >= 0.
+__device__ __forceinline__ double multinomial_spacing(const double* u, int s, int n, uint64_t seed, int step) {
+  double uu = multinomial_uniform(u, n - 1 - s, seed, step);
+  return -__ddiv_rn(log(uu), (double)(s + 1));
+}
+
+// ---------------------------------------------------------------------------
+// weight tile sums (+ spacing tile sums for multinomial)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock)
+k_weight_tile_sums(const double* __restrict__ lw, int n, StepStats* st,
+                   u128* tile_sum, u128* tile_prefix,
+                   int with_spacings, const double* u, uint64_t seed, int step,
+                   u128* vtile_sum, u128* vtile_prefix,
+                   unsigned* counter, const int* gate) {
+  if (gate_closed(gate, st)) return;
+  const double mx = st->mx;
+  const int t = blockIdx.x;
+  const int i0 = t * kTile + threadIdx.x * kItems;
+  double v[kItems];
+  load_blocked(lw, i0, n, v);
+  u128 acc = u128_zero(), vacc = u128_zero();
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) {
+    if (i0 + k < n) {
+      double w = nanexp(__dsub_rn(v[k], mx));
+      u128 q; q.lo = weight_to_fixed(w); q.hi = 0;
+      acc = u128_add(acc, q);
+      if (with_spacings) vacc = u128_add(vacc, spacing_to_fixed(multinomial_spacing(u, i0 + k, n, seed, step)));
+    }
+  }
+  u128 tot;
+  block_exclusive_scan_u128(acc, &tot);
+  if (threadIdx.x == 0) tile_sum[t] = tot;
+  if (with_spacings) {
+    u128 vtot;
+    block_exclusive_scan_u128(vacc, &vtot);
+    if (threadIdx.x == 0) vtile_sum[t] = vtot;
+  }
+  if (last_block_arrive(counter)) {
+    block_scan_tiles_u128(tile_sum, tile_prefix, gridDim.x);
+    if (with_spacings) block_scan_tiles_u128(vtile_sum, vtile_prefix, gridDim.x);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      *counter = 0;
+      // SystematicResampler::cumulativeOffspring throws
+      // ParticleFilterDegeneratedException unless W > 0
+      // (share/src/bi/resampler/SystematicResampler.hpp:118-129)
+      double W = u128_to_weight(tile_prefix[gridDim.x]);
+      if (!(W > 0.0)) st->status = BPF_E_DEGENERATE;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// systematic: cumulative offspring and childless counts per tile
+// ---------------------------------------------------------------------------
+// Os_i = min(n, int(Ws_i / W * n + a)): resample_cumulative_offspring,
+// share/src/bi/resampler/SystematicResampler.hpp:47-50, evaluated as three
+// rounded FP64 operations in that order and truncated.
+__device__ __forceinline__ int systematic_Os(double Ws, double W, double nd, double a, int n) {
+  double r = __dadd_rn(__dmul_rn(__ddiv_rn(Ws, W), nd), a);
+  int o = __double2int_rz(r);
+  return o < n ? o : n;
+}
+
+__global__ void __launch_bounds__(kBlock)
+k_systematic_offspring(const double* __restrict__ lw, int n, StepStats* st,
+                       const u128* tile_prefix, const double* a_in, uint64_t seed, int step,
+                       int* Os, int* zcount, int* zprefix, unsigned* counter, const int* gate) {
+  if (gate_closed(gate, st)) return;
+  __shared__ int s_last[kBlock];
+  const double mx = st->mx;
+  const int t = blockIdx.x;
+  const int T = gridDim.x;
+  const int i0 = t * kTile + threadIdx.x * kItems;
+  double a;
+  if (a_in) {
+    a = *a_in;
+  } else {
+    bpf_u32x4 r = bpf_draw(seed, 0u, (uint32_t)step, 0u, BPF_RNG_SYSTEMATIC);
+    a = bpf_u01d(r.v[0], r.v[1]);
+  }
+  const double W = u128_to_weight(tile_prefix[T]);
+  const double nd = (double)n;
+
+  double v[kItems];
+  load_blocked(lw, i0, n, v);
+  unsigned long long q[kItems];
+  u128 loc = u128_zero();
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) {
+    q[k] = (i0 + k < n) ? weight_to_fixed(nanexp(__dsub_rn(v[k], mx))) : 0ull;
+    u128 qq; qq.lo = q[k]; qq.hi = 0;
+    loc = u128_add(loc, qq);
+  }
+  u128 tot;
+  u128 Q = u128_add(tile_prefix[t], block_exclusive_scan_u128(loc, &tot));
+  int os[kItems];
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) {
+    u128 qq; qq.lo = q[k]; qq.hi = 0;
+    Q = u128_add(Q, qq);
+    os[k] = systematic_Os(u128_to_weight(Q), W, nd, a, n);
+  }
+  s_last[threadIdx.x] = os[kItems - 1];
+  __syncthreads();
+  int prev;
+  if (threadIdx.x > 0) {
+    prev = s_last[threadIdx.x - 1];
+  } else {
+    prev = t == 0 ? 0 : systematic_Os(u128_to_weight(tile_prefix[t]), W, nd, a, n);
+  }
+  int zeros = 0;
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) {
+    if (i0 + k < n) {
+      Os[i0 + k] = os[k];
+      zeros += (os[k] == prev);
+    }
+    prev = os[k];
+  }
+  int ztot;
+  block_exclusive_scan_int(zeros, &ztot);
+  if (threadIdx.x == 0) zcount[t] = ztot;
+  if (last_block_arrive(counter)) {
+    block_scan_tiles_int(zcount, zprefix, T);
+    if (threadIdx.x == 0) *counter = 0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// cumulative offspring from offspring counts o[] (Metropolis) or from sorted
+// ancestors (multinomial), with childless counts per tile
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock)
+k_count_tile_sums(const int* __restrict__ o, int n, const StepStats* st, int* icount, int* iprefix,
+                  unsigned* counter, const int* gate) {
+  if (gate_closed(gate, st)) return;
+  const int t = blockIdx.x;
+  const int i0 = t * kTile + threadIdx.x * kItems;
+  int loc = 0;
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) loc += (i0 + k < n) ? o[i0 + k] : 0;
+  int tot;
+  block_exclusive_scan_int(loc, &tot);
+  if (threadIdx.x == 0) icount[t] = tot;
+  if (last_block_arrive(counter)) {
+    block_scan_tiles_int(icount, iprefix, gridDim.x);
+    if (threadIdx.x == 0) *counter = 0;
+  }
+}
+
+// mode 0: o[] are offspring counts, Os = iprefix + inclusive scan
+// mode 1: sorted[] are non-decreasing ancestors, Os_i = upper_bound(sorted, i)
+__global__ void __launch_bounds__(kBlock)
+k_offspring_from(const int* __restrict__ src, int n, int mode, const StepStats* st,
+                 const int* iprefix, int* Os, int* zcount, int* zprefix,
+                 unsigned* counter, const int* gate) {
+  if (gate_closed(gate, st)) return;
+  __shared__ int s_last[kBlock];
+  const int t = blockIdx.x;
+  const int T = gridDim.x;
+  const int i0 = t * kTile + threadIdx.x * kItems;
+  int os[kItems];
+  if (mode == 0) {
+    int v[kItems];
+    int loc = 0;
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) { v[k] = (i0 + k < n) ? src[i0 + k] : 0; loc += v[k]; }
+    int tot;
+    int run = iprefix[t] + block_exclusive_scan_int(loc, &tot);
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) { run += v[k]; os[k] = run; }
+  } else {
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+      int key = i0 + k, lo = 0, hi = n;
+      while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (__ldg(src + mid) <= key) lo = mid + 1; else hi = mid;
+      }
+      os[k] = lo;
+    }
+  }
+  s_last[threadIdx.x] = os[kItems - 1];
+  __syncthreads();
+  int prev;
+  if (threadIdx.x > 0) {
+    prev = s_last[threadIdx.x - 1];
+  } else if (t == 0) {
+    prev = 0;
+  } else if (mode == 0) {
+    prev = iprefix[t];
+  } else {
+    int key = i0 - 1, lo = 0, hi = n;
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      if (__ldg(src + mid) <= key) lo = mid + 1; else hi = mid;
+    }
+    prev = lo;
+  }
+  int zeros = 0;
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) {
+    if (i0 + k < n) {
+      Os[i0 + k] = os[k];
+      zeros += (os[k] == prev);
+    }
+    prev = os[k];
+  }
+  int ztot;
+  block_exclusive_scan_int(zeros, &ztot);
+  if (threadIdx.x == 0) zcount[t] = ztot;
+  if (last_block_arrive(counter)) {
+    block_scan_tiles_int(zcount, zprefix, T);
+    if (threadIdx.x == 0) *counter = 0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// permutation: the rule of ResamplerHost::cumulativeOffspringToAncestorsPermute
+// (share/src/bi/host/resampler/ResamplerHost.hpp:134-168) in closed form.
+//   o_i  = Os_i - Os_{i-1};  Z_i = #{m < i : o_m = 0}  (rank of a childless slot)
+//   E_i  = #{extra copies of ancestors < i} = Os_{i-1} - i + Z_i
+// Particle i with o_i > 0 keeps slot i; childless slot k of rank r receives
+// the ancestor a with E_a <= r < E_{a+1}.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock)
+k_permute_survivors(const int* __restrict__ Os, int n, const int* zprefix, int* as, int* E,
+                    const StepStats* st, const int* gate) {
+  if (gate_closed(gate, st)) return;
+  const int t = blockIdx.x;
+  const int i0 = t * kTile + threadIdx.x * kItems;
+  int prev = i0 > 0 && i0 - 1 < n ? Os[i0 - 1] : 0;
+  int os[kItems];
+  int z[kItems];
+  int loc = 0;
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) {
+    os[k] = (i0 + k < n) ? Os[i0 + k] : prev;
+    z[k] = (i0 + k < n) && (os[k] == (k == 0 ? prev : os[k - 1]));
+    loc += z[k];
+  }
+  int tot;
+  int Z = zprefix[t] + block_exclusive_scan_int(loc, &tot);
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) {
+    int i = i0 + k;
+    int before = (k == 0 ? prev : os[k - 1]);
+    if (i < n) {
+      E[i] = before - i + Z;
+      as[i] = z[k] ? -(Z + 1) : i;
+    }
+    Z += z[k];
+  }
+}
+
+__global__ void __launch_bounds__(kBlock)
+k_permute_fill(int* as, const int* __restrict__ E, int n, const StepStats* st, const int* gate) {
+  if (gate_closed(gate, st)) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    int v = as[i];
+    if (v < 0) {
+      int r = -v - 1, lo = 0, hi = n;
+      while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (__ldg(E + mid) <= r) lo = mid + 1; else hi = mid;
+      }
+      as[i] = lo - 1;
+    }
+  }
+}
+
+// Unpermuted: as_j = i for Os_{i-1} <= j < Os_i, i.e. upper_bound(Os, j)
+// (ResamplerHost::cumulativeOffspringToAncestors, ResamplerHost.hpp:110-131).
+__global__ void __launch_bounds__(kBlock)
+k_ancestors_from_Os(const int* __restrict__ Os, int n, int* as, const StepStats* st, const int* gate) {
+  if (gate_closed(gate, st)) return;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      if (__ldg(Os + mid) <= j) lo = mid + 1; else hi = mid;
+    }
+    as[j] = lo;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// multinomial (sorted draws, Bentley & Saxe 1979), following
+// MultinomialResamplerHost::ancestors (MultinomialResamplerHost.hpp:29-65)
+// with one host thread: slot s gets the number of m with log(Ws_m) <= lu_s,
+// lu_s = log(W) + lMax_s, lMax_s = sum_{i > s} log(u)/i.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock)
+k_multinomial_prepare(const double* __restrict__ lw, int n, StepStats* st,
+                      const u128* tile_prefix, const u128* vtile_prefix,
+                      const double* u, uint64_t seed, int step,
+                      double* Ws, double* lu, const int* gate) {
+  if (gate_closed(gate, st)) return;
+  const double mx = st->mx;
+  const int t = blockIdx.x;
+  const int T = gridDim.x;
+  const int i0 = t * kTile + threadIdx.x * kItems;
+  const double lW = log(u128_to_weight(tile_prefix[T]));
+  const u128 Vtot = vtile_prefix[T];
+  double v[kItems];
+  load_blocked(lw, i0, n, v);
+  unsigned long long q[kItems];
+  u128 vv[kItems];
+  u128 loc = u128_zero(), vloc = u128_zero();
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) {
+    bool in = i0 + k < n;
+    q[k] = in ? weight_to_fixed(nanexp(__dsub_rn(v[k], mx))) : 0ull;
+    vv[k] = in ? spacing_to_fixed(multinomial_spacing(u, i0 + k, n, seed, step)) : u128_zero();
+    u128 qq; qq.lo = q[k]; qq.hi = 0;
+    loc = u128_add(loc, qq);
+    vloc = u128_add(vloc, vv[k]);
+  }
+  u128 tot, vtot;
+  u128 Q = u128_add(tile_prefix[t], block_exclusive_scan_u128(loc, &tot));
+  u128 V = u128_add(vtile_prefix[t], block_exclusive_scan_u128(vloc, &vtot));
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) {
+    u128 qq; qq.lo = q[k]; qq.hi = 0;
+    Q = u128_add(Q, qq);
+    if (i0 + k < n) {
+      Ws[i0 + k] = u128_to_weight(Q);
+      // suffix sum over slots >= s of the spacings, then lu = lW + lMax
+      double lmax = -fixed_to_spacing(u128_sub(Vtot, V));
+      lu[i0 + k] = __dadd_rn(lW, lmax);
+    }
+    V = u128_add(V, vv[k]);
+  }
+}
+
+__global__ void __launch_bounds__(kBlock)
+k_multinomial_search(const double* __restrict__ Ws, const double* __restrict__ lu, int n, int* as,
+                     const StepStats* st, const int* gate) {
+  if (gate_closed(gate, st)) return;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    const double x = lu[s];
+    int lo = 0, hi = n;
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      if (log(__ldg(Ws + mid)) <= x) lo = mid + 1; else hi = mid;
+    }
+    // the reference's loop can leave j = n when lu rounds up to log(W); clamp
+    as[s] = lo < n ? lo : n - 1;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Metropolis, following MetropolisResamplerHost::ancestors
+// (share/src/bi/host/resampler/MetropolisResamplerHost.hpp:290-321): B steps
+// per particle; draw k uses (u_int, u_acc) = uniforms[2(p*B+k)], [2(p*B+k)+1].
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock)
+k_metropolis(const double* __restrict__ lw, int n, int B, const double* u, uint64_t seed, int step,
+             int* as, int* o, const StepStats* st, const int* gate) {
+  if (gate_closed(gate, st)) return;
+  const double nd = (double)n;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    int p1 = p;
+    double lw1 = lw[p];
+    for (int k = 0; k < B; ++k) {
+      double ui, ua;
+      if (u) {
+        size_t idx = 2 * ((size_t)p * B + k);
+        ui = u[idx];
+        ua = u[idx + 1];
+      } else {
+        bpf_u32x4 r = bpf_draw(seed, (uint32_t)p, (uint32_t)step, (uint32_t)k, BPF_RNG_METROPOLIS);
+        ui = bpf_u01d(r.v[0], r.v[1]);
+        ua = bpf_u01d(r.v[2], r.v[3]);
+      }
+      int p2 = __double2int_rz(__dmul_rn(ui, nd));
+      p2 = p2 < n - 1 ? p2 : n - 1;
+      double lw2 = __ldg(lw + p2);
+      if (log(ua) < __dsub_rn(lw2, lw1)) {
+        p1 = p2;
+        lw1 = lw2;
+      }
+    }
+    as[p] = p1;
+    if (o) atomicAdd(o + p1, 1);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// gather_rows, out of place: Y[j*ld + i] = X[j*ld + as[i]]
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(kBlock)
+k_gather(const int* __restrict__ as, const T* __restrict__ X, T* __restrict__ Y, int n, int d, int ld,
+         const int* gate) {
+  if (gate != nullptr && *gate == 0) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int a = as[i];
+  for (int j = 0; j < d; ++j) Y[(size_t)j * ld + i] = __ldg(X + (size_t)j * ld + a);
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+int scratch_alloc(ResampleScratch& s, int max_n) {
+  s.max_n = max_n;
+  s.max_tiles = ntiles(max_n);
+  const size_t T1 = (size_t)s.max_tiles + 1;
+  const size_t N = (size_t)max_n;
+  s.max_partials = (max_n + 127) / 128 + 1;
+#define ALLOC(ptr, bytes) \
+  if (cudaMalloc((void**)&(ptr), (bytes)) != cudaSuccess) { scratch_free(s); return BPF_E_NOMEM; }
+  ALLOC(s.tile_sum, T1 * sizeof(u128));
+  ALLOC(s.tile_prefix, T1 * sizeof(u128));
+  ALLOC(s.vtile_sum, T1 * sizeof(u128));
+  ALLOC(s.vtile_prefix, T1 * sizeof(u128));
+  ALLOC(s.zcount, T1 * sizeof(int));
+  ALLOC(s.zprefix, T1 * sizeof(int));
+  ALLOC(s.icount, T1 * sizeof(int));
+  ALLOC(s.iprefix, T1 * sizeof(int));
+  ALLOC(s.Os, N * sizeof(int));
+  ALLOC(s.E, N * sizeof(int));
+  ALLOC(s.o, N * sizeof(int));
+  ALLOC(s.Ws, N * sizeof(double));
+  ALLOC(s.lu, N * sizeof(double));
+  ALLOC(s.counters, 16 * sizeof(unsigned));
+  ALLOC(s.stats, sizeof(StepStats));
+  ALLOC(s.partials, (size_t)s.max_partials * sizeof(LwPartial));
+#undef ALLOC
+  if (cudaMemset(s.counters, 0, 16 * sizeof(unsigned)) != cudaSuccess) { scratch_free(s); return BPF_E_CUDA; }
+  StepStats z{};
+  z.status = BPF_OK;
+  if (cudaMemcpy(s.stats, &z, sizeof(z), cudaMemcpyHostToDevice) != cudaSuccess) { scratch_free(s); return BPF_E_CUDA; }
+  return BPF_OK;
+}
+
+void scratch_free(ResampleScratch& s) {
+  void* ptrs[] = {s.tile_sum, s.tile_prefix, s.vtile_sum, s.vtile_prefix, s.zcount, s.zprefix,
+                  s.icount, s.iprefix, s.Os, s.E, s.o, s.Ws, s.lu, s.counters, s.stats, s.partials};
+  for (void* p : ptrs) if (p) cudaFree(p);
+  s = ResampleScratch();
+}
+
+static inline int grid_stride_blocks(int n) {
+  int b = (n + kBlock - 1) / kBlock;
+  return b < 148 * 8 ? (b > 0 ? b : 1) : 148 * 8;
+}
+
+int launch_resample(const ResampleArgs& a, ResampleScratch& s, cudaStream_t st) {
+  if (a.n <= 0 || a.n > s.max_n || a.as == nullptr) return BPF_E_INVALID;
+  const int n = a.n;
+  const int T = ntiles(n);
+  int* Os = a.Os_out ? a.Os_out : s.Os;
+  unsigned* c = s.counters;
+  if (!a.max_known && a.kind != BPF_RESAMPLER_METROPOLIS) {
+    int rc = launch_lw_reduce(a.lw, n, s, st);
+    if (rc) return rc;
+  }
+  switch (a.kind) {
+    case BPF_RESAMPLER_SYSTEMATIC: {
+      k_weight_tile_sums<<<T, kBlock, 0, st>>>(a.lw, n, s.stats, s.tile_sum, s.tile_prefix, 0, nullptr,
+                                               a.seed, a.step, nullptr, nullptr, c + 0, a.gate);
+      k_systematic_offspring<<<T, kBlock, 0, st>>>(a.lw, n, s.stats, s.tile_prefix, a.uniforms, a.seed,
+                                                   a.step, Os, s.zcount, s.zprefix, c + 1, a.gate);
+      if (a.permute) {
+        k_permute_survivors<<<T, kBlock, 0, st>>>(Os, n, s.zprefix, a.as, s.E, s.stats, a.gate);
+        k_permute_fill<<<grid_stride_blocks(n), kBlock, 0, st>>>(a.as, s.E, n, s.stats, a.gate);
+      } else {
+        k_ancestors_from_Os<<<grid_stride_blocks(n), kBlock, 0, st>>>(Os, n, a.as, s.stats, a.gate);
+      }
+      break;
+    }
+    case BPF_RESAMPLER_MULTINOMIAL: {
+      k_weight_tile_sums<<<T, kBlock, 0, st>>>(a.lw, n, s.stats, s.tile_sum, s.tile_prefix, 1, a.uniforms,
+                                               a.seed, a.step, s.vtile_sum, s.vtile_prefix, c + 0, a.gate);
+      k_multinomial_prepare<<<T, kBlock, 0, st>>>(a.lw, n, s.stats, s.tile_prefix, s.vtile_prefix,
+                                                  a.uniforms, a.seed, a.step, s.Ws, s.lu, a.gate);
+      k_multinomial_search<<<grid_stride_blocks(n), kBlock, 0, st>>>(s.Ws, s.lu, n, a.as, s.stats, a.gate);
+      if (a.permute || a.Os_out) {
+        k_offspring_from<<<T, kBlock, 0, st>>>(a.as, n, 1, s.stats, nullptr, Os, s.zcount, s.zprefix, c + 1,
+                                               a.gate);
+      }
+      if (a.permute) {
+        k_permute_survivors<<<T, kBlock, 0, st>>>(Os, n, s.zprefix, a.as, s.E, s.stats, a.gate);
+        k_permute_fill<<<grid_stride_blocks(n), kBlock, 0, st>>>(a.as, s.E, n, s.stats, a.gate);
+      }
+      break;
+    }
+    case BPF_RESAMPLER_METROPOLIS: {
+      const bool need_counts = a.permute || a.Os_out;
+      if (need_counts) BPF_TRY(cudaMemsetAsync(s.o, 0, (size_t)n * sizeof(int), st));
+      k_metropolis<<<grid_stride_blocks(n), kBlock, 0, st>>>(a.lw, n, a.B, a.uniforms, a.seed, a.step, a.as,
+                                                            need_counts ? s.o : nullptr, s.stats, a.gate);
+      if (need_counts) {
+        k_count_tile_sums<<<T, kBlock, 0, st>>>(s.o, n, s.stats, s.icount, s.iprefix, c + 2, a.gate);
+        k_offspring_from<<<T, kBlock, 0, st>>>(s.o, n, 0, s.stats, s.iprefix, Os, s.zcount, s.zprefix, c + 1,
+                                               a.gate);
+      }
+      if (a.permute) {
+        k_permute_survivors<<<T, kBlock, 0, st>>>(Os, n, s.zprefix, a.as, s.E, s.stats, a.gate);
+        k_permute_fill<<<grid_stride_blocks(n), kBlock, 0, st>>>(a.as, s.E, n, s.stats, a.gate);
+      }
+      break;
+    }
+    default:
+      return BPF_E_INVALID;
+  }
+  BPF_TRY(cudaGetLastError());
+  return BPF_OK;
+}
+
+int launch_gather(const int* as, const void* X, void* Y, int n, int d, int ld, int esz, const int* gate,
+                  cudaStream_t st) {
+  if (n <= 0 || d <= 0 || ld < n) return BPF_E_INVALID;
+  const int g = (n + kBlock - 1) / kBlock;
+  if (esz == 4) {
+    k_gather<float><<<g, kBlock, 0, st>>>(as, (const float*)X, (float*)Y, n, d, ld, gate);
+  } else if (esz == 8) {
+    k_gather<double><<<g, kBlock, 0, st>>>(as, (const double*)X, (double*)Y, n, d, ld, gate);
+  } else {
+    return BPF_E_INVALID;
+  }
+  BPF_TRY(cudaGetLastError());
+  return BPF_OK;
+}
+
+}  // namespace bpf

@@ -1,0 +1,348 @@
+"""Host-side mirror of LibBi's bootstrap particle filter API, over the C ABI.
+
+Names follow the reference's classes so that calling code reads like it:
+
+    reference (share/src/bi/...)                 here
+    Model<L96>, Model<PZ> (generated)            ModelL96, ModelPZ
+    Resampler<SystematicResampler> etc.          SystematicResampler, MultinomialResampler,
+                                                 MetropolisResampler
+    Resampler::reduce / ancestors[Permute]       Resampler.reduce / .ancestors / .ancestors_permute
+    logsumexp_reduce, gather_rows                Resampler.logsumexp, gather_rows
+    BootstrapPF::step / correct / term           BootstrapPF.step / .filter
+    Filter<BootstrapPF>::filter                  BootstrapPF.filter
+    BootstrapPFState (lws, as, ess, LL)          BootstrapPF.state(), .ess, .log_likelihood
+
+Device memory is passed as torch CUDA tensors (torch is the plumbing for
+device memory and streams); all compute runs in the CUDA kernels of the
+shared library.  Errors raise BpfError, and a degenerate resample raises
+ParticleFilterDegeneratedException as the reference does.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _native as N
+
+
+# ---------------------------------------------------------------------------
+# device views of raw pointers
+# ---------------------------------------------------------------------------
+class _DeviceArray:
+    def __init__(self, ptr: int, shape, typestr: str, strides=None):
+        self.__cuda_array_interface__ = {
+            "shape": tuple(shape), "typestr": typestr, "data": (int(ptr), False),
+            "version": 3, "strides": strides,
+        }
+
+
+def _view(ptr: int, shape, dtype: str):
+    import torch
+
+    typestr = {"f4": "<f4", "f8": "<f8", "i4": "<i4"}[dtype]
+    return torch.as_tensor(_DeviceArray(ptr, shape, typestr), device="cuda")
+
+
+def _ptr(t) -> Optional[int]:
+    if t is None:
+        return None
+    if not t.is_cuda or not t.is_contiguous():
+        raise ValueError("expected a contiguous CUDA tensor")
+    return t.data_ptr()
+
+
+# ---------------------------------------------------------------------------
+# models
+# ---------------------------------------------------------------------------
+@dataclass
+class ModelL96:
+    """Lorenz '96 with additive noise: transition(delta) { eta ~ N(0, sigma_eta);
+    ode(RK4, h) { dx[i]/dt = (x[i+1]-x[i-2])*x[i-1] - x[i] + F }; x <- x + eta },
+    observation { y[i] ~ N(x[i], sigma_y) }, initial { x[i] ~ N(x0_mean, x0_std) }."""
+
+    dim: int = 40
+    F: float = 8.0
+    sigma_eta: float = 0.1
+    sigma_y: float = 1.0
+    h: float = 0.01
+    x0_mean: Optional[float] = None
+    x0_std: float = 0.01
+    precision: str = "f32"
+
+    @property
+    def nobs(self) -> int:
+        return self.dim
+
+    @property
+    def np_dtype(self):
+        return np.float32 if self.precision == "f32" else np.float64
+
+    def desc(self) -> N.ModelDesc:
+        d = N.ModelDesc()
+        d.kind = N.BPF_MODEL_L96
+        d.dim = self.dim
+        d.precision = N.BPF_F32 if self.precision == "f32" else N.BPF_F64
+        d.integrator = N.BPF_ODE_RK4
+        d.h = self.h
+        th = [self.F, self.sigma_eta, self.sigma_y, self.F if self.x0_mean is None else self.x0_mean, self.x0_std]
+        for i, v in enumerate(th):
+            d.theta[i] = v
+        return d
+
+
+@dataclass
+class ModelPZ:
+    """Phytoplankton-zooplankton: transition(delta) { alpha ~ log_normal(mu, sigma);
+    ode(RK4(3), h0, atoler, rtoler) { dP/dt = alpha P - c P Z; dZ/dt = e c P Z - m Z - q Z^2 } },
+    observation { y ~ N(log P, sigma_y) }, initial { P, Z ~ log_normal }."""
+
+    c: float = 0.25
+    e: float = 0.3
+    m: float = 0.1
+    q: float = 0.1
+    mu: float = math.log(0.3)
+    sigma: float = 0.2
+    sigma_y: float = 0.2
+    p0_mu: float = math.log(2.0)
+    p0_sigma: float = 0.2
+    z0_mu: float = math.log(2.0)
+    z0_sigma: float = 0.2
+    h: float = 0.1
+    atoler: float = 1e-3
+    rtoler: float = 1e-3
+    precision: str = "f64"
+    dim: int = 2
+
+    @property
+    def nobs(self) -> int:
+        return 1
+
+    @property
+    def np_dtype(self):
+        return np.float64
+
+    def desc(self) -> N.ModelDesc:
+        d = N.ModelDesc()
+        d.kind = N.BPF_MODEL_PZ
+        d.dim = 2
+        d.precision = N.BPF_F64
+        d.integrator = N.BPF_ODE_RK43
+        d.h, d.atoler, d.rtoler = self.h, self.atoler, self.rtoler
+        th = [self.c, self.e, self.m, self.q, self.mu, self.sigma, self.sigma_y,
+              self.p0_mu, self.p0_sigma, self.z0_mu, self.z0_sigma]
+        for i, v in enumerate(th):
+            d.theta[i] = v
+        return d
+
+
+# ---------------------------------------------------------------------------
+# resamplers
+# ---------------------------------------------------------------------------
+class Resampler:
+    """Resampler<R> (share/src/bi/resampler/Resampler.hpp:33-117) on device
+    log-weights (FP64 torch CUDA tensors)."""
+
+    kind = N.BPF_RESAMPLER_SYSTEMATIC
+
+    def __init__(self, ess_rel: float = 0.5, max_n: int = 1 << 20, B: int = 0, stream=None):
+        if not (0.0 <= ess_rel <= 1.0):
+            raise ValueError("essRel must lie in [0, 1]")
+        self.ess_rel = ess_rel
+        self.B = B
+        self.max_n = max_n
+        self._h = ctypes.c_void_p()
+        N.check(N.lib().bpf_resampler_create(self.kind, max_n, B, stream, ctypes.byref(self._h)),
+                "bpf_resampler_create")
+
+    def close(self):
+        if self._h:
+            N.load_library().bpf_resampler_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def reduce(self, lws):
+        """ESS and lW = log mean exp(lws): Resampler::reduce -> ess_reduce."""
+        lW, ess = ctypes.c_double(), ctypes.c_double()
+        N.check(N.lib().bpf_ess_reduce(self._h, _ptr(lws), lws.numel(), ctypes.byref(lW), ctypes.byref(ess)),
+                "bpf_ess_reduce")
+        return ess.value, lW.value
+
+    def logsumexp(self, lws) -> float:
+        out = ctypes.c_double()
+        N.check(N.lib().bpf_logsumexp_reduce(self._h, _ptr(lws), lws.numel(), ctypes.byref(out)),
+                "bpf_logsumexp_reduce")
+        return out.value
+
+    def ancestors(self, lws, uniforms=None, permute: bool = False, with_offspring: bool = False):
+        import torch
+
+        n = lws.numel()
+        a = torch.empty(n, dtype=torch.int32, device=lws.device)
+        Os = torch.empty(n, dtype=torch.int32, device=lws.device) if with_offspring else None
+        N.check(N.lib().bpf_resampler_ancestors(self._h, _ptr(lws), n, _ptr(uniforms), int(permute), _ptr(a),
+                                                _ptr(Os)), "bpf_resampler_ancestors")
+        return (a, Os) if with_offspring else a
+
+    def ancestors_permute(self, lws, uniforms=None):
+        return self.ancestors(lws, uniforms, permute=True)
+
+
+class SystematicResampler(Resampler):
+    kind = N.BPF_RESAMPLER_SYSTEMATIC
+
+
+class MultinomialResampler(Resampler):
+    kind = N.BPF_RESAMPLER_MULTINOMIAL
+
+
+class MetropolisResampler(Resampler):
+    kind = N.BPF_RESAMPLER_METROPOLIS
+
+
+RESAMPLERS = {"systematic": N.BPF_RESAMPLER_SYSTEMATIC, "multinomial": N.BPF_RESAMPLER_MULTINOMIAL,
+              "metropolis": N.BPF_RESAMPLER_METROPOLIS}
+
+
+def gather_rows(as_, X, Y, d: int, ld: int, stream=None):
+    """Y[j*ld + i] = X[j*ld + as[i]] (gather_rows, out of place)."""
+    n = as_.numel()
+    N.check(N.lib().bpf_gather_rows(_ptr(as_), _ptr(X), _ptr(Y), n, d, ld, X.element_size(), stream),
+            "bpf_gather_rows")
+
+
+# ---------------------------------------------------------------------------
+# filter
+# ---------------------------------------------------------------------------
+@dataclass
+class StepResult:
+    ess: float
+    log_weight_sum: float
+    log_increment: float
+    log_likelihood: float
+    resampled: bool
+
+
+class BootstrapPF:
+    """BootstrapPF<B,F,O,R> + BootstrapPFState for one model on one GPU."""
+
+    def __init__(self, model, nparticles: int, resampler: str = "systematic", ess_rel: float = 0.5,
+                 seed: int = 0, metropolis_steps: int = 0, stream=None):
+        self.model = model
+        self.n = nparticles
+        cfg = N.Config()
+        cfg.nparticles = nparticles
+        cfg.resampler = RESAMPLERS[resampler]
+        cfg.metropolis_steps = metropolis_steps
+        cfg.ess_rel = ess_rel
+        cfg.seed = seed
+        cfg.stream = stream
+        self._desc = model.desc()
+        self._cfg = cfg
+        self._h = ctypes.c_void_p()
+        N.check(N.lib().bpf_create(ctypes.byref(self._desc), ctypes.byref(cfg), ctypes.byref(self._h)), "bpf_create")
+
+    def close(self):
+        if self._h:
+            N.load_library().bpf_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def init(self):
+        N.check(N.lib().bpf_init(self._h), "bpf_init")
+
+    def _y_host(self, y):
+        if y is None:
+            return None, None
+        arr = np.ascontiguousarray(np.asarray(y, dtype=self.model.np_dtype).reshape(-1))
+        if arr.size != self.model.nobs:
+            raise ValueError(f"expected {self.model.nobs} observations")
+        return arr, arr.ctypes.data_as(ctypes.c_void_p)
+
+    def step(self, t1: float, t2: float, y=None) -> StepResult:
+        """One BootstrapPF::step to the observation y at t2 (host values)."""
+        arr, p = self._y_host(y)
+        out = N.StepOut()
+        N.check(N.lib().bpf_step(self._h, t1, t2, p, ctypes.byref(out)), "bpf_step")
+        return StepResult(out.ess, out.log_weight_sum, out.log_increment, out.log_likelihood, bool(out.resampled))
+
+    def step_device(self, t1: float, t2: float, y_dev=None, sync: bool = True) -> Optional[StepResult]:
+        """BootstrapPF::step with the observation already on the device."""
+        if not sync:
+            N.check(N.lib().bpf_step_device(self._h, t1, t2, _ptr(y_dev), None), "bpf_step_device")
+            return None
+        out = N.StepOut()
+        N.check(N.lib().bpf_step_device(self._h, t1, t2, _ptr(y_dev), ctypes.byref(out)), "bpf_step_device")
+        return StepResult(out.ess, out.log_weight_sum, out.log_increment, out.log_likelihood, bool(out.resampled))
+
+    def filter(self, y, t0: float = 0.0, dt: float = 1.0):
+        """Filter<BootstrapPF>::filter over T observations; returns
+        (logLikelihood, logIncrements[T], ess[T])."""
+        arr = np.ascontiguousarray(np.asarray(y, dtype=self.model.np_dtype).reshape(-1))
+        T = arr.size // self.model.nobs
+        inc = np.zeros(T)
+        ess = np.zeros(T)
+        ll = ctypes.c_double()
+        N.check(N.lib().bpf_filter(self._h, T, t0, dt, arr.ctypes.data_as(ctypes.c_void_p),
+                                   inc.ctypes.data_as(ctypes.c_void_p), ess.ctypes.data_as(ctypes.c_void_p),
+                                   ctypes.byref(ll)), "bpf_filter")
+        return ll.value, inc, ess
+
+    def reduce(self):
+        lW, ess = ctypes.c_double(), ctypes.c_double()
+        N.check(N.lib().bpf_reduce(self._h, ctypes.byref(lW), ctypes.byref(ess)), "bpf_reduce")
+        return ess.value, lW.value
+
+    def resample(self, uniforms=None):
+        import torch
+
+        out = torch.empty(self.n, dtype=torch.int32, device="cuda")
+        N.check(N.lib().bpf_resample(self._h, _ptr(uniforms), _ptr(out)), "bpf_resample")
+        return out
+
+    def state(self):
+        """Device views (x[dim, ld], lws[n], as[n]) of the particle store."""
+        x, lw, as_, ld = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_int()
+        N.check(N.lib().bpf_state_ptrs(self._h, ctypes.byref(x), ctypes.byref(lw), ctypes.byref(as_),
+                                       ctypes.byref(ld)), "bpf_state_ptrs")
+        dt = "f4" if self.model.precision == "f32" else "f8"
+        return (_view(x.value, (self.model.dim, ld.value), dt), _view(lw.value, (self.n,), "f8"),
+                _view(as_.value, (self.n,), "i4"))
+
+    def timing(self, enable: bool = True):
+        N.check(N.lib().bpf_timing_enable(self._h, int(enable)), "bpf_timing_enable")
+
+    def timing_read(self, reset: bool = True):
+        """(resample_ms, transition_ms, steps) summed since the last reset."""
+        r, t, k = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        N.check(N.lib().bpf_timing_read(self._h, int(reset), ctypes.byref(r), ctypes.byref(t), ctypes.byref(k)),
+                "bpf_timing_read")
+        return r.value, t.value, k.value
+
+    def snapshot(self) -> bytes:
+        size = ctypes.c_uint64()
+        N.check(N.lib().bpf_snapshot_size(self._h, ctypes.byref(size)), "bpf_snapshot_size")
+        buf = ctypes.create_string_buffer(size.value)
+        N.check(N.lib().bpf_snapshot(self._h, buf, size.value), "bpf_snapshot")
+        return buf.raw
+
+    def restore(self, blob: bytes):
+        buf = ctypes.create_string_buffer(blob, len(blob))
+        N.check(N.lib().bpf_restore(self._h, buf, len(blob)), "bpf_restore")

@@ -1,0 +1,10 @@
+// Oracle test infrastructure: declared only so the reference headers compile;
+// the oracle never draws from this distribution.
+#pragma once
+#include <stdexcept>
+namespace boost {
+template<class A = double, class B = double> struct binomial_distribution {
+  template<class... X> binomial_distribution(X...) {}
+  template<class E> A operator()(E&) const { throw std::runtime_error("binomial_distribution not on the oracle path"); }
+};
+}
