@@ -68,7 +68,7 @@ enum { BPF_F32 = 0, BPF_F64 = 1 };
 
 typedef struct {
   int kind;        /* BPF_MODEL_* */
-  int dim;         /* state components: d for L96 (1..64), 2 for PZ */
+  int dim;         /* state components: d for L96 (4, 8, 16, 32 or 40), 2 for PZ */
   int precision;   /* BPF_F32 or BPF_F64: state, ODE and log-density arithmetic
                       (L96: either; PZ: BPF_F64) */
   int integrator;  /* BPF_ODE_RK4 or BPF_ODE_RK43 (ode block 'alg') */

@@ -53,7 +53,7 @@ int check_model(const bpf_model_desc* m) {
   if (m->precision != BPF_F32 && m->precision != BPF_F64) return BPF_E_INVALID;
   if (m->kind == BPF_MODEL_L96) {
     if (m->integrator != BPF_ODE_RK4) return BPF_E_INVALID;
-    const int ok_dims[] = {4, 8, 16, 32, 40, 64};
+    const int ok_dims[] = {4, 8, 16, 32, 40};
     bool ok = false;
     for (int d : ok_dims) ok |= (m->dim == d);
     if (!ok) return BPF_E_INVALID;
@@ -140,6 +140,7 @@ int enqueue_step(bpf_handle* h, double t1, double t2, const void* y_dev) {
   ta.step = k;
   ta.stats = h->rs.stats;
   ta.partials = h->rs.partials;
+  ta.max_partials = h->rs.max_partials;
   ta.counter = h->rs.counters + 4;
   rc = bpf::launch_transition(h->model, ta, h->stream);
   if (rc) return rc;

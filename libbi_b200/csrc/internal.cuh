@@ -16,9 +16,10 @@ void bpf_set_last_cuda_error(cudaError_t e);
 
 namespace bpf {
 
-// Resampler tile: 256 threads x 8 items.
+// Resampler tile: 256 threads x 2 items (512 log-weights), so that the
+// N = 65536 workload spreads over 128 blocks.
 constexpr int kBlock = 256;
-constexpr int kItems = 8;
+constexpr int kItems = 2;
 constexpr int kTile = kBlock * kItems;
 
 inline int ntiles(int n) { return (n + kTile - 1) / kTile; }
@@ -198,6 +199,8 @@ struct ResampleScratch {
   int* iprefix = nullptr;
   int* Os = nullptr;            // cumulative offspring
   int* E = nullptr;             // cumulative extra copies
+  int* slot = nullptr;          // childless slot of each rank
+  int* etile = nullptr;         // every 2^k-th value of E (coarse search index)
   int* o = nullptr;             // offspring counts (Metropolis)
   double* Ws = nullptr;         // FP64 cumulative weights (multinomial search)
   double* lu = nullptr;         // log sorted uniforms (multinomial)
@@ -256,6 +259,7 @@ struct TransitionArgs {
   int step;
   StepStats* stats;   // reads resample flag / ll; finalised by the last block
   LwPartial* partials;
+  int max_partials;   // capacity of partials (one per block)
   unsigned* counter;
 };
 int launch_transition(const ModelArgs& m, const TransitionArgs& a, cudaStream_t st);

@@ -75,18 +75,26 @@ __device__ __forceinline__ void l96_dfdt(const T (&x)[D], T (&k)[D], T F) {
   }
 }
 
+// Blocks of 64 threads, at most 128 registers each: 8 blocks fit an SM, so
+// N = 65536 particles (1024 blocks) run as a single wave on 148 SMs with 6 or
+// 7 blocks on every SM.
+constexpr int kL96Block = 64;
+
 template <class T, int D>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(kL96Block, (sizeof(T) == 4 && D <= 40 ? 8 : 4))
 k_l96_transition(const T* __restrict__ x_in, T* __restrict__ x_out, int ld, int n,
                  int* __restrict__ as, double* __restrict__ lw, const T* __restrict__ y,
                  double t1d, double t2d, uint64_t seed, int step, L96Params prm,
                  StepStats* st, LwPartial* partials, unsigned* counter) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  // state staged here for the rolled noise/observation epilogue
+  __shared__ T sx[D][kL96Block];
+  const int p = blockIdx.x * kL96Block + threadIdx.x;
   const int resampled = st->resample;
   const bool ok = st->status == BPF_OK;
   const T F = (T)prm.F, h0 = (T)prm.h;
+  const double ll = st->ll;
   LwPartial part = lw_empty();
-  if (p < n && ok) {
+  if (ok && p < n) {
     const int src = resampled ? as[p] : p;
     T x0[D];
 #pragma unroll
@@ -119,14 +127,17 @@ k_l96_transition(const T* __restrict__ x_in, T* __restrict__ x_out, int ld, int 
       for (int i = 0; i < D; ++i) { acc[i] = Prec<T>::fma_(b4, k[i], acc[i]); x0[i] = Prec<T>::fma_(h, acc[i], x0[i]); }
       t += h;
     }
+#pragma unroll
+    for (int i = 0; i < D; ++i) sx[i][threadIdx.x] = x0[i];
 
     // eta[i] ~ gaussian(0, sigma_eta); x[i] <- x[i] + eta[i]; then
-    // lp += -0.5*((y - x)/sigma)^2 - BI_HALF_LOG_TWO_PI - log(sigma)
+    // lp += -0.5*((y - x)/sigma)^2 - BI_HALF_LOG_TWO_PI - log(sigma),
+    // four components per Philox block, in component order
     const T se = (T)prm.sigma_eta;
     const T sy = (T)prm.sigma_y, isy = (T)prm.inv_sigma_y;
     const T c2 = (T)prm.c_half_log_2pi, ls = (T)prm.log_sigma_y;
-    double l = resampled ? st->ll : lw[p];
-#pragma unroll
+    double l = resampled ? ll : lw[p];
+#pragma unroll 1
     for (int b = 0; b < (D + 3) / 4; ++b) {
       bpf_u32x4 r = bpf_draw(seed, (uint32_t)p, (uint32_t)step, (uint32_t)b, BPF_RNG_NOISE);
       T z[4];
@@ -136,9 +147,10 @@ k_l96_transition(const T* __restrict__ x_in, T* __restrict__ x_out, int ld, int 
       for (int j = 0; j < 4; ++j) {
         const int i = 4 * b + j;
         if (i < D) {
-          x0[i] = Prec<T>::add_(x0[i], Prec<T>::mul_(se, z[j]));
+          const T xi = Prec<T>::add_(sx[i][threadIdx.x], Prec<T>::mul_(se, z[j]));
+          x_out[(size_t)i * ld + p] = xi;
           if (y) {
-            T dz = __ldg(y + i) - x0[i];
+            T dz = __ldg(y + i) - xi;
             dz = isy != (T)0 ? dz * isy : dz / sy;
             T term = Prec<T>::fma_((T)-0.5, dz * dz, -c2) - ls;
             l += (double)term;
@@ -146,8 +158,6 @@ k_l96_transition(const T* __restrict__ x_in, T* __restrict__ x_out, int ld, int 
         }
       }
     }
-#pragma unroll
-    for (int i = 0; i < D; ++i) x_out[(size_t)i * ld + p] = x0[i];
     lw[p] = l;
     if (resampled) as[p] = src;
     lw_push(part, l);
@@ -407,14 +417,16 @@ static PZParams pz_params(const ModelArgs& m) {
 
 #define L96_CASE(DD)                                                                                   \
   case DD:                                                                                             \
-    k_l96_transition<T, DD><<<blocks, 128, 0, st>>>((const T*)a.x_in, (T*)a.x_out, a.ld, a.n,          \
+    k_l96_transition<T, DD><<<blocks, kL96Block, 0, st>>>((const T*)a.x_in, (T*)a.x_out, a.ld, a.n,          \
         (int*)a.as, a.lw, (const T*)a.y, a.t1, a.t2, a.seed, a.step, prm, a.stats, a.partials, a.counter); \
     break;
 
 template <class T>
 static int transition_t(const ModelArgs& m, const TransitionArgs& a, cudaStream_t st) {
-  const int blocks = (a.n + 127) / 128;
   if (m.kind == BPF_MODEL_L96) {
+    // one particle per thread: 64-thread blocks spread evenly over the SMs
+    const int blocks = (a.n + kL96Block - 1) / kL96Block;
+    if (blocks > a.max_partials) return BPF_E_INVALID;
     L96Params prm = l96_params<T>(m);
     switch (m.dim) {
       L96_CASE(4)
@@ -422,11 +434,12 @@ static int transition_t(const ModelArgs& m, const TransitionArgs& a, cudaStream_
       L96_CASE(16)
       L96_CASE(32)
       L96_CASE(40)
-      L96_CASE(64)
       default:
         return BPF_E_INVALID;
     }
   } else if (m.kind == BPF_MODEL_PZ) {
+    const int blocks = (a.n + 127) / 128;
+    if (blocks > a.max_partials) return BPF_E_INVALID;
     PZParams prm = pz_params<T>(m);
     k_pz_transition<T><<<blocks, 128, 0, st>>>((const T*)a.x_in, (T*)a.x_out, a.ld, a.n, (int*)a.as, a.lw,
                                                (const T*)a.y, a.t1, a.t2, a.seed, a.step, prm, a.stats,

@@ -4,28 +4,15 @@
 // (share/src/bi/primitive/vector_primitive.hpp:933-974), which make two
 // Thrust passes (max_element with nan_less_functor, then a transform_reduce of
 // (e, e^2) with e = nanexp(lw - max)) and return scalars to the host.  Here
-// each thread keeps an online (max, sum e, sum e^2) in FP64, blocks combine
-// them with warp shuffles, and the last block to finish combines the block
-// partials in a fixed order, so the result is deterministic and stays on the
+// each thread keeps an online (max, sum e, sum e^2) in FP64; a block takes the
+// maximum of its threads' maxima, rescales each thread's sums with one exp and
+// adds them; the last block to finish combines the block partials the same
+// way in a fixed order, so the result is deterministic and stays on the
 // device.
 #pragma once
 #include "internal.cuh"
 
 namespace bpf {
-
-__device__ __forceinline__ LwPartial lw_combine(LwPartial a, LwPartial b) {
-  LwPartial r;
-  r.mx = nan_max(a.mx, b.mx);
-  if (isinf(r.mx)) {  // both empty / all -inf, or a +inf log-weight
-    r.s1 = 0.0; r.s2 = 0.0;
-    return r;
-  }
-  double fa = a.s1 == 0.0 ? 0.0 : exp(a.mx - r.mx);
-  double fb = b.s1 == 0.0 ? 0.0 : exp(b.mx - r.mx);
-  r.s1 = a.s1 * fa + b.s1 * fb;
-  r.s2 = a.s2 * fa * fa + b.s2 * fb * fb;
-  return r;
-}
 
 __device__ __forceinline__ LwPartial lw_empty() {
   LwPartial r; r.mx = -INFINITY; r.s1 = 0.0; r.s2 = 0.0; return r;
@@ -53,32 +40,45 @@ __device__ __forceinline__ void lw_push(LwPartial& a, double x) {
   }
 }
 
-__device__ __forceinline__ LwPartial warp_combine(LwPartial v) {
+__device__ __forceinline__ double warp_max(double v) {
 #pragma unroll
-  for (int d = 16; d > 0; d >>= 1) {
-    LwPartial o;
-    o.mx = __shfl_down_sync(0xffffffffu, v.mx, d);
-    o.s1 = __shfl_down_sync(0xffffffffu, v.s1, d);
-    o.s2 = __shfl_down_sync(0xffffffffu, v.s2, d);
-    v = lw_combine(v, o);
-  }
+  for (int d = 16; d > 0; d >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, d));
   return v;
 }
 
-// Combine one partial per thread across the block; result valid in thread 0.
-__device__ __forceinline__ LwPartial block_combine(LwPartial v) {
-  __shared__ LwPartial wp[32];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int nw = (blockDim.x + 31) >> 5;
-  v = warp_combine(v);
-  if (lane == 0) wp[warp] = v;
-  __syncthreads();
-  if (warp == 0) {
-    v = lane < nw ? wp[lane] : lw_empty();
-    v = warp_combine(v);
-  }
-  __syncthreads();
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
   return v;
+}
+
+// Combine one partial per thread across the block (blockDim.x a multiple of
+// 32, at most 1024); the result is valid in every thread.  Max first, then one
+// rescaling exp per partial and plain sums, so the critical path holds a
+// single exp.
+__device__ __forceinline__ LwPartial block_combine(LwPartial v) {
+  __shared__ double s_m[32], s_1[32], s_2[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
+  double m = warp_max(v.mx);  // partial maxima are never NaN
+  if (lane == 0) s_m[warp] = m;
+  __syncthreads();
+  double M = lane < nw ? s_m[lane] : -INFINITY;
+  M = warp_max(M);
+  // empty partials (s1 == 0) contribute nothing, also when M is infinite
+  const double f = v.s1 == 0.0 ? 0.0 : exp(v.mx - M);
+  double a = warp_sum(v.s1 * f), b = warp_sum(v.s2 * f * f);
+  if (lane == 0) { s_1[warp] = a; s_2[warp] = b; }
+  __syncthreads();
+  a = lane < nw ? s_1[lane] : 0.0;
+  b = lane < nw ? s_2[lane] : 0.0;
+  LwPartial r;
+  r.mx = M;
+  r.s1 = warp_sum(a);
+  r.s2 = warp_sum(b);
+  if (isinf(M)) { r.s1 = 0.0; r.s2 = 0.0; }
+  __syncthreads();
+  return r;
 }
 
 enum FinalizeMode { kFinalizeReduce = 0, kFinalizeStep = 1, kFinalizeLogsumexp = 2 };
@@ -87,13 +87,42 @@ enum FinalizeMode { kFinalizeReduce = 0, kFinalizeStep = 1, kFinalizeLogsumexp =
 // fixed order and write the statistics.
 __device__ __forceinline__ void finalize_partials(const LwPartial* partials, int np, int n,
                                                   StepStats* st, int mode, int observed) {
-  LwPartial v = lw_empty();
-  for (int i = threadIdx.x; i < np; i += blockDim.x) {
-    LwPartial p;
-    p.mx = __ldcg(&partials[i].mx);
-    p.s1 = __ldcg(&partials[i].s1);
-    p.s2 = __ldcg(&partials[i].s2);
-    v = lw_combine(v, p);
+  // each thread folds a fixed, strided subset of the partials (max first,
+  // then rescaled sums); loads are issued kBatch at a time so that the last
+  // block waits for a few memory round trips, not one per partial
+  constexpr int kBatch = 8;
+  const int nt = blockDim.x;
+  double m = -INFINITY;
+  for (int base = 0; base < np; base += nt * kBatch) {
+    double v[kBatch];
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) {
+      const int i = base + k * nt + threadIdx.x;
+      v[k] = i < np ? __ldcg(&partials[i].mx) : -INFINITY;
+    }
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) m = fmax(m, v[k]);
+  }
+  LwPartial v;
+  v.mx = m; v.s1 = 0.0; v.s2 = 0.0;
+  if (!isinf(m)) {
+    for (int base = 0; base < np; base += nt * kBatch) {
+      double pm[kBatch], p1[kBatch], p2[kBatch];
+#pragma unroll
+      for (int k = 0; k < kBatch; ++k) {
+        const int i = base + k * nt + threadIdx.x;
+        pm[k] = i < np ? __ldcg(&partials[i].mx) : 0.0;
+        p1[k] = i < np ? __ldcg(&partials[i].s1) : 0.0;
+        p2[k] = i < np ? __ldcg(&partials[i].s2) : 0.0;
+      }
+#pragma unroll
+      for (int k = 0; k < kBatch; ++k) {
+        if (p1[k] == 0.0) continue;
+        const double f = exp(pm[k] - m);
+        v.s1 += p1[k] * f;
+        v.s2 += p2[k] * f * f;
+      }
+    }
   }
   v = block_combine(v);
   if (threadIdx.x == 0) {

@@ -354,12 +354,12 @@ k_offspring_from(const int* __restrict__ src, int n, int mode, const StepStats* 
 // (share/src/bi/host/resampler/ResamplerHost.hpp:134-168) in closed form.
 //   o_i  = Os_i - Os_{i-1};  Z_i = #{m < i : o_m = 0}  (rank of a childless slot)
 //   E_i  = #{extra copies of ancestors < i} = Os_{i-1} - i + Z_i
-// Particle i with o_i > 0 keeps slot i; childless slot k of rank r receives
+// Particle i with o_i > 0 keeps slot i; the childless slot of rank r receives
 // the ancestor a with E_a <= r < E_{a+1}.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kBlock)
-k_permute_survivors(const int* __restrict__ Os, int n, const int* zprefix, int* as, int* E,
-                    const StepStats* st, const int* gate) {
+k_permute_survivors(const int* __restrict__ Os, int n, const int* zprefix, int* as, int* E, int* ecoarse,
+                    int coarse_shift, int* slot, const StepStats* st, const int* gate) {
   if (gate_closed(gate, st)) return;
   const int t = blockIdx.x;
   const int i0 = t * kTile + threadIdx.x * kItems;
@@ -380,26 +380,45 @@ k_permute_survivors(const int* __restrict__ Os, int n, const int* zprefix, int* 
     int i = i0 + k;
     int before = (k == 0 ? prev : os[k - 1]);
     if (i < n) {
-      E[i] = before - i + Z;
-      as[i] = z[k] ? -(Z + 1) : i;
+      const int e = before - i + Z;
+      E[i] = e;
+      if ((i & ((1 << coarse_shift) - 1)) == 0) ecoarse[i >> coarse_shift] = e;  // coarse search index
+      if (z[k]) slot[Z] = i;
+      else as[i] = i;
     }
     Z += z[k];
   }
 }
 
+// Childless slot of rank r receives the ancestor a with E_a <= r < E_{a+1}:
+// a search over every 2^coarse_shift-th value of E (held in shared memory),
+// then within that short segment.  One thread per rank, so the work is
+// balanced however the copies are distributed.
+constexpr int kMaxCoarse = 12288;  // 48 KB of coarse index
+
 __global__ void __launch_bounds__(kBlock)
-k_permute_fill(int* as, const int* __restrict__ E, int n, const StepStats* st, const int* gate) {
+k_permute_fill(int* as, const int* __restrict__ E, const int* __restrict__ ecoarse, int coarse_shift,
+               const int* __restrict__ slot, const int* zprefix, int n, int T, const StepStats* st,
+               const int* gate) {
   if (gate_closed(gate, st)) return;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    int v = as[i];
-    if (v < 0) {
-      int r = -v - 1, lo = 0, hi = n;
-      while (lo < hi) {
-        int mid = (lo + hi) >> 1;
-        if (__ldg(E + mid) <= r) lo = mid + 1; else hi = mid;
-      }
-      as[i] = lo - 1;
+  extern __shared__ int s_coarse[];
+  const int nc = ((n - 1) >> coarse_shift) + 1;
+  for (int i = threadIdx.x; i < nc; i += blockDim.x) s_coarse[i] = ecoarse[i];
+  __syncthreads();
+  const int R = zprefix[T];
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < R; r += gridDim.x * blockDim.x) {
+    int clo = 0, chi = nc;  // last segment whose first value is <= r (E[0] = 0 <= r)
+    while (clo < chi) {
+      int mid = (clo + chi) >> 1;
+      if (s_coarse[mid] <= r) clo = mid + 1; else chi = mid;
     }
+    int lo = (clo - 1) << coarse_shift;
+    int hi = min(n, lo + (1 << coarse_shift));
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      if (__ldg(E + mid) <= r) lo = mid + 1; else hi = mid;
+    }
+    as[__ldg(slot + r)] = lo - 1;
   }
 }
 
@@ -414,7 +433,7 @@ k_ancestors_from_Os(const int* __restrict__ Os, int n, int* as, const StepStats*
       int mid = (lo + hi) >> 1;
       if (__ldg(Os + mid) <= j) lo = mid + 1; else hi = mid;
     }
-    as[j] = lo;
+    as[j] = lo < n ? lo : n - 1;  // Os[n-1] == n for valid offsets; bounds any other
   }
 }
 
@@ -508,7 +527,8 @@ k_metropolis(const double* __restrict__ lw, int n, int B, const double* u, uint6
         ua = bpf_u01d(r.v[2], r.v[3]);
       }
       int p2 = __double2int_rz(__dmul_rn(ui, nd));
-      p2 = p2 < n - 1 ? p2 : n - 1;
+      p2 = p2 < n - 1 ? p2 : n - 1;  // uniformInt(0, n-1); also bounds caller-supplied uniforms
+      p2 = p2 > 0 ? p2 : 0;
       double lw2 = __ldg(lw + p2);
       if (log(ua) < __dsub_rn(lw2, lw1)) {
         p1 = p2;
@@ -531,6 +551,7 @@ k_gather(const int* __restrict__ as, const T* __restrict__ X, T* __restrict__ Y,
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int a = as[i];
+  if (a < 0 || a >= n) return;  // an ancestor out of range leaves the row untouched
   for (int j = 0; j < d; ++j) Y[(size_t)j * ld + i] = __ldg(X + (size_t)j * ld + a);
 }
 
@@ -542,7 +563,8 @@ int scratch_alloc(ResampleScratch& s, int max_n) {
   s.max_tiles = ntiles(max_n);
   const size_t T1 = (size_t)s.max_tiles + 1;
   const size_t N = (size_t)max_n;
-  s.max_partials = (max_n + 127) / 128 + 1;
+  // one partial per block of the widest per-step grid (64-thread transition blocks)
+  s.max_partials = (max_n + 63) / 64 + 1;
 #define ALLOC(ptr, bytes) \
   if (cudaMalloc((void**)&(ptr), (bytes)) != cudaSuccess) { scratch_free(s); return BPF_E_NOMEM; }
   ALLOC(s.tile_sum, T1 * sizeof(u128));
@@ -555,6 +577,8 @@ int scratch_alloc(ResampleScratch& s, int max_n) {
   ALLOC(s.iprefix, T1 * sizeof(int));
   ALLOC(s.Os, N * sizeof(int));
   ALLOC(s.E, N * sizeof(int));
+  ALLOC(s.slot, N * sizeof(int));
+  ALLOC(s.etile, (N / 16 + 2) * sizeof(int));
   ALLOC(s.o, N * sizeof(int));
   ALLOC(s.Ws, N * sizeof(double));
   ALLOC(s.lu, N * sizeof(double));
@@ -571,10 +595,20 @@ int scratch_alloc(ResampleScratch& s, int max_n) {
 
 void scratch_free(ResampleScratch& s) {
   void* ptrs[] = {s.tile_sum, s.tile_prefix, s.vtile_sum, s.vtile_prefix, s.zcount, s.zprefix,
-                  s.icount, s.iprefix, s.Os, s.E, s.o, s.Ws, s.lu, s.counters, s.stats, s.partials};
+                  s.icount, s.iprefix, s.Os, s.E, s.slot, s.etile, s.o, s.Ws, s.lu, s.counters, s.stats, s.partials};
   for (void* p : ptrs) if (p) cudaFree(p);
   s = ResampleScratch();
 }
+
+// coarse index stride: the smallest power of two >= 16 that keeps the index
+// within kMaxCoarse entries
+static inline int coarse_shift(int n) {
+  int sh = 4;
+  while ((((long long)n + (1ll << sh) - 1) >> sh) > kMaxCoarse) ++sh;
+  return sh;
+}
+
+static inline size_t fill_smem(int n) { return (size_t)(((n - 1) >> coarse_shift(n)) + 1) * sizeof(int); }
 
 static inline int grid_stride_blocks(int n) {
   int b = (n + kBlock - 1) / kBlock;
@@ -598,8 +632,10 @@ int launch_resample(const ResampleArgs& a, ResampleScratch& s, cudaStream_t st) 
       k_systematic_offspring<<<T, kBlock, 0, st>>>(a.lw, n, s.stats, s.tile_prefix, a.uniforms, a.seed,
                                                    a.step, Os, s.zcount, s.zprefix, c + 1, a.gate);
       if (a.permute) {
-        k_permute_survivors<<<T, kBlock, 0, st>>>(Os, n, s.zprefix, a.as, s.E, s.stats, a.gate);
-        k_permute_fill<<<grid_stride_blocks(n), kBlock, 0, st>>>(a.as, s.E, n, s.stats, a.gate);
+        k_permute_survivors<<<T, kBlock, 0, st>>>(Os, n, s.zprefix, a.as, s.E, s.etile, coarse_shift(n), s.slot,
+                                                  s.stats, a.gate);
+        k_permute_fill<<<grid_stride_blocks(n), kBlock, fill_smem(n), st>>>(a.as, s.E, s.etile, coarse_shift(n),
+                                                                             s.slot, s.zprefix, n, T, s.stats, a.gate);
       } else {
         k_ancestors_from_Os<<<grid_stride_blocks(n), kBlock, 0, st>>>(Os, n, a.as, s.stats, a.gate);
       }
@@ -616,8 +652,10 @@ int launch_resample(const ResampleArgs& a, ResampleScratch& s, cudaStream_t st) 
                                                a.gate);
       }
       if (a.permute) {
-        k_permute_survivors<<<T, kBlock, 0, st>>>(Os, n, s.zprefix, a.as, s.E, s.stats, a.gate);
-        k_permute_fill<<<grid_stride_blocks(n), kBlock, 0, st>>>(a.as, s.E, n, s.stats, a.gate);
+        k_permute_survivors<<<T, kBlock, 0, st>>>(Os, n, s.zprefix, a.as, s.E, s.etile, coarse_shift(n), s.slot,
+                                                  s.stats, a.gate);
+        k_permute_fill<<<grid_stride_blocks(n), kBlock, fill_smem(n), st>>>(a.as, s.E, s.etile, coarse_shift(n),
+                                                                             s.slot, s.zprefix, n, T, s.stats, a.gate);
       }
       break;
     }
@@ -632,8 +670,10 @@ int launch_resample(const ResampleArgs& a, ResampleScratch& s, cudaStream_t st) 
                                                a.gate);
       }
       if (a.permute) {
-        k_permute_survivors<<<T, kBlock, 0, st>>>(Os, n, s.zprefix, a.as, s.E, s.stats, a.gate);
-        k_permute_fill<<<grid_stride_blocks(n), kBlock, 0, st>>>(a.as, s.E, n, s.stats, a.gate);
+        k_permute_survivors<<<T, kBlock, 0, st>>>(Os, n, s.zprefix, a.as, s.E, s.etile, coarse_shift(n), s.slot,
+                                                  s.stats, a.gate);
+        k_permute_fill<<<grid_stride_blocks(n), kBlock, fill_smem(n), st>>>(a.as, s.E, s.etile, coarse_shift(n),
+                                                                             s.slot, s.zprefix, n, T, s.stats, a.gate);
       }
       break;
     }
