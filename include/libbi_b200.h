@@ -33,7 +33,8 @@ enum {
   BPF_E_INVALID = 2,   /* bad argument (size, kind, null pointer) */
   BPF_E_CUDA = 3,      /* a CUDA runtime call failed */
   BPF_E_TIMEOUT = 4,   /* a bounded device-side wait gave up */
-  BPF_E_NOMEM = 5      /* device allocation failed */
+  BPF_E_NOMEM = 5,     /* device allocation failed */
+  BPF_E_TOO_LARGE = 6  /* n exceeds BPF_STATIC_MAX_PARTICLES (bpf_systematic_ancestors_static) */
 };
 
 /* ---- model description ------------------------------------------------ */
@@ -222,6 +223,25 @@ int bpf_resampler_ancestors(bpf_resampler* r, const double* lw, int n,
  * elem_size is 4 or 8. */
 int bpf_gather_rows(const int* as, const void* X, void* Y, int n, int d, int ld,
                     int elem_size, void* stream);
+
+/* Systematic resampling that allocates nothing.  No counterpart in the
+ * reference: this entry point exists for callers that cannot let the library
+ * allocate device memory, such as an application that has reserved the GPU's
+ * memory up front for its own allocator, or a real-time loop in which a
+ * cudaMalloc (which may synchronise the device) is not allowed.  It computes
+ * exactly what bpf_resampler_ancestors computes for a systematic resampler
+ * (same arguments: device lw[n], optional device offset a, permute, device
+ * as[n], optional device Os[n]; work on `stream`), but its scratch is one
+ * fixed-size __device__ array inside the library (under 1 MiB, held on every
+ * GPU that loads the library until the process exits), so n may be at most
+ * BPF_STATIC_MAX_PARTICLES; larger n returns BPF_E_TOO_LARGE.  The first call
+ * on each device looks up that array's address; make it before any stream
+ * capture.  All calls share the array, so calls that overlap on the GPU race
+ * and must be ordered by the caller.  Synchronises `stream` and returns
+ * BPF_E_DEGENERATE when the weights sum to zero or are not finite. */
+#define BPF_STATIC_MAX_PARTICLES 65536
+int bpf_systematic_ancestors_static(const double* lw, int n, const double* a, int permute, int* as, int* Os,
+                                    void* stream);
 
 /* ---- checkpoint (BootstrapPFState save/load,
  *      share/src/bi/state/BootstrapPFState.hpp:216-231) ------------------- */

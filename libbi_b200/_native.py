@@ -19,6 +19,8 @@ BPF_E_INVALID = 2
 BPF_E_CUDA = 3
 BPF_E_TIMEOUT = 4
 BPF_E_NOMEM = 5
+BPF_E_TOO_LARGE = 6
+BPF_STATIC_MAX_PARTICLES = 65536
 
 BPF_MODEL_L96 = 1
 BPF_MODEL_PZ = 2
@@ -38,7 +40,7 @@ EXPORTS = (
     "bpf_resampler_create", "bpf_resampler_destroy", "bpf_ess_reduce",
     "bpf_logsumexp_reduce", "bpf_resampler_ancestors", "bpf_gather_rows",
     "bpf_snapshot_size", "bpf_snapshot", "bpf_restore", "bpf_version",
-    "bpf_status_string", "bpf_timing_enable", "bpf_timing_read",
+    "bpf_status_string", "bpf_timing_enable", "bpf_timing_read", "bpf_systematic_ancestors_static",
 )
 
 
@@ -103,6 +105,8 @@ def _declare(L):
         "bpf_restore": (c_int, [H, c_void_p, c_uint64]),
         "bpf_timing_enable": (c_int, [H, c_int]),
         "bpf_timing_read": (c_int, [H, c_int, POINTER(c_double), POINTER(c_double), POINTER(c_int)]),
+        "bpf_systematic_ancestors_static": (c_int, [c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p,
+                                                    c_void_p]),
         "bpf_version": (c_char_p, []),
         "bpf_status_string": (c_char_p, [c_int]),
     }

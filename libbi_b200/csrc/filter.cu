@@ -182,6 +182,7 @@ const char* bpf_status_string(int s) {
     case BPF_E_CUDA: return cudaGetErrorString(g_last_cuda_error);
     case BPF_E_TIMEOUT: return "bounded device wait gave up";
     case BPF_E_NOMEM: return "device allocation failed";
+    case BPF_E_TOO_LARGE: return "more particles than the static scratch holds (BPF_STATIC_MAX_PARTICLES)";
     default: return "unknown status";
   }
 }
