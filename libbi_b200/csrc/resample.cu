@@ -114,6 +114,8 @@ __device__ __forceinline__ void load_blocked(const double* __restrict__ lw, int 
   }
 }
 
+__device__ __forceinline__ int ntiles_dev(int n) { return (n + kTile - 1) / kTile; }
+
 __device__ __forceinline__ bool gate_closed(const int* gate, const StepStats* st) {
   if (gate != nullptr && *gate == 0) return true;
   return st->status != BPF_OK;
@@ -257,6 +259,225 @@ k_systematic_offspring(const double* __restrict__ lw, int n, StepStats* st,
   if (last_block_arrive(counter)) {
     block_scan_tiles_int(zcount, zprefix, T);
     if (threadIdx.x == 0) *counter = 0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// systematic resampling in one cooperative launch
+//
+// The four passes above (weight sums, offspring, survivors, fill) run as
+// phases of one kernel separated by grid-wide barriers.  The grid is at most
+// as large as the GPU can hold at once and is launched cooperatively, so every
+// block is resident and every barrier is reached; each wait is still bounded
+// by a clock limit after which the kernel records BPF_E_TIMEOUT and returns.
+// Block b owns the contiguous tiles [b T / G, (b+1) T / G); prefix sums over
+// blocks are formed from the G block totals published at each barrier.
+// Data written during the kernel is read with ld.global.cg (never through the
+// read-only cache).
+// ---------------------------------------------------------------------------
+constexpr long long kBarrierTimeoutCycles = 4000000000ll;  // ~2 s at 2 GHz
+
+// Bounded grid barrier.  counter returns to zero after every barrier; gen
+// counts completed barriers.  Returns false (in every thread) on timeout.
+__device__ __forceinline__ bool grid_barrier(unsigned* counter, unsigned* gen, StepStats* st) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* vgen = gen;
+    const unsigned g = *vgen;
+    __threadfence();
+    const unsigned arrived = atomicAdd(counter, 1u);
+    int ok = 1;
+    if (arrived == gridDim.x - 1) {
+      *counter = 0;
+      __threadfence();
+      atomicAdd(gen, 1u);
+    } else {
+      const long long t0 = clock64();
+      while (*vgen == g) {
+        if (clock64() - t0 > kBarrierTimeoutCycles) {
+          ok = 0;
+          st->status = BPF_E_TIMEOUT;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+__device__ __forceinline__ void load_blocked_cg(const double* __restrict__ lw, int i0, int n, double v[kItems]) {
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) v[k] = (i0 + k < n) ? lw[i0 + k] : NAN;
+}
+
+__device__ __forceinline__ u128 block_sum_u128_from_global(const u128* a, int count) {
+  // sum of a[0..count) by the whole block (exact, any order)
+  u128 acc = u128_zero();
+  for (int i = threadIdx.x; i < count; i += blockDim.x) acc = u128_add(acc, ldcg_u128(&a[i]));
+  u128 tot;
+  block_exclusive_scan_u128(acc, &tot);
+  return tot;
+}
+
+__device__ __forceinline__ int block_sum_int_from_global(const int* a, int count) {
+  int acc = 0;
+  for (int i = threadIdx.x; i < count; i += blockDim.x) acc += __ldcg(&a[i]);
+  int tot;
+  block_exclusive_scan_int(acc, &tot);
+  return tot;
+}
+
+__global__ void __launch_bounds__(kBlock)
+k_systematic_coop(const double* __restrict__ lw, int n, StepStats* st, const double* a_in, uint64_t seed, int step,
+                  int* Os, int* as, int* E, int* ecoarse, int coarse_shift, int* slot,
+                  u128* block_w, int* block_z, unsigned* bar_counter, unsigned* bar_gen, const int* gate) {
+  if (gate_closed(gate, st)) return;
+  extern __shared__ int s_coarse[];
+  __shared__ int s_prev_os;
+  const int G = gridDim.x, b = blockIdx.x;
+  const int T = ntiles_dev(n);
+  const int tb0 = (int)(((long long)b * T) / G), tb1 = (int)(((long long)(b + 1) * T) / G);
+  const double mx = st->mx;
+  double a;
+  if (a_in) {
+    a = *a_in;
+  } else {
+    bpf_u32x4 r = bpf_draw(seed, 0u, (uint32_t)step, 0u, BPF_RNG_SYSTEMATIC);
+    a = bpf_u01d(r.v[0], r.v[1]);
+  }
+
+  // phase 1: exact fixed-point weight total of this block's tiles
+  u128 wsum = u128_zero();
+  for (int t = tb0; t < tb1; ++t) {
+    const int i0 = t * kTile + threadIdx.x * kItems;
+    double v[kItems];
+    load_blocked(lw, i0, n, v);
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+      if (i0 + k < n) {
+        u128 q; q.lo = weight_to_fixed(nanexp(__dsub_rn(v[k], mx))); q.hi = 0;
+        wsum = u128_add(wsum, q);
+      }
+    }
+  }
+  u128 btot;
+  block_exclusive_scan_u128(wsum, &btot);
+  if (threadIdx.x == 0) block_w[b] = btot;
+  if (!grid_barrier(bar_counter, bar_gen, st)) return;
+
+  // phase 2: prefix of this block, total W, cumulative offspring, childless counts
+  const u128 prefix_b = block_sum_u128_from_global(block_w, b);
+  const u128 total = block_sum_u128_from_global(block_w, G);
+  const double W = u128_to_weight(total);
+  // SystematicResampler::cumulativeOffspring throws unless W > 0
+  // (share/src/bi/resampler/SystematicResampler.hpp:118-129); every block
+  // computes the same W and leaves together
+  if (!(W > 0.0)) {
+    if (b == 0 && threadIdx.x == 0) st->status = BPF_E_DEGENERATE;
+    return;
+  }
+  const double nd = (double)n;
+  __shared__ int s_last[kBlock];
+  u128 carry = prefix_b;
+  int zeros = 0;
+  if (threadIdx.x == 0) s_prev_os = tb0 == 0 ? 0 : systematic_Os(u128_to_weight(prefix_b), W, nd, a, n);
+  for (int t = tb0; t < tb1; ++t) {
+    const int i0 = t * kTile + threadIdx.x * kItems;
+    double v[kItems];
+    load_blocked(lw, i0, n, v);
+    unsigned long long q[kItems];
+    u128 loc = u128_zero();
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+      q[k] = (i0 + k < n) ? weight_to_fixed(nanexp(__dsub_rn(v[k], mx))) : 0ull;
+      u128 qq; qq.lo = q[k]; qq.hi = 0;
+      loc = u128_add(loc, qq);
+    }
+    u128 ttot;
+    u128 Q = u128_add(carry, block_exclusive_scan_u128(loc, &ttot));
+    int os[kItems];
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+      u128 qq; qq.lo = q[k]; qq.hi = 0;
+      Q = u128_add(Q, qq);
+      os[k] = systematic_Os(u128_to_weight(Q), W, nd, a, n);
+    }
+    s_last[threadIdx.x] = os[kItems - 1];
+    __syncthreads();
+    int prev = threadIdx.x > 0 ? s_last[threadIdx.x - 1] : s_prev_os;
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+      if (i0 + k < n) {
+        Os[i0 + k] = os[k];
+        zeros += (os[k] == prev);
+      }
+      prev = os[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == kBlock - 1) s_prev_os = os[kItems - 1];
+    carry = u128_add(carry, ttot);
+    __syncthreads();
+  }
+  int ztot;
+  block_exclusive_scan_int(zeros, &ztot);
+  if (threadIdx.x == 0) block_z[b] = ztot;
+  if (!grid_barrier(bar_counter, bar_gen, st)) return;
+
+  // phase 3: ranks of childless slots, extra-copy counts, survivors in place
+  int zcarry = block_sum_int_from_global(block_z, b);
+  const int R = block_sum_int_from_global(block_z, G);
+  for (int t = tb0; t < tb1; ++t) {
+    const int i0 = t * kTile + threadIdx.x * kItems;
+    int prev = i0 > 0 && i0 - 1 < n ? __ldcg(Os + i0 - 1) : 0;
+    int os[kItems], z[kItems];
+    int loc = 0;
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+      os[k] = (i0 + k < n) ? __ldcg(Os + i0 + k) : prev;
+      z[k] = (i0 + k < n) && (os[k] == (k == 0 ? prev : os[k - 1]));
+      loc += z[k];
+    }
+    int ttot;
+    int Z = zcarry + block_exclusive_scan_int(loc, &ttot);
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+      const int i = i0 + k;
+      const int before = (k == 0 ? prev : os[k - 1]);
+      if (i < n) {
+        const int e = before - i + Z;
+        E[i] = e;
+        if ((i & ((1 << coarse_shift) - 1)) == 0) ecoarse[i >> coarse_shift] = e;
+        if (z[k]) slot[Z] = i;
+        else as[i] = i;
+      }
+      Z += z[k];
+    }
+    zcarry += ttot;
+  }
+  if (!grid_barrier(bar_counter, bar_gen, st)) return;
+
+  // phase 4: childless slot of rank r <- ancestor a with E_a <= r < E_{a+1}
+  const int nc = ((n - 1) >> coarse_shift) + 1;
+  for (int i = threadIdx.x; i < nc; i += blockDim.x) s_coarse[i] = __ldcg(ecoarse + i);
+  __syncthreads();
+  for (int r = b * blockDim.x + threadIdx.x; r < R; r += G * blockDim.x) {
+    int clo = 0, chi = nc;
+    while (clo < chi) {
+      int mid = (clo + chi) >> 1;
+      if (s_coarse[mid] <= r) clo = mid + 1; else chi = mid;
+    }
+    int lo = (clo - 1) << coarse_shift;
+    int hi = min(n, lo + (1 << coarse_shift));
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      if (__ldcg(E + mid) <= r) lo = mid + 1; else hi = mid;
+    }
+    as[__ldcg(slot + r)] = lo - 1;
   }
 }
 
@@ -601,14 +822,22 @@ void scratch_free(ResampleScratch& s) {
 }
 
 // coarse index stride: the smallest power of two >= 16 that keeps the index
-// within kMaxCoarse entries
-static inline int coarse_shift(int n) {
+// within max_entries entries
+static inline int coarse_shift(int n, int max_entries = kMaxCoarse) {
   int sh = 4;
-  while ((((long long)n + (1ll << sh) - 1) >> sh) > kMaxCoarse) ++sh;
+  while ((((long long)n + (1ll << sh) - 1) >> sh) > max_entries) ++sh;
   return sh;
 }
 
-static inline size_t fill_smem(int n) { return (size_t)(((n - 1) >> coarse_shift(n)) + 1) * sizeof(int); }
+static inline size_t fill_smem(int n, int max_entries = kMaxCoarse) {
+  return (size_t)(((n - 1) >> coarse_shift(n, max_entries)) + 1) * sizeof(int);
+}
+
+// the cooperative kernel keeps its coarse index within 32 KB, leaving room
+// for its static shared memory under the default 48 KB limit
+constexpr int kMaxCoarseCoop = 8192;
+
+static int launch_systematic_coop(const ResampleArgs& a, ResampleScratch& s, int* Os, cudaStream_t st);
 
 static inline int grid_stride_blocks(int n) {
   int b = (n + kBlock - 1) / kBlock;
@@ -627,6 +856,10 @@ int launch_resample(const ResampleArgs& a, ResampleScratch& s, cudaStream_t st) 
   }
   switch (a.kind) {
     case BPF_RESAMPLER_SYSTEMATIC: {
+      if (a.permute) {
+        int rc = launch_systematic_coop(a, s, Os, st);
+        if (rc != BPF_E_INVALID) return rc;  // BPF_E_INVALID: cooperative launch unavailable, use the passes
+      }
       k_weight_tile_sums<<<T, kBlock, 0, st>>>(a.lw, n, s.stats, s.tile_sum, s.tile_prefix, 0, nullptr,
                                                a.seed, a.step, nullptr, nullptr, c + 0, a.gate);
       k_systematic_offspring<<<T, kBlock, 0, st>>>(a.lw, n, s.stats, s.tile_prefix, a.uniforms, a.seed,
@@ -681,6 +914,55 @@ int launch_resample(const ResampleArgs& a, ResampleScratch& s, cudaStream_t st) 
       return BPF_E_INVALID;
   }
   BPF_TRY(cudaGetLastError());
+  return BPF_OK;
+}
+
+// Cooperative launch of k_systematic_coop over at most as many blocks as the
+// GPU holds at once (and at most one per tile).  Returns BPF_E_INVALID when a
+// cooperative launch is not possible, so the caller can run the passes.
+static int launch_systematic_coop(const ResampleArgs& a, ResampleScratch& s, int* Os, cudaStream_t st) {
+  static int coop_supported = -1, sms = 0;
+  int dev = 0;
+  BPF_TRY(cudaGetDevice(&dev));
+  if (coop_supported < 0) {
+    BPF_TRY(cudaDeviceGetAttribute(&coop_supported, cudaDevAttrCooperativeLaunch, dev));
+    BPF_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  }
+  if (!coop_supported) return BPF_E_INVALID;
+  const int n = a.n;
+  const int sh = coarse_shift(n, kMaxCoarseCoop);
+  const size_t smem = fill_smem(n, kMaxCoarseCoop);
+  // resident blocks per SM, cached per shared-memory size (the launch is on
+  // every filter step)
+  static size_t cached_smem = (size_t)-1;
+  static int per_sm = 0;
+  if (smem != cached_smem) {
+    BPF_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_systematic_coop, kBlock, smem));
+    cached_smem = smem;
+  }
+  const int T = ntiles(n);
+  int G = sms * per_sm;
+  if (G > T) G = T;
+  if (G < 1) return BPF_E_INVALID;
+  const double* lw = a.lw;
+  StepStats* stats = s.stats;
+  const double* a_in = a.uniforms;
+  uint64_t seed = a.seed;
+  int step = a.step;
+  int* as = a.as;
+  int* E = s.E;
+  int* ec = s.etile;
+  int* slot = s.slot;
+  u128* bw = s.tile_sum;     // G <= T block totals
+  int* bz = s.zcount;
+  unsigned* bc = s.counters + 8;
+  unsigned* bg = s.counters + 9;
+  const int* gate = a.gate;
+  int nn = n;
+  void* args[] = {(void*)&lw, (void*)&nn, (void*)&stats, (void*)&a_in, (void*)&seed, (void*)&step, (void*)&Os,
+                  (void*)&as, (void*)&E, (void*)&ec, (void*)&sh, (void*)&slot, (void*)&bw, (void*)&bz,
+                  (void*)&bc, (void*)&bg, (void*)&gate};
+  BPF_TRY(cudaLaunchCooperativeKernel((const void*)k_systematic_coop, dim3(G), dim3(kBlock), args, smem, st));
   return BPF_OK;
 }
 
