@@ -38,10 +38,10 @@ ESS_REL = 0.5
 SEED = 2
 DATA_SEED = 102
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
-# our kernels per step with the systematic resampler: weight tile sums,
-# offspring, survivors, fill (launched every step, gated on the device) +
-# the fused transition
-LAUNCHES_PER_STEP = 5
+# our kernels per step with the systematic resampler: the cooperative
+# resample kernel (launched every step, gated on the device) + the fused
+# transition
+LAUNCHES_PER_STEP = 2
 # algorithmic bytes of the fused transition per particle: state read + write
 # (2 * d * 4 B) and FP64 log-weight read + write (16 B); the ancestor index
 # (4 B) is read only on resample steps
@@ -168,6 +168,58 @@ def cpu_baseline(y, seconds: float = 12.0):
                       f"observation steps (incl. initial draw), {threads} OpenMP threads, {el:.1f} s"}
 
 
+def large_n_kernels(sizes=(1 << 22, 1 << 24), reps=5):
+    """The memory-bound kernels at working sets beyond L2: log-weight
+    reduction (ess_reduce), permuted systematic resampling and the ancestor
+    gather (40 FP32 components).  Device time from CUDA events around each
+    call (each call ends with a small device-to-host status read), L2 flushed
+    before every repetition; achieved GB/s counts algorithmic bytes:
+    reduce 8 B, resample 8 + 4 B (log-weight in, ancestor out), gather
+    2*40*4 + 4 B per particle."""
+    import torch
+    from libbi_b200 import SystematicResampler, gather_rows
+
+    hbm, _, _ = peaks()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    out = {}
+    for n in sizes:
+        g = torch.Generator(device="cuda")
+        g.manual_seed(n)
+        lw = torch.randn(n, dtype=torch.float64, device="cuda", generator=g) * 2.0
+        a = torch.full((1,), 0.37, dtype=torch.float64, device="cuda")
+        R = SystematicResampler(max_n=n)
+        ld = (n + 31) // 32 * 32
+        X = torch.randn((DIM, ld), dtype=torch.float32, device="cuda", generator=g)
+        Y = torch.empty_like(X)
+        as_ = R.ancestors(lw, a, permute=True)
+
+        def timed(fn):
+            ts = []
+            for _ in range(reps):
+                flush.zero_()
+                s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                s0.record()
+                fn()
+                s1.record()
+                torch.cuda.synchronize()
+                ts.append(s0.elapsed_time(s1) / 1e3)
+            return min(ts)
+
+        t_red = timed(lambda: R.reduce(lw))
+        t_res = timed(lambda: R.ancestors(lw, a, permute=True))
+        t_gat = timed(lambda: (gather_rows(as_, X, Y, DIM, ld), torch.cuda.synchronize()))
+        rows = {}
+        for name, t, byt in (("ess_reduce", t_red, 8 * n), ("systematic_resample", t_res, 12 * n),
+                             ("gather_rows_d40", t_gat, (2 * DIM * 4 + 4) * n)):
+            gbs = byt / t / 1e9
+            rows[name] = {"ms": t * 1e3, "GB/s": gbs, "frac_hbm": gbs / hbm}
+        out[str(n)] = rows
+        R.close()
+        del lw, X, Y, as_
+        torch.cuda.empty_cache()
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -200,6 +252,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-large-n", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -327,6 +380,8 @@ def main():
         "wall_s": wall,
         "clocks": clocks,
     }
+    if rank == 0 and not args.no_large_n:
+        line["kernels_large_n"] = large_n_kernels()
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(y_host)
     pf.close()

@@ -29,18 +29,32 @@
 
 #include "bpf_philox.h"
 
-#if defined(__CUDACC__)
 #define BPF_MATH_FMA(a, b, c) fma((a), (b), (c))
 #define BPF_MATH_FMAF(a, b, c) fmaf((a), (b), (c))
+/* a product that must be rounded on its own before it feeds a sum */
+#if defined(__CUDA_ARCH__)
+#define BPF_MATH_MUL(a, b) __dmul_rn((a), (b))
+#define BPF_MATH_MULF(a, b) __fmul_rn((a), (b))
 #else
-#define BPF_MATH_FMA(a, b, c) fma((a), (b), (c))
-#define BPF_MATH_FMAF(a, b, c) fmaf((a), (b), (c))
+#define BPF_MATH_MUL(a, b) ((a) * (b))
+#define BPF_MATH_MULF(a, b) ((a) * (b))
 #endif
 
 BPF_HD uint64_t bpf_dbits(double x) { uint64_t u; memcpy(&u, &x, 8); return u; }
 BPF_HD double bpf_bitsd(uint64_t u) { double x; memcpy(&x, &u, 8); return x; }
 BPF_HD uint32_t bpf_fbits(float x) { uint32_t u; memcpy(&u, &x, 4); return u; }
 BPF_HD float bpf_bitsf(uint32_t u) { float x; memcpy(&x, &u, 4); return x; }
+
+/* Exact conversions without integer<->float instructions, for the integer
+ * ranges used below: 2^23 + k (float) and 2^52 + k (double) hold k in their
+ * low mantissa bits, so adding 1.5*2^23 (1.5*2^52) rounds a value to the
+ * nearest integer (ties to even) and exposes its low bits. */
+BPF_HD float bpf_small_int_to_float(int k) {      /* |k| < 2^21 */
+  return bpf_bitsf(0x4B000000u | (uint32_t)(k + (1 << 22))) - 12582912.0f;
+}
+BPF_HD double bpf_small_int_to_double(int k) {    /* |k| < 2^30 */
+  return bpf_bitsd(0x4330000000000000ull | (uint64_t)(uint32_t)(k + (1 << 30))) - 4503600701112320.0;
+}
 
 /* ---------------------------------------------------------------- double */
 
@@ -51,7 +65,10 @@ BPF_HD double bpf_exp(double x) {
   if (x != x) return x;
   if (x > 709.782712893384) return INFINITY;
   if (x < -745.1332191019412) return 0.0;
-  double k = rint(x * inv_ln2);
+  /* k = rint(x / ln2) by the 1.5*2^52 rounding constant; its low bits are k */
+  const double t = BPF_MATH_MUL(x, inv_ln2) + 6755399441055744.0;
+  const double k = t - 6755399441055744.0;
+  const int ki = (int)(uint32_t)bpf_dbits(t);
   double r = BPF_MATH_FMA(-k, ln2_hi, x);
   r = BPF_MATH_FMA(-k, ln2_lo, r);
   /* e^r = sum r^j / j!, j <= 13 */
@@ -69,7 +86,6 @@ BPF_HD double bpf_exp(double x) {
   p = BPF_MATH_FMA(p, r, 0.5);
   p = BPF_MATH_FMA(p, r, 1.0);
   p = BPF_MATH_FMA(p, r, 1.0);
-  int ki = (int)k;
   if (ki >= -1022) {
     if (ki > 1023) return p * bpf_bitsd((uint64_t)(1023 + 1023) << 52) * 2.0;
     return p * bpf_bitsd((uint64_t)(ki + 1023) << 52);
@@ -111,13 +127,22 @@ BPF_HD double bpf_log(double x) {
   p = p * s2;
   double t = 2.0 * s;
   double lm = BPF_MATH_FMA(t, p, t);
-  double ed = (double)e;
+  const double ed = bpf_small_int_to_double(e);
   return BPF_MATH_FMA(ed, ln2_hi, BPF_MATH_FMA(ed, ln2_lo, lm));
 }
 
 /* sin(pi x) and cos(pi x) */
 BPF_HD void bpf_sincospi(double x, double* sp, double* cp) {
-  double q = rint(2.0 * x);
+  double q;
+  int qi;
+  if (fabs(x) < 1.0e15) {  /* q = rint(2x) by the rounding constant; quadrant = low bits */
+    const double t = 2.0 * x + 6755399441055744.0;
+    q = t - 6755399441055744.0;
+    qi = (int)(bpf_dbits(t) & 3u);
+  } else {
+    q = rint(2.0 * x);
+    qi = ((int)fmod(q, 4.0) + 4) & 3;
+  }
   double r = BPF_MATH_FMA(-0.5, q, x);
   double r2 = r * r;
   double s = -2.2948428997269873e-08;            /* -pi^19/19! */
@@ -141,7 +166,6 @@ BPF_HD void bpf_sincospi(double x, double* sp, double* cp) {
   c = BPF_MATH_FMA(c, r2, 4.0587121264167685);
   c = BPF_MATH_FMA(c, r2, -4.934802200544679);
   c = BPF_MATH_FMA(c, r2, 1.0);
-  int qi = ((int)(q - 4.0 * floor(q * 0.25))) & 3;
   switch (qi) {
     case 0: *sp = s; *cp = c; break;
     case 1: *sp = c; *cp = -s; break;
@@ -159,7 +183,9 @@ BPF_HD float bpf_expf(float x) {
   if (x != x) return x;
   if (x > 88.72283f) return INFINITY;
   if (x < -103.97208f) return 0.0f;
-  float k = rintf(x * inv_ln2);
+  const float t = BPF_MATH_MULF(x, inv_ln2) + 12582912.0f;
+  const float k = t - 12582912.0f;
+  const int ki = (int)(bpf_fbits(t) & 0x7FFFFFu) - 0x400000;
   float r = BPF_MATH_FMAF(-k, ln2_hi, x);
   r = BPF_MATH_FMAF(-k, ln2_lo, r);
   float p = 1.0f / 5040.0f;
@@ -170,7 +196,6 @@ BPF_HD float bpf_expf(float x) {
   p = BPF_MATH_FMAF(p, r, 0.5f);
   p = BPF_MATH_FMAF(p, r, 1.0f);
   p = BPF_MATH_FMAF(p, r, 1.0f);
-  int ki = (int)k;
   if (ki >= -126) {
     if (ki > 127) return p * bpf_bitsf((uint32_t)(127 + 127) << 23) * 2.0f;
     return p * bpf_bitsf((uint32_t)(ki + 127) << 23);
@@ -204,12 +229,21 @@ BPF_HD float bpf_logf(float x) {
   p = p * s2;
   float t = 2.0f * s;
   float lm = BPF_MATH_FMAF(t, p, t);
-  float ef = (float)e;
+  const float ef = bpf_small_int_to_float(e);
   return BPF_MATH_FMAF(ef, ln2_hi, BPF_MATH_FMAF(ef, ln2_lo, lm));
 }
 
 BPF_HD void bpf_sincospif(float x, float* sp, float* cp) {
-  float q = rintf(2.0f * x);
+  float q;
+  int qi;
+  if (fabsf(x) < 1048576.0f) {  /* q = rint(2x) by the rounding constant; quadrant = low bits */
+    const float t = 2.0f * x + 12582912.0f;
+    q = t - 12582912.0f;
+    qi = (int)(bpf_fbits(t) & 3u);
+  } else {
+    q = rintf(2.0f * x);
+    qi = ((int)fmodf(q, 4.0f) + 4) & 3;
+  }
   float r = BPF_MATH_FMAF(-0.5f, q, x);
   float r2 = r * r;
   float s = 0.08214588463306427f;                /* pi^9/9! */
@@ -224,7 +258,6 @@ BPF_HD void bpf_sincospif(float x, float* sp, float* cp) {
   c = BPF_MATH_FMAF(c, r2, 4.058712005615234f);
   c = BPF_MATH_FMAF(c, r2, -4.934802055358887f);
   c = BPF_MATH_FMAF(c, r2, 1.0f);
-  int qi = ((int)(q - 4.0f * floorf(q * 0.25f))) & 3;
   switch (qi) {
     case 0: *sp = s; *cp = c; break;
     case 1: *sp = c; *cp = -s; break;

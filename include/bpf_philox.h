@@ -71,9 +71,12 @@ BPF_HD bpf_u32x4 bpf_draw(uint64_t seed, uint32_t p, uint32_t step, uint32_t blk
 }
 
 /* 32 random bits -> float uniform on (0,1): (2m+1)*2^-24 with m the top 23
- * bits; exactly representable, never 0 or 1. */
+ * bits; exactly representable, never 0 or 1.  Formed from the bit pattern
+ * 1 + m*2^-23 (two exact additions, no integer-to-float conversion). */
 BPF_HD float bpf_u01f(uint32_t x) {
-  return (float)(2u*(x >> 9) + 1u) * 5.9604644775390625e-08f; /* 2^-24 */
+  union { uint32_t u; float f; } b;
+  b.u = 0x3F800000u | (x >> 9);
+  return (b.f - 1.0f) + 5.9604644775390625e-08f; /* 2^-24 */
 }
 
 /* 64 random bits -> double uniform on (0,1): (2m+1)*2^-53 with m the top 52

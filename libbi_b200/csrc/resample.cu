@@ -21,6 +21,8 @@
 #include "internal.cuh"
 #include "reduce.cuh"
 
+#include <cooperative_groups.h>
+
 namespace bpf {
 
 // ---------------------------------------------------------------------------
@@ -481,6 +483,381 @@ k_systematic_coop(const double* __restrict__ lw, int n, StepStats* st, const dou
   }
 }
 
+// One tile per block (n <= G * kTile): each thread keeps its fixed-point
+// weights and cumulative offspring in registers across the grid barriers, so
+// after the log-weights are read the only global traffic is the G block
+// totals, the extra-copy index for the fill, and the ancestors.
+__device__ __forceinline__ void block_sum_pair_u128(const u128* a, int count, int split, u128* below, u128* all) {
+  // *below = sum a[0..split), *all = sum a[0..count), one pass, exact
+  u128 lo = u128_zero(), tot = u128_zero();
+  for (int i = threadIdx.x; i < count; i += blockDim.x) {
+    const u128 v = ldcg_u128(&a[i]);
+    tot = u128_add(tot, v);
+    if (i < split) lo = u128_add(lo, v);
+  }
+  block_exclusive_scan_u128(lo, below);
+  block_exclusive_scan_u128(tot, all);
+}
+
+__device__ __forceinline__ void block_sum_pair_int(const int* a, int count, int split, int* below, int* all) {
+  int lo = 0, tot = 0;
+  for (int i = threadIdx.x; i < count; i += blockDim.x) {
+    const int v = __ldcg(&a[i]);
+    tot += v;
+    if (i < split) lo += v;
+  }
+  block_exclusive_scan_int(lo, below);
+  block_exclusive_scan_int(tot, all);
+}
+
+__global__ void __launch_bounds__(kBlock)
+k_systematic_coop1(const double* __restrict__ lw, int n, StepStats* st, const double* a_in, uint64_t seed,
+                   int step, int* Os_out, int* as, int* E, int* ecoarse, int coarse_shift, int* slot,
+                   u128* block_w, int* block_z, unsigned* bar_counter, unsigned* bar_gen, const int* gate) {
+  if (gate_closed(gate, st)) return;
+  extern __shared__ int s_coarse[];
+  __shared__ int s_last[kBlock];
+  const int G = gridDim.x, b = blockIdx.x;
+  const int i0 = b * kTile + threadIdx.x * kItems;
+  const double mx = st->mx;
+  double a;
+  if (a_in) {
+    a = *a_in;
+  } else {
+    bpf_u32x4 r = bpf_draw(seed, 0u, (uint32_t)step, 0u, BPF_RNG_SYSTEMATIC);
+    a = bpf_u01d(r.v[0], r.v[1]);
+  }
+
+  // phase 1: fixed-point weights (registers) and the block total
+  double v[kItems];
+  load_blocked(lw, i0, n, v);
+  unsigned long long q[kItems];
+  u128 loc = u128_zero();
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) {
+    q[k] = (i0 + k < n) ? weight_to_fixed(nanexp(__dsub_rn(v[k], mx))) : 0ull;
+    u128 qq; qq.lo = q[k]; qq.hi = 0;
+    loc = u128_add(loc, qq);
+  }
+  u128 btot;
+  const u128 texcl = block_exclusive_scan_u128(loc, &btot);
+  if (threadIdx.x == 0) block_w[b] = btot;
+  if (!grid_barrier(bar_counter, bar_gen, st)) return;
+
+  // phase 2: block prefix and total W; cumulative offspring (registers)
+  u128 prefix, total;
+  block_sum_pair_u128(block_w, G, b, &prefix, &total);
+  const double W = u128_to_weight(total);
+  if (!(W > 0.0)) {  // every block sees the same W and leaves here
+    if (b == 0 && threadIdx.x == 0) st->status = BPF_E_DEGENERATE;
+    return;
+  }
+  const double nd = (double)n;
+  int os[kItems];
+  {
+    u128 Q = u128_add(prefix, texcl);
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+      u128 qq; qq.lo = q[k]; qq.hi = 0;
+      Q = u128_add(Q, qq);
+      os[k] = systematic_Os(u128_to_weight(Q), W, nd, a, n);
+    }
+  }
+  s_last[threadIdx.x] = os[kItems - 1];
+  __syncthreads();
+  const int before0 = threadIdx.x > 0 ? s_last[threadIdx.x - 1]
+                                      : (b == 0 ? 0 : systematic_Os(u128_to_weight(prefix), W, nd, a, n));
+  int zl = 0;
+  {
+    int prev = before0;
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+      if (i0 + k < n) {
+        zl += (os[k] == prev);
+        if (Os_out) Os_out[i0 + k] = os[k];
+      }
+      prev = os[k];
+    }
+  }
+  int ztot;
+  const int zexcl = block_exclusive_scan_int(zl, &ztot);
+  if (threadIdx.x == 0) block_z[b] = ztot;
+  if (!grid_barrier(bar_counter, bar_gen, st)) return;
+
+  // phase 3: ranks of childless slots, E, survivors in place
+  int zprefix, R;
+  block_sum_pair_int(block_z, G, b, &zprefix, &R);
+  {
+    int Z = zprefix + zexcl;
+    int prev = before0;
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+      const int i = i0 + k;
+      if (i < n) {
+        const bool zero = os[k] == prev;
+        const int e = prev - i + Z;
+        E[i] = e;
+        if ((i & ((1 << coarse_shift) - 1)) == 0) ecoarse[i >> coarse_shift] = e;
+        if (zero) slot[Z] = i;
+        else as[i] = i;
+        Z += zero;
+      }
+      prev = os[k];
+    }
+  }
+  if (!grid_barrier(bar_counter, bar_gen, st)) return;
+
+  // phase 4: childless slot of rank r <- ancestor a with E_a <= r < E_{a+1}
+  const int nc = ((n - 1) >> coarse_shift) + 1;
+  for (int i = threadIdx.x; i < nc; i += blockDim.x) s_coarse[i] = __ldcg(ecoarse + i);
+  __syncthreads();
+  for (int r = b * blockDim.x + threadIdx.x; r < R; r += G * blockDim.x) {
+    int clo = 0, chi = nc;
+    while (clo < chi) {
+      int mid = (clo + chi) >> 1;
+      if (s_coarse[mid] <= r) clo = mid + 1; else chi = mid;
+    }
+    int lo = (clo - 1) << coarse_shift;
+    int hi = min(n, lo + (1 << coarse_shift));
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      if (__ldcg(E + mid) <= r) lo = mid + 1; else hi = mid;
+    }
+    as[__ldcg(slot + r)] = lo - 1;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// systematic resampling in one thread-block cluster (n <= kClusterMaxN)
+//
+// Eight CTAs of 1024 threads each own a contiguous chunk of at most 8192
+// log-weights.  Everything between reading the log-weights and writing the
+// ancestors stays on chip: fixed-point weights and cumulative offspring in
+// registers, the extra-copy counts E and the childless slots in shared
+// memory; CTAs exchange their totals and search each other's E through
+// distributed shared memory, and synchronise with hardware cluster
+// barriers.  Global traffic is the log-weights in and the ancestors out.
+// ---------------------------------------------------------------------------
+namespace cg = cooperative_groups;
+constexpr int kClusterCtas = 8;
+constexpr int kClusterThreads = 1024;
+constexpr int kClusterItems = 8;
+constexpr int kClusterChunk = kClusterThreads * kClusterItems;
+constexpr int kClusterMaxN = kClusterCtas * kClusterChunk;
+
+template <int NT>
+__device__ __forceinline__ u128 block_exclusive_scan_u128_nt(u128 v, u128* total) {
+  __shared__ u128 wt[NT / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  u128 inc = v;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    u128 o = shfl_up_u128(inc, d);
+    if (lane >= d) inc = u128_add(inc, o);
+  }
+  if (lane == 31) wt[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    u128 t = lane < NT / 32 ? wt[lane] : u128_zero();
+#pragma unroll
+    for (int d = 1; d < NT / 32; d <<= 1) {
+      u128 o = shfl_up_u128(t, d);
+      if (lane >= d) t = u128_add(t, o);
+    }
+    if (lane < NT / 32) wt[lane] = t;
+  }
+  __syncthreads();
+  u128 r = u128_add(warp > 0 ? wt[warp - 1] : u128_zero(), u128_sub(inc, v));
+  *total = wt[NT / 32 - 1];
+  __syncthreads();
+  return r;
+}
+
+template <int NT>
+__device__ __forceinline__ int block_exclusive_scan_int_nt(int v, int* total) {
+  __shared__ int wt[NT / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int inc = v;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    int o = __shfl_up_sync(0xffffffffu, inc, d);
+    if (lane >= d) inc += o;
+  }
+  if (lane == 31) wt[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    int t = lane < NT / 32 ? wt[lane] : 0;
+#pragma unroll
+    for (int d = 1; d < NT / 32; d <<= 1) {
+      int o = __shfl_up_sync(0xffffffffu, t, d);
+      if (lane >= d) t += o;
+    }
+    if (lane < NT / 32) wt[lane] = t;
+  }
+  __syncthreads();
+  int r = (warp > 0 ? wt[warp - 1] : 0) + inc - v;
+  *total = wt[NT / 32 - 1];
+  __syncthreads();
+  return r;
+}
+
+struct ClusterShared {
+  u128 wtot;        // this CTA's weight total
+  int ztot;         // this CTA's childless count
+  int efirst;       // E at this CTA's first particle
+  int begin, len;   // this CTA's chunk
+};
+
+__global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kClusterThreads)
+k_systematic_cluster(const double* __restrict__ lw, int n, StepStats* st, const double* a_in, uint64_t seed,
+                     int step, int* Os_out, int* as, const int* gate) {
+  if (gate_closed(gate, st)) return;  // uniform over the cluster
+  cg::cluster_group cluster = cg::this_cluster();
+  const int c = (int)cluster.block_rank();
+  extern __shared__ int s_dyn[];
+  int* sE = s_dyn;                       // kClusterChunk
+  int* sslot = s_dyn + kClusterChunk;    // kClusterChunk
+  __shared__ ClusterShared sh;
+  __shared__ int s_last[kClusterThreads];
+  __shared__ u128 s_wtot[kClusterCtas];
+  __shared__ int s_misc[3 * kClusterCtas];
+
+  const int begin = (int)(((long long)c * n) / kClusterCtas);
+  const int end = (int)(((long long)(c + 1) * n) / kClusterCtas);
+  const int len = end - begin;
+  const int l0 = threadIdx.x * kClusterItems;  // local index of this thread's first item
+  const double mx = st->mx;
+  double a;
+  if (a_in) {
+    a = *a_in;
+  } else {
+    bpf_u32x4 r = bpf_draw(seed, 0u, (uint32_t)step, 0u, BPF_RNG_SYSTEMATIC);
+    a = bpf_u01d(r.v[0], r.v[1]);
+  }
+
+  // phase 1: fixed-point weights, kept in registers
+  unsigned long long q[kClusterItems];
+  u128 loc = u128_zero();
+#pragma unroll
+  for (int k = 0; k < kClusterItems; ++k) {
+    const int li = l0 + k;
+    q[k] = li < len ? weight_to_fixed(nanexp(__dsub_rn(__ldg(lw + begin + li), mx))) : 0ull;
+    u128 qq; qq.lo = q[k]; qq.hi = 0;
+    loc = u128_add(loc, qq);
+  }
+  u128 ctot;
+  const u128 texcl = block_exclusive_scan_u128_nt<kClusterThreads>(loc, &ctot);
+  if (threadIdx.x == 0) { sh.wtot = ctot; sh.begin = begin; sh.len = len; }
+  cluster.sync();
+
+  // phase 2: prefix of this CTA and the total W from the other CTAs' totals
+  if (threadIdx.x < kClusterCtas) {
+    ClusterShared* rs = cluster.map_shared_rank(&sh, threadIdx.x);
+    s_wtot[threadIdx.x] = rs->wtot;
+  }
+  __syncthreads();
+  u128 prefix = u128_zero(), total = u128_zero();
+#pragma unroll
+  for (int j = 0; j < kClusterCtas; ++j) {
+    total = u128_add(total, s_wtot[j]);
+    if (j < c) prefix = u128_add(prefix, s_wtot[j]);
+  }
+  const double W = u128_to_weight(total);
+  // SystematicResampler::cumulativeOffspring throws unless W > 0
+  // (share/src/bi/resampler/SystematicResampler.hpp:118-129)
+  if (!(W > 0.0)) {
+    if (c == 0 && threadIdx.x == 0) st->status = BPF_E_DEGENERATE;
+    cluster.sync();  // no CTA leaves while another may still read its shared memory
+    return;
+  }
+  const double nd = (double)n;
+  int os[kClusterItems];
+  {
+    u128 Q = u128_add(prefix, texcl);
+#pragma unroll
+    for (int k = 0; k < kClusterItems; ++k) {
+      u128 qq; qq.lo = q[k]; qq.hi = 0;
+      Q = u128_add(Q, qq);
+      os[k] = systematic_Os(u128_to_weight(Q), W, nd, a, n);
+    }
+  }
+  s_last[threadIdx.x] = os[kClusterItems - 1];
+  __syncthreads();
+  const int before0 = threadIdx.x > 0 ? s_last[threadIdx.x - 1]
+                                      : (begin == 0 ? 0 : systematic_Os(u128_to_weight(prefix), W, nd, a, n));
+  int zl = 0;
+  {
+    int prev = before0;
+#pragma unroll
+    for (int k = 0; k < kClusterItems; ++k) {
+      const int li = l0 + k;
+      if (li < len) {
+        zl += (os[k] == prev);
+        if (Os_out) Os_out[begin + li] = os[k];
+      }
+      prev = os[k];
+    }
+  }
+  int czt;
+  const int zexcl = block_exclusive_scan_int_nt<kClusterThreads>(zl, &czt);
+  if (threadIdx.x == 0) sh.ztot = czt;
+  cluster.sync();
+
+  // phase 3: ranks of childless slots, E, survivors in place
+  if (threadIdx.x < kClusterCtas) {
+    ClusterShared* rs = cluster.map_shared_rank(&sh, threadIdx.x);
+    s_misc[threadIdx.x] = rs->ztot;
+  }
+  __syncthreads();
+  int zprefix = 0;
+#pragma unroll
+  for (int j = 0; j < kClusterCtas; ++j) if (j < c) zprefix += s_misc[j];
+  {
+    int Z = zprefix + zexcl;
+    int prev = before0;
+#pragma unroll
+    for (int k = 0; k < kClusterItems; ++k) {
+      const int li = l0 + k;
+      if (li < len) {
+        const int i = begin + li;
+        const bool zero = os[k] == prev;
+        const int e = prev - i + Z;
+        sE[li] = e;
+        if (li == 0) sh.efirst = e;
+        if (zero) sslot[Z - zprefix] = i;
+        else as[i] = i;
+        Z += zero;
+      }
+      prev = os[k];
+    }
+  }
+  cluster.sync();
+
+  // phase 4: childless slot of rank r <- ancestor a with E_a <= r < E_{a+1},
+  // found by CTA (first E of each chunk) and then within that CTA's E
+  if (threadIdx.x < kClusterCtas) {
+    ClusterShared* rs = cluster.map_shared_rank(&sh, threadIdx.x);
+    s_misc[kClusterCtas + threadIdx.x] = rs->len > 0 ? rs->efirst : 0x7fffffff;
+    s_misc[2 * kClusterCtas + threadIdx.x] = rs->begin;
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < czt; j += kClusterThreads) {
+    const int r = zprefix + j;
+    int cc = 0;  // last CTA whose chunk starts with E <= r (CTA 0 starts with E = 0)
+#pragma unroll
+    for (int k = 1; k < kClusterCtas; ++k) if (s_misc[kClusterCtas + k] <= r) cc = k;
+    const int* rE = cluster.map_shared_rank(sE, cc);
+    const ClusterShared* rs = cluster.map_shared_rank(&sh, cc);
+    int lo = 0, hi = rs->len;
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      if (rE[mid] <= r) lo = mid + 1; else hi = mid;
+    }
+    as[sslot[j]] = s_misc[2 * kClusterCtas + cc] + lo - 1;
+  }
+  cluster.sync();  // keep this CTA's shared memory alive until every search is done
+}
+
 // ---------------------------------------------------------------------------
 // cumulative offspring from offspring counts o[] (Metropolis) or from sorted
 // ancestors (multinomial), with childless counts per tile
@@ -838,6 +1215,7 @@ static inline size_t fill_smem(int n, int max_entries = kMaxCoarse) {
 constexpr int kMaxCoarseCoop = 8192;
 
 static int launch_systematic_coop(const ResampleArgs& a, ResampleScratch& s, int* Os, cudaStream_t st);
+static int launch_systematic_cluster(const ResampleArgs& a, ResampleScratch& s, int* Os, cudaStream_t st);
 
 static inline int grid_stride_blocks(int n) {
   int b = (n + kBlock - 1) / kBlock;
@@ -857,7 +1235,7 @@ int launch_resample(const ResampleArgs& a, ResampleScratch& s, cudaStream_t st) 
   switch (a.kind) {
     case BPF_RESAMPLER_SYSTEMATIC: {
       if (a.permute) {
-        int rc = launch_systematic_coop(a, s, Os, st);
+        int rc = launch_systematic_coop(a, s, a.Os_out, st);
         if (rc != BPF_E_INVALID) return rc;  // BPF_E_INVALID: cooperative launch unavailable, use the passes
       }
       k_weight_tile_sums<<<T, kBlock, 0, st>>>(a.lw, n, s.stats, s.tile_sum, s.tile_prefix, 0, nullptr,
@@ -920,7 +1298,7 @@ int launch_resample(const ResampleArgs& a, ResampleScratch& s, cudaStream_t st) 
 // Cooperative launch of k_systematic_coop over at most as many blocks as the
 // GPU holds at once (and at most one per tile).  Returns BPF_E_INVALID when a
 // cooperative launch is not possible, so the caller can run the passes.
-static int launch_systematic_coop(const ResampleArgs& a, ResampleScratch& s, int* Os, cudaStream_t st) {
+static int launch_systematic_coop(const ResampleArgs& a, ResampleScratch& s, int* Os_out, cudaStream_t st) {
   static int coop_supported = -1, sms = 0;
   int dev = 0;
   BPF_TRY(cudaGetDevice(&dev));
@@ -930,18 +1308,20 @@ static int launch_systematic_coop(const ResampleArgs& a, ResampleScratch& s, int
   }
   if (!coop_supported) return BPF_E_INVALID;
   const int n = a.n;
-  const int sh = coarse_shift(n, kMaxCoarseCoop);
+  int sh = coarse_shift(n, kMaxCoarseCoop);
   const size_t smem = fill_smem(n, kMaxCoarseCoop);
-  // resident blocks per SM, cached per shared-memory size (the launch is on
-  // every filter step)
+  // resident blocks per SM of each variant, cached per shared-memory size
+  // (the launch is on every filter step)
   static size_t cached_smem = (size_t)-1;
-  static int per_sm = 0;
+  static int per_sm = 0, per_sm1 = 0;
   if (smem != cached_smem) {
     BPF_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_systematic_coop, kBlock, smem));
+    BPF_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm1, k_systematic_coop1, kBlock, smem));
     cached_smem = smem;
   }
   const int T = ntiles(n);
-  int G = sms * per_sm;
+  const bool one_tile = T <= sms * per_sm1;
+  int G = one_tile ? T : sms * per_sm;
   if (G > T) G = T;
   if (G < 1) return BPF_E_INVALID;
   const double* lw = a.lw;
@@ -959,10 +1339,39 @@ static int launch_systematic_coop(const ResampleArgs& a, ResampleScratch& s, int
   unsigned* bg = s.counters + 9;
   const int* gate = a.gate;
   int nn = n;
-  void* args[] = {(void*)&lw, (void*)&nn, (void*)&stats, (void*)&a_in, (void*)&seed, (void*)&step, (void*)&Os,
-                  (void*)&as, (void*)&E, (void*)&ec, (void*)&sh, (void*)&slot, (void*)&bw, (void*)&bz,
-                  (void*)&bc, (void*)&bg, (void*)&gate};
-  BPF_TRY(cudaLaunchCooperativeKernel((const void*)k_systematic_coop, dim3(G), dim3(kBlock), args, smem, st));
+  int* Os = Os_out ? Os_out : s.Os;  // the multi-tile variant keeps Os in global memory
+  if (one_tile) {
+    int* Oo = Os_out;
+    void* args[] = {(void*)&lw, (void*)&nn, (void*)&stats, (void*)&a_in, (void*)&seed, (void*)&step, (void*)&Oo,
+                    (void*)&as, (void*)&E, (void*)&ec, (void*)&sh, (void*)&slot, (void*)&bw, (void*)&bz,
+                    (void*)&bc, (void*)&bg, (void*)&gate};
+    BPF_TRY(cudaLaunchCooperativeKernel((const void*)k_systematic_coop1, dim3(G), dim3(kBlock), args, smem, st));
+  } else {
+    void* args[] = {(void*)&lw, (void*)&nn, (void*)&stats, (void*)&a_in, (void*)&seed, (void*)&step, (void*)&Os,
+                    (void*)&as, (void*)&E, (void*)&ec, (void*)&sh, (void*)&slot, (void*)&bw, (void*)&bz,
+                    (void*)&bc, (void*)&bg, (void*)&gate};
+    BPF_TRY(cudaLaunchCooperativeKernel((const void*)k_systematic_coop, dim3(G), dim3(kBlock), args, smem, st));
+  }
+  return BPF_OK;
+}
+
+// One cluster of kClusterCtas CTAs; returns BPF_E_INVALID when the device
+// cannot launch clusters, so the caller can use another path.
+static int launch_systematic_cluster(const ResampleArgs& a, ResampleScratch& s, int* Os, cudaStream_t st) {
+  static int checked = 0, ok = 0;
+  const size_t smem = 2 * (size_t)kClusterChunk * sizeof(int);
+  if (!checked) {
+    int dev = 0, cl = 0;
+    BPF_TRY(cudaGetDevice(&dev));
+    BPF_TRY(cudaDeviceGetAttribute(&cl, cudaDevAttrClusterLaunch, dev));
+    ok = cl && cudaFuncSetAttribute(k_systematic_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem) == cudaSuccess;
+    checked = 1;
+  }
+  if (!ok) return BPF_E_INVALID;
+  k_systematic_cluster<<<kClusterCtas, kClusterThreads, smem, st>>>(a.lw, a.n, s.stats, a.uniforms, a.seed, a.step,
+                                                                    Os, a.as, a.gate);
+  BPF_TRY(cudaGetLastError());
   return BPF_OK;
 }
 
