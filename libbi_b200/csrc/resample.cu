@@ -118,6 +118,50 @@ __device__ __forceinline__ void load_blocked(const double* __restrict__ lw, int 
 
 __device__ __forceinline__ int ntiles_dev(int n) { return (n + kTile - 1) / kTile; }
 
+__device__ __forceinline__ int block_max_int(int v) {
+  __shared__ int wm[kBlock / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, d));
+  if (lane == 0) wm[warp] = v;
+  __syncthreads();
+  int r = lane < kBlock / 32 ? wm[lane] : 0;
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) r = max(r, __shfl_xor_sync(0xffffffffu, r, d));
+  __syncthreads();
+  return r;
+}
+
+// Block-wide exclusive max-scan of non-negative ints (identity 0).
+__device__ __forceinline__ int block_exclusive_scan_max_int(int v, int* total) {
+  __shared__ int wt[kBlock / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int inc = v;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    int o = __shfl_up_sync(0xffffffffu, inc, d);
+    if (lane >= d) inc = max(inc, o);
+  }
+  int exc = __shfl_up_sync(0xffffffffu, inc, 1);
+  if (lane == 0) exc = 0;
+  if (lane == 31) wt[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    int t = lane < kBlock / 32 ? wt[lane] : 0;
+#pragma unroll
+    for (int d = 1; d < kBlock / 32; d <<= 1) {
+      int o = __shfl_up_sync(0xffffffffu, t, d);
+      if (lane >= d) t = max(t, o);
+    }
+    if (lane < kBlock / 32) wt[lane] = t;
+  }
+  __syncthreads();
+  const int r = max(warp > 0 ? wt[warp - 1] : 0, exc);
+  *total = wt[kBlock / 32 - 1];
+  __syncthreads();
+  return r;
+}
+
 __device__ __forceinline__ bool gate_closed(const int* gate, const StepStats* st) {
   if (gate != nullptr && *gate == 0) return true;
   return st->status != BPF_OK;
@@ -336,10 +380,9 @@ __device__ __forceinline__ int block_sum_int_from_global(const int* a, int count
 
 __global__ void __launch_bounds__(kBlock)
 k_systematic_coop(const double* __restrict__ lw, int n, StepStats* st, const double* a_in, uint64_t seed, int step,
-                  int* Os, int* as, int* E, int* ecoarse, int coarse_shift, int* slot,
-                  u128* block_w, int* block_z, unsigned* bar_counter, unsigned* bar_gen, const int* gate) {
+                  int* Os, int* as, int* marks, int* slot, u128* block_w, int* block_z, int* block_m,
+                  unsigned* bar_counter, unsigned* bar_gen, const int* gate) {
   if (gate_closed(gate, st)) return;
-  extern __shared__ int s_coarse[];
   __shared__ int s_prev_os;
   const int G = gridDim.x, b = blockIdx.x;
   const int T = ntiles_dev(n);
@@ -416,6 +459,7 @@ k_systematic_coop(const double* __restrict__ lw, int n, StepStats* st, const dou
     for (int k = 0; k < kItems; ++k) {
       if (i0 + k < n) {
         Os[i0 + k] = os[k];
+        marks[i0 + k] = 0;
         zeros += (os[k] == prev);
       }
       prev = os[k];
@@ -451,9 +495,8 @@ k_systematic_coop(const double* __restrict__ lw, int n, StepStats* st, const dou
       const int i = i0 + k;
       const int before = (k == 0 ? prev : os[k - 1]);
       if (i < n) {
-        const int e = before - i + Z;
-        E[i] = e;
-        if ((i & ((1 << coarse_shift) - 1)) == 0) ecoarse[i >> coarse_shift] = e;
+        // the first further copy of i (if any) has rank E_i = Os_{i-1} - i + Z_i
+        if (os[k] - before >= 2) marks[before - i + Z] = i + 1;
         if (z[k]) slot[Z] = i;
         else as[i] = i;
       }
@@ -463,23 +506,40 @@ k_systematic_coop(const double* __restrict__ lw, int n, StepStats* st, const dou
   }
   if (!grid_barrier(bar_counter, bar_gen, st)) return;
 
-  // phase 4: childless slot of rank r <- ancestor a with E_a <= r < E_{a+1}
-  const int nc = ((n - 1) >> coarse_shift) + 1;
-  for (int i = threadIdx.x; i < nc; i += blockDim.x) s_coarse[i] = __ldcg(ecoarse + i);
-  __syncthreads();
-  for (int r = b * blockDim.x + threadIdx.x; r < R; r += G * blockDim.x) {
-    int clo = 0, chi = nc;
-    while (clo < chi) {
-      int mid = (clo + chi) >> 1;
-      if (s_coarse[mid] <= r) clo = mid + 1; else chi = mid;
+  // phase 4: the ancestor of rank r is the last a whose first further copy
+  // has rank <= r, i.e. the running maximum of the marks up to r (load
+  // balanced however the copies are distributed)
+  const int TR = (R + kTile - 1) / kTile;
+  const int rb0 = (int)(((long long)b * TR) / G), rb1 = (int)(((long long)(b + 1) * TR) / G);
+  int mloc = 0;
+  for (int t = rb0; t < rb1; ++t) {
+    const int r0 = t * kTile + threadIdx.x * kItems;
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) if (r0 + k < R) mloc = max(mloc, __ldcg(marks + r0 + k));
+  }
+  const int bmax = block_max_int(mloc);
+  if (threadIdx.x == 0) block_m[b] = bmax;
+  if (!grid_barrier(bar_counter, bar_gen, st)) return;
+  int mcarry = 0;
+  for (int j = threadIdx.x; j < b; j += blockDim.x) mcarry = max(mcarry, __ldcg(block_m + j));
+  mcarry = block_max_int(mcarry);
+  for (int t = rb0; t < rb1; ++t) {
+    const int r0 = t * kTile + threadIdx.x * kItems;
+    int m[kItems];
+    int run = 0;
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+      m[k] = (r0 + k < R) ? __ldcg(marks + r0 + k) : 0;
+      run = max(run, m[k]);
     }
-    int lo = (clo - 1) << coarse_shift;
-    int hi = min(n, lo + (1 << coarse_shift));
-    while (lo < hi) {
-      int mid = (lo + hi) >> 1;
-      if (__ldcg(E + mid) <= r) lo = mid + 1; else hi = mid;
+    int tmax;
+    int ex = max(mcarry, block_exclusive_scan_max_int(run, &tmax));
+#pragma unroll
+    for (int k = 0; k < kItems; ++k) {
+      ex = max(ex, m[k]);
+      if (r0 + k < R) as[__ldcg(slot + r0 + k)] = ex - 1;
     }
-    as[__ldcg(slot + r)] = lo - 1;
+    mcarry = max(mcarry, tmax);
   }
 }
 
@@ -1315,7 +1375,7 @@ static int launch_systematic_coop(const ResampleArgs& a, ResampleScratch& s, int
   static size_t cached_smem = (size_t)-1;
   static int per_sm = 0, per_sm1 = 0;
   if (smem != cached_smem) {
-    BPF_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_systematic_coop, kBlock, smem));
+    BPF_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_systematic_coop, kBlock, 0));
     BPF_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm1, k_systematic_coop1, kBlock, smem));
     cached_smem = smem;
   }
@@ -1347,10 +1407,12 @@ static int launch_systematic_coop(const ResampleArgs& a, ResampleScratch& s, int
                     (void*)&bc, (void*)&bg, (void*)&gate};
     BPF_TRY(cudaLaunchCooperativeKernel((const void*)k_systematic_coop1, dim3(G), dim3(kBlock), args, smem, st));
   } else {
+    int* marks = s.o;     // n ints
+    int* bm = s.icount;   // G <= T block maxima
     void* args[] = {(void*)&lw, (void*)&nn, (void*)&stats, (void*)&a_in, (void*)&seed, (void*)&step, (void*)&Os,
-                    (void*)&as, (void*)&E, (void*)&ec, (void*)&sh, (void*)&slot, (void*)&bw, (void*)&bz,
+                    (void*)&as, (void*)&marks, (void*)&slot, (void*)&bw, (void*)&bz, (void*)&bm,
                     (void*)&bc, (void*)&bg, (void*)&gate};
-    BPF_TRY(cudaLaunchCooperativeKernel((const void*)k_systematic_coop, dim3(G), dim3(kBlock), args, smem, st));
+    BPF_TRY(cudaLaunchCooperativeKernel((const void*)k_systematic_coop, dim3(G), dim3(kBlock), args, 0, st));
   }
   return BPF_OK;
 }

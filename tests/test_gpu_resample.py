@@ -167,3 +167,25 @@ def test_gather_rows(cuda, oracle):
         want = np.zeros_like(X)
         oracle.L.orc_gather(as_.ctypes.data, X.ctypes.data, want.ctypes.data, n, d, ld, X.itemsize)
         np.testing.assert_array_equal(Y.cpu().numpy()[:, :n], want[:, :n])
+
+
+@pytest.mark.parametrize("n", [700001, 1300000])
+def test_systematic_multi_tile_matches_oracle(cuda, oracle, n):
+    """Sizes beyond one 512-tile per resident block take the multi-tile
+    cooperative kernel; ancestors must still equal the oracle's."""
+    import torch
+    from libbi_b200 import SystematicResampler
+
+    rng = np.random.default_rng(n)
+    lw = rng.standard_normal(n) * 3.0
+    a = rng.random(1)
+    R = SystematicResampler(max_n=n)
+    perm, Os = R.ancestors(_t(lw, torch.float64), _t(a, torch.float64), permute=True, with_offspring=True)
+    rc, _, Os_o, perm_o = oracle.systematic(lw, a[0], permute=True)
+    assert rc == 0
+    assert _near_tie_ok(oracle, lw, a[0], Os.cpu().numpy(), Os_o)
+    np.testing.assert_array_equal(perm.cpu().numpy(), perm_o)
+    ess, lW = R.reduce(_t(lw, torch.float64))
+    ess_o, lW_o = oracle.ess_reduce(lw)
+    np.testing.assert_allclose([ess, lW], [ess_o, lW_o], rtol=1e-11)
+    R.close()
