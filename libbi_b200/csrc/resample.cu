@@ -236,9 +236,16 @@ k_weight_tile_sums(const double* __restrict__ lw, int n, StepStats* st,
 // ---------------------------------------------------------------------------
 // Os_i = min(n, int(Ws_i / W * n + a)): resample_cumulative_offspring,
 // share/src/bi/resampler/SystematicResampler.hpp:47-50, evaluated as three
-// rounded FP64 operations in that order and truncated.
-__device__ __forceinline__ int systematic_Os(double Ws, double W, double nd, double a, int n) {
-  double r = __dadd_rn(__dmul_rn(__ddiv_rn(Ws, W), nd), a);
+// rounded FP64 operations in that order and truncated.  The quotient Ws/W is
+// formed as q0 = Ws*y, r = fma(-q0, W, Ws), q = fma(r, y, q0) with y the
+// correctly rounded 1/W, which equals the IEEE quotient (Markstein).
+__device__ __forceinline__ double quotient(double Ws, double W, double y) {
+  const double q0 = __dmul_rn(Ws, y);
+  return __fma_rn(__fma_rn(-q0, W, Ws), y, q0);
+}
+
+__device__ __forceinline__ int systematic_Os(double Ws, double W, double y, double nd, double a, int n) {
+  double r = __dadd_rn(__dmul_rn(quotient(Ws, W, y), nd), a);
   int o = __double2int_rz(r);
   return o < n ? o : n;
 }
@@ -261,6 +268,7 @@ k_systematic_offspring(const double* __restrict__ lw, int n, StepStats* st,
     a = bpf_u01d(r.v[0], r.v[1]);
   }
   const double W = u128_to_weight(tile_prefix[T]);
+  const double yW = __ddiv_rn(1.0, W);
   const double nd = (double)n;
 
   double v[kItems];
@@ -280,7 +288,7 @@ k_systematic_offspring(const double* __restrict__ lw, int n, StepStats* st,
   for (int k = 0; k < kItems; ++k) {
     u128 qq; qq.lo = q[k]; qq.hi = 0;
     Q = u128_add(Q, qq);
-    os[k] = systematic_Os(u128_to_weight(Q), W, nd, a, n);
+    os[k] = systematic_Os(u128_to_weight(Q), W, yW, nd, a, n);
   }
   s_last[threadIdx.x] = os[kItems - 1];
   __syncthreads();
@@ -288,7 +296,7 @@ k_systematic_offspring(const double* __restrict__ lw, int n, StepStats* st,
   if (threadIdx.x > 0) {
     prev = s_last[threadIdx.x - 1];
   } else {
-    prev = t == 0 ? 0 : systematic_Os(u128_to_weight(tile_prefix[t]), W, nd, a, n);
+    prev = t == 0 ? 0 : systematic_Os(u128_to_weight(tile_prefix[t]), W, yW, nd, a, n);
   }
   int zeros = 0;
 #pragma unroll
@@ -356,6 +364,22 @@ __device__ __forceinline__ bool grid_barrier(unsigned* counter, unsigned* gen, S
   return s_ok != 0;
 }
 
+template <int IT>
+__device__ __forceinline__ void load_blocked_n(const double* __restrict__ lw, int i0, int n, double (&v)[IT]) {
+  if (i0 + IT <= n && ((reinterpret_cast<uintptr_t>(lw + i0) & 15) == 0)) {
+    const double2* p = reinterpret_cast<const double2*>(lw + i0);
+#pragma unroll
+    for (int k = 0; k < IT / 2; ++k) {
+      double2 t = __ldg(p + k);
+      v[2 * k] = t.x;
+      v[2 * k + 1] = t.y;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < IT; ++k) v[k] = (i0 + k < n) ? __ldg(lw + i0 + k) : NAN;
+  }
+}
+
 __device__ __forceinline__ void load_blocked_cg(const double* __restrict__ lw, int i0, int n, double v[kItems]) {
 #pragma unroll
   for (int k = 0; k < kItems; ++k) v[k] = (i0 + k < n) ? lw[i0 + k] : NAN;
@@ -378,14 +402,16 @@ __device__ __forceinline__ int block_sum_int_from_global(const int* a, int count
   return tot;
 }
 
+template <int IT>
 __global__ void __launch_bounds__(kBlock)
 k_systematic_coop(const double* __restrict__ lw, int n, StepStats* st, const double* a_in, uint64_t seed, int step,
-                  int* Os, int* as, int* marks, int* slot, u128* block_w, int* block_z, int* block_m,
+                  int* Os, int* as, int* marks, int* slot, unsigned long long* qbuf, u128* block_w, int* block_z, int* block_m,
                   unsigned* bar_counter, unsigned* bar_gen, const int* gate) {
   if (gate_closed(gate, st)) return;
   __shared__ int s_prev_os;
   const int G = gridDim.x, b = blockIdx.x;
-  const int T = ntiles_dev(n);
+  constexpr int TL = kBlock * IT;
+  const int T = (n + TL - 1) / TL;
   const int tb0 = (int)(((long long)b * T) / G), tb1 = (int)(((long long)(b + 1) * T) / G);
   const double mx = st->mx;
   double a;
@@ -399,13 +425,14 @@ k_systematic_coop(const double* __restrict__ lw, int n, StepStats* st, const dou
   // phase 1: exact fixed-point weight total of this block's tiles
   u128 wsum = u128_zero();
   for (int t = tb0; t < tb1; ++t) {
-    const int i0 = t * kTile + threadIdx.x * kItems;
-    double v[kItems];
-    load_blocked(lw, i0, n, v);
+    const int i0 = t * TL + threadIdx.x * IT;
+    double v[IT];
+    load_blocked_n<IT>(lw, i0, n, v);
 #pragma unroll
-    for (int k = 0; k < kItems; ++k) {
+    for (int k = 0; k < IT; ++k) {
       if (i0 + k < n) {
         u128 q; q.lo = weight_to_fixed(nanexp(__dsub_rn(v[k], mx))); q.hi = 0;
+        qbuf[i0 + k] = q.lo;  // phase 2 reads these instead of recomputing the exp
         wsum = u128_add(wsum, q);
       }
     }
@@ -427,36 +454,35 @@ k_systematic_coop(const double* __restrict__ lw, int n, StepStats* st, const dou
     return;
   }
   const double nd = (double)n;
+  const double yW = __ddiv_rn(1.0, W);
   __shared__ int s_last[kBlock];
   u128 carry = prefix_b;
   int zeros = 0;
-  if (threadIdx.x == 0) s_prev_os = tb0 == 0 ? 0 : systematic_Os(u128_to_weight(prefix_b), W, nd, a, n);
+  if (threadIdx.x == 0) s_prev_os = tb0 == 0 ? 0 : systematic_Os(u128_to_weight(prefix_b), W, yW, nd, a, n);
   for (int t = tb0; t < tb1; ++t) {
-    const int i0 = t * kTile + threadIdx.x * kItems;
-    double v[kItems];
-    load_blocked(lw, i0, n, v);
-    unsigned long long q[kItems];
+    const int i0 = t * TL + threadIdx.x * IT;
+    unsigned long long q[IT];
     u128 loc = u128_zero();
 #pragma unroll
-    for (int k = 0; k < kItems; ++k) {
-      q[k] = (i0 + k < n) ? weight_to_fixed(nanexp(__dsub_rn(v[k], mx))) : 0ull;
+    for (int k = 0; k < IT; ++k) {
+      q[k] = (i0 + k < n) ? __ldcg(qbuf + i0 + k) : 0ull;
       u128 qq; qq.lo = q[k]; qq.hi = 0;
       loc = u128_add(loc, qq);
     }
     u128 ttot;
     u128 Q = u128_add(carry, block_exclusive_scan_u128(loc, &ttot));
-    int os[kItems];
+    int os[IT];
 #pragma unroll
-    for (int k = 0; k < kItems; ++k) {
+    for (int k = 0; k < IT; ++k) {
       u128 qq; qq.lo = q[k]; qq.hi = 0;
       Q = u128_add(Q, qq);
-      os[k] = systematic_Os(u128_to_weight(Q), W, nd, a, n);
+      os[k] = systematic_Os(u128_to_weight(Q), W, yW, nd, a, n);
     }
-    s_last[threadIdx.x] = os[kItems - 1];
+    s_last[threadIdx.x] = os[IT - 1];
     __syncthreads();
     int prev = threadIdx.x > 0 ? s_last[threadIdx.x - 1] : s_prev_os;
 #pragma unroll
-    for (int k = 0; k < kItems; ++k) {
+    for (int k = 0; k < IT; ++k) {
       if (i0 + k < n) {
         Os[i0 + k] = os[k];
         marks[i0 + k] = 0;
@@ -465,7 +491,7 @@ k_systematic_coop(const double* __restrict__ lw, int n, StepStats* st, const dou
       prev = os[k];
     }
     __syncthreads();
-    if (threadIdx.x == kBlock - 1) s_prev_os = os[kItems - 1];
+    if (threadIdx.x == kBlock - 1) s_prev_os = os[IT - 1];
     carry = u128_add(carry, ttot);
     __syncthreads();
   }
@@ -478,12 +504,12 @@ k_systematic_coop(const double* __restrict__ lw, int n, StepStats* st, const dou
   int zcarry = block_sum_int_from_global(block_z, b);
   const int R = block_sum_int_from_global(block_z, G);
   for (int t = tb0; t < tb1; ++t) {
-    const int i0 = t * kTile + threadIdx.x * kItems;
+    const int i0 = t * TL + threadIdx.x * IT;
     int prev = i0 > 0 && i0 - 1 < n ? __ldcg(Os + i0 - 1) : 0;
-    int os[kItems], z[kItems];
+    int os[IT], z[IT];
     int loc = 0;
 #pragma unroll
-    for (int k = 0; k < kItems; ++k) {
+    for (int k = 0; k < IT; ++k) {
       os[k] = (i0 + k < n) ? __ldcg(Os + i0 + k) : prev;
       z[k] = (i0 + k < n) && (os[k] == (k == 0 ? prev : os[k - 1]));
       loc += z[k];
@@ -491,7 +517,7 @@ k_systematic_coop(const double* __restrict__ lw, int n, StepStats* st, const dou
     int ttot;
     int Z = zcarry + block_exclusive_scan_int(loc, &ttot);
 #pragma unroll
-    for (int k = 0; k < kItems; ++k) {
+    for (int k = 0; k < IT; ++k) {
       const int i = i0 + k;
       const int before = (k == 0 ? prev : os[k - 1]);
       if (i < n) {
@@ -509,13 +535,13 @@ k_systematic_coop(const double* __restrict__ lw, int n, StepStats* st, const dou
   // phase 4: the ancestor of rank r is the last a whose first further copy
   // has rank <= r, i.e. the running maximum of the marks up to r (load
   // balanced however the copies are distributed)
-  const int TR = (R + kTile - 1) / kTile;
+  const int TR = (R + TL - 1) / TL;
   const int rb0 = (int)(((long long)b * TR) / G), rb1 = (int)(((long long)(b + 1) * TR) / G);
   int mloc = 0;
   for (int t = rb0; t < rb1; ++t) {
-    const int r0 = t * kTile + threadIdx.x * kItems;
+    const int r0 = t * TL + threadIdx.x * IT;
 #pragma unroll
-    for (int k = 0; k < kItems; ++k) if (r0 + k < R) mloc = max(mloc, __ldcg(marks + r0 + k));
+    for (int k = 0; k < IT; ++k) if (r0 + k < R) mloc = max(mloc, __ldcg(marks + r0 + k));
   }
   const int bmax = block_max_int(mloc);
   if (threadIdx.x == 0) block_m[b] = bmax;
@@ -524,18 +550,18 @@ k_systematic_coop(const double* __restrict__ lw, int n, StepStats* st, const dou
   for (int j = threadIdx.x; j < b; j += blockDim.x) mcarry = max(mcarry, __ldcg(block_m + j));
   mcarry = block_max_int(mcarry);
   for (int t = rb0; t < rb1; ++t) {
-    const int r0 = t * kTile + threadIdx.x * kItems;
-    int m[kItems];
+    const int r0 = t * TL + threadIdx.x * IT;
+    int m[IT];
     int run = 0;
 #pragma unroll
-    for (int k = 0; k < kItems; ++k) {
+    for (int k = 0; k < IT; ++k) {
       m[k] = (r0 + k < R) ? __ldcg(marks + r0 + k) : 0;
       run = max(run, m[k]);
     }
     int tmax;
     int ex = max(mcarry, block_exclusive_scan_max_int(run, &tmax));
 #pragma unroll
-    for (int k = 0; k < kItems; ++k) {
+    for (int k = 0; k < IT; ++k) {
       ex = max(ex, m[k]);
       if (r0 + k < R) as[__ldcg(slot + r0 + k)] = ex - 1;
     }
@@ -613,6 +639,7 @@ k_systematic_coop1(const double* __restrict__ lw, int n, StepStats* st, const do
     return;
   }
   const double nd = (double)n;
+  const double yW = __ddiv_rn(1.0, W);
   int os[kItems];
   {
     u128 Q = u128_add(prefix, texcl);
@@ -620,13 +647,13 @@ k_systematic_coop1(const double* __restrict__ lw, int n, StepStats* st, const do
     for (int k = 0; k < kItems; ++k) {
       u128 qq; qq.lo = q[k]; qq.hi = 0;
       Q = u128_add(Q, qq);
-      os[k] = systematic_Os(u128_to_weight(Q), W, nd, a, n);
+      os[k] = systematic_Os(u128_to_weight(Q), W, yW, nd, a, n);
     }
   }
   s_last[threadIdx.x] = os[kItems - 1];
   __syncthreads();
   const int before0 = threadIdx.x > 0 ? s_last[threadIdx.x - 1]
-                                      : (b == 0 ? 0 : systematic_Os(u128_to_weight(prefix), W, nd, a, n));
+                                      : (b == 0 ? 0 : systematic_Os(u128_to_weight(prefix), W, yW, nd, a, n));
   int zl = 0;
   {
     int prev = before0;
@@ -831,6 +858,7 @@ k_systematic_cluster(const double* __restrict__ lw, int n, StepStats* st, const 
     return;
   }
   const double nd = (double)n;
+  const double yW = __ddiv_rn(1.0, W);
   int os[kClusterItems];
   {
     u128 Q = u128_add(prefix, texcl);
@@ -838,13 +866,13 @@ k_systematic_cluster(const double* __restrict__ lw, int n, StepStats* st, const 
     for (int k = 0; k < kClusterItems; ++k) {
       u128 qq; qq.lo = q[k]; qq.hi = 0;
       Q = u128_add(Q, qq);
-      os[k] = systematic_Os(u128_to_weight(Q), W, nd, a, n);
+      os[k] = systematic_Os(u128_to_weight(Q), W, yW, nd, a, n);
     }
   }
   s_last[threadIdx.x] = os[kClusterItems - 1];
   __syncthreads();
   const int before0 = threadIdx.x > 0 ? s_last[threadIdx.x - 1]
-                                      : (begin == 0 ? 0 : systematic_Os(u128_to_weight(prefix), W, nd, a, n));
+                                      : (begin == 0 ? 0 : systematic_Os(u128_to_weight(prefix), W, yW, nd, a, n));
   int zl = 0;
   {
     int prev = before0;
@@ -1273,6 +1301,8 @@ static inline size_t fill_smem(int n, int max_entries = kMaxCoarse) {
 // the cooperative kernel keeps its coarse index within 32 KB, leaving room
 // for its static shared memory under the default 48 KB limit
 constexpr int kMaxCoarseCoop = 8192;
+// items per thread of the multi-tile cooperative kernel (tiles of 512)
+constexpr int kCoopItems = 2;
 
 static int launch_systematic_coop(const ResampleArgs& a, ResampleScratch& s, int* Os, cudaStream_t st);
 static int launch_systematic_cluster(const ResampleArgs& a, ResampleScratch& s, int* Os, cudaStream_t st);
@@ -1375,15 +1405,18 @@ static int launch_systematic_coop(const ResampleArgs& a, ResampleScratch& s, int
   static size_t cached_smem = (size_t)-1;
   static int per_sm = 0, per_sm1 = 0;
   if (smem != cached_smem) {
-    BPF_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_systematic_coop, kBlock, 0));
+    BPF_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_systematic_coop<kCoopItems>, kBlock, 0));
     BPF_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm1, k_systematic_coop1, kBlock, smem));
     cached_smem = smem;
   }
   const int T = ntiles(n);
   const bool one_tile = T <= sms * per_sm1;
+  const int T8 = (n + kBlock * kCoopItems - 1) / (kBlock * kCoopItems);  // tiles of the multi-tile variant
   int G = one_tile ? T : sms * per_sm;
-  if (G > T) G = T;
+  if (G > (one_tile ? T : T8)) G = one_tile ? T : T8;
   if (G < 1) return BPF_E_INVALID;
+  // the multi-tile variant also needs marks, stored weights and block maxima
+  if (!one_tile && (s.o == nullptr || s.Ws == nullptr || s.icount == nullptr)) return BPF_E_INVALID;
   const double* lw = a.lw;
   StepStats* stats = s.stats;
   const double* a_in = a.uniforms;
@@ -1409,10 +1442,12 @@ static int launch_systematic_coop(const ResampleArgs& a, ResampleScratch& s, int
   } else {
     int* marks = s.o;     // n ints
     int* bm = s.icount;   // G <= T block maxima
+    unsigned long long* qb = reinterpret_cast<unsigned long long*>(s.Ws);  // n fixed-point weights
     void* args[] = {(void*)&lw, (void*)&nn, (void*)&stats, (void*)&a_in, (void*)&seed, (void*)&step, (void*)&Os,
-                    (void*)&as, (void*)&marks, (void*)&slot, (void*)&bw, (void*)&bz, (void*)&bm,
+                    (void*)&as, (void*)&marks, (void*)&slot, (void*)&qb, (void*)&bw, (void*)&bz, (void*)&bm,
                     (void*)&bc, (void*)&bg, (void*)&gate};
-    BPF_TRY(cudaLaunchCooperativeKernel((const void*)k_systematic_coop, dim3(G), dim3(kBlock), args, 0, st));
+    BPF_TRY(cudaLaunchCooperativeKernel((const void*)k_systematic_coop<kCoopItems>, dim3(G), dim3(kBlock), args, 0,
+                                        st));
   }
   return BPF_OK;
 }
