@@ -49,6 +49,10 @@ TRANSITION_BYTES_PER_PARTICLE = 2 * DIM * 4 + 16
 # FP32 operations per particle-step of the fused transition (FMA = 2):
 # RK4 5 sub-steps x 40 components x 31 + noise add 2 x 40 + observation 6 x 40
 TRANSITION_FLOP_PER_PARTICLE = 5 * DIM * 31 + 2 * DIM + 6 * DIM
+# DRAM bytes (read + write) of one transition launch at this workload from an
+# ncu capture (profiles/k_l96_transition_l96_d40_n65536.md): 10.8 MB read,
+# nothing written back within the launch (the new state stays in L2)
+TRANSITION_DRAM_BYTES_PER_LAUNCH = 10_813_440 + 0
 
 
 def peaks():
@@ -171,9 +175,10 @@ def cpu_baseline(y, seconds: float = 12.0):
 def large_n_kernels(sizes=(1 << 22, 1 << 24), reps=5):
     """The memory-bound kernels at working sets beyond L2: log-weight
     reduction (ess_reduce), permuted systematic resampling and the ancestor
-    gather (40 FP32 components).  Device time from CUDA events around each
-    call (each call ends with a small device-to-host status read), L2 flushed
-    before every repetition; achieved GB/s counts algorithmic bytes:
+    gather (40 FP32 components).  Device time of the kernels from CUDA events
+    (for the resampler calls, the events the resampler records around its own
+    kernels), L2 flushed before every repetition; achieved GB/s counts
+    algorithmic bytes:
     reduce 8 B, resample 8 + 4 B (log-weight in, ancestor out), gather
     2*40*4 + 4 B per particle."""
     import torch
@@ -193,21 +198,28 @@ def large_n_kernels(sizes=(1 << 22, 1 << 24), reps=5):
         Y = torch.empty_like(X)
         as_ = R.ancestors(lw, a, permute=True)
 
-        def timed(fn):
+        def timed(fn, kernel_only):
+            # kernel_only: the resampler's own events around its kernels
+            # (the call's status reset and read-back excluded); otherwise
+            # events around the whole call, which enqueues one kernel
             ts = []
             for _ in range(reps):
                 flush.zero_()
                 s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                R.timing_read(reset=True)
                 s0.record()
                 fn()
                 s1.record()
                 torch.cuda.synchronize()
-                ts.append(s0.elapsed_time(s1) / 1e3)
+                ms, calls = R.timing_read(reset=True)
+                ts.append(ms / calls / 1e3 if kernel_only else s0.elapsed_time(s1) / 1e3)
             return min(ts)
 
-        t_red = timed(lambda: R.reduce(lw))
-        t_res = timed(lambda: R.ancestors(lw, a, permute=True))
-        t_gat = timed(lambda: (gather_rows(as_, X, Y, DIM, ld), torch.cuda.synchronize()))
+        R.timing(True)
+        t_red = timed(lambda: R.reduce(lw), True)
+        t_res = timed(lambda: R.ancestors(lw, a, permute=True), True)
+        t_gat = timed(lambda: gather_rows(as_, X, Y, DIM, ld), False)
+        R.timing(False)
         rows = {}
         for name, t, byt in (("ess_reduce", t_red, 8 * n), ("systematic_resample", t_res, 12 * n),
                              ("gather_rows_d40", t_gat, (2 * DIM * 4 + 4) * n)):
@@ -371,7 +383,9 @@ def main():
         "gpu_launches": LAUNCHES_PER_STEP * args.steps,
         "roofline": {"kernel": "k_l96_transition<float,40>", "bound": "hbm", "achieved": achieved,
                      "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_source": how,
-                     "traffic": None, "algorithmic_bytes_per_launch": bytes_launch,
+                     "traffic": TRANSITION_DRAM_BYTES_PER_LAUNCH,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch",
+                     "algorithmic_bytes_per_launch": bytes_launch,
                      "launch_ms": t_launch * 1e3,
                      "fp32": {"achieved_tflops": fp32_ach, "peak_tflops": fp32_peak,
                               "frac": fp32_ach / fp32_peak,

@@ -217,6 +217,15 @@ int bpf_logsumexp_reduce(bpf_resampler* r, const double* lw, int n, double* out)
 int bpf_resampler_ancestors(bpf_resampler* r, const double* lw, int n,
                             const double* uniforms, int permute, int* as, int* Os);
 
+/* Device timing of a resampler's compute kernels, the counterpart of
+ * bpf_timing_enable for the stand-alone primitives: when enabled, every
+ * bpf_ess_reduce, bpf_logsumexp_reduce and bpf_resampler_ancestors call
+ * records CUDA events around its kernels (not around the status reset or the
+ * read-back of the results), and bpf_resampler_timing_read returns the summed
+ * milliseconds and the number of timed calls since the last reset. */
+int bpf_resampler_timing_enable(bpf_resampler* r, int enable);
+int bpf_resampler_timing_read(bpf_resampler* r, int reset, double* ms, int* calls);
+
 /* gather_rows (share/src/bi/primitive/matrix_primitive.hpp:630-638,
  * share/src/bi/cuda/primitive/matrix_primitive_kernel.cuh:50-57), out of
  * place on device SoA buffers: Y[j*ld + i] = X[j*ld + as[i]], j < d, i < n.

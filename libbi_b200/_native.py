@@ -41,6 +41,7 @@ EXPORTS = (
     "bpf_logsumexp_reduce", "bpf_resampler_ancestors", "bpf_gather_rows",
     "bpf_snapshot_size", "bpf_snapshot", "bpf_restore", "bpf_version",
     "bpf_status_string", "bpf_timing_enable", "bpf_timing_read", "bpf_systematic_ancestors_static",
+    "bpf_resampler_timing_enable", "bpf_resampler_timing_read",
 )
 
 
@@ -105,6 +106,8 @@ def _declare(L):
         "bpf_restore": (c_int, [H, c_void_p, c_uint64]),
         "bpf_timing_enable": (c_int, [H, c_int]),
         "bpf_timing_read": (c_int, [H, c_int, POINTER(c_double), POINTER(c_double), POINTER(c_int)]),
+        "bpf_resampler_timing_enable": (c_int, [H, c_int]),
+        "bpf_resampler_timing_read": (c_int, [H, c_int, POINTER(c_double), POINTER(c_int)]),
         "bpf_systematic_ancestors_static": (c_int, [c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p,
                                                     c_void_p]),
         "bpf_version": (c_char_p, []),

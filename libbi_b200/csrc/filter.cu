@@ -44,6 +44,12 @@ struct bpf_resampler {
   int kind = 0, B = 0;
   cudaStream_t stream = nullptr;
   bpf::ResampleScratch rs;
+  // optional device timing of the compute kernels of each call (events
+  // after the status reset and before the read-back)
+  bool timing = false;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  double timed_ms = 0.0;
+  int timed_calls = 0;
 };
 
 namespace {
@@ -477,6 +483,8 @@ int bpf_resampler_create(int kind, int max_n, int metropolis_steps, void* stream
 int bpf_resampler_destroy(bpf_resampler* r) {
   if (!r) return BPF_OK;
   if (r->stream) cudaStreamSynchronize(r->stream); else cudaDeviceSynchronize();
+  for (cudaEvent_t e : r->ev)
+    if (e) cudaEventDestroy(e);
   bpf::scratch_free(r->rs);
   delete r;
   return BPF_OK;
@@ -488,9 +496,47 @@ static int reset_status(bpf_resampler* r) {
   return BPF_OK;
 }
 
+static int timing_begin(bpf_resampler* r) {
+  if (r->timing) BPF_TRY(cudaEventRecord(r->ev[0], r->stream));
+  return BPF_OK;
+}
+
+static int timing_end(bpf_resampler* r) {
+  if (r->timing) BPF_TRY(cudaEventRecord(r->ev[1], r->stream));
+  return BPF_OK;
+}
+
+// called after the stream has been synchronised
+static int timing_collect(bpf_resampler* r) {
+  if (!r->timing) return BPF_OK;
+  float ms = 0.0f;
+  BPF_TRY(cudaEventElapsedTime(&ms, r->ev[0], r->ev[1]));
+  r->timed_ms += ms;
+  r->timed_calls += 1;
+  return BPF_OK;
+}
+
 static int read_rs_stats(bpf_resampler* r, bpf::StepStats* s) {
   BPF_TRY(cudaMemcpyAsync(s, r->rs.stats, sizeof(*s), cudaMemcpyDeviceToHost, r->stream));
   BPF_TRY(cudaStreamSynchronize(r->stream));
+  return timing_collect(r);
+}
+
+int bpf_resampler_timing_enable(bpf_resampler* r, int enable) {
+  if (!r) return BPF_E_INVALID;
+  if (enable) {
+    for (cudaEvent_t& e : r->ev)
+      if (!e) BPF_TRY(cudaEventCreate(&e));
+  }
+  r->timing = enable != 0;
+  return BPF_OK;
+}
+
+int bpf_resampler_timing_read(bpf_resampler* r, int reset, double* ms, int* calls) {
+  if (!r) return BPF_E_INVALID;
+  if (ms) *ms = r->timed_ms;
+  if (calls) *calls = r->timed_calls;
+  if (reset) { r->timed_ms = 0.0; r->timed_calls = 0; }
   return BPF_OK;
 }
 
@@ -498,8 +544,10 @@ int bpf_ess_reduce(bpf_resampler* r, const double* lw, int n, double* lW, double
   if (!r || !lw || n <= 0 || n > r->rs.max_n) return BPF_E_INVALID;
   int rc = reset_status(r);
   if (rc) return rc;
+  if ((rc = timing_begin(r))) return rc;
   rc = bpf::launch_lw_reduce(lw, n, r->rs, r->stream);
   if (rc) return rc;
+  if ((rc = timing_end(r))) return rc;
   bpf::StepStats s;
   rc = read_rs_stats(r, &s);
   if (rc) return rc;
@@ -512,8 +560,10 @@ int bpf_logsumexp_reduce(bpf_resampler* r, const double* lw, int n, double* out)
   if (!r || !lw || n <= 0 || n > r->rs.max_n) return BPF_E_INVALID;
   int rc = reset_status(r);
   if (rc) return rc;
+  if ((rc = timing_begin(r))) return rc;
   rc = bpf::launch_logsumexp(lw, n, r->rs, r->stream);
   if (rc) return rc;
+  if ((rc = timing_end(r))) return rc;
   bpf::StepStats s;
   rc = read_rs_stats(r, &s);
   if (rc) return rc;
@@ -539,8 +589,10 @@ int bpf_resampler_ancestors(bpf_resampler* r, const double* lw, int n, const dou
   ra.Os_out = Os;
   ra.gate = nullptr;
   ra.max_known = false;
+  if ((rc = timing_begin(r))) return rc;
   rc = bpf::launch_resample(ra, r->rs, r->stream);
   if (rc) return rc;
+  if ((rc = timing_end(r))) return rc;
   bpf::StepStats s;
   rc = read_rs_stats(r, &s);
   if (rc) return rc;

@@ -169,6 +169,17 @@ class Resampler:
         except Exception:
             pass
 
+    def timing(self, enable: bool = True):
+        """Record CUDA events around the kernels of every later call."""
+        N.check(N.lib().bpf_resampler_timing_enable(self._h, int(enable)), "bpf_resampler_timing_enable")
+
+    def timing_read(self, reset: bool = True):
+        """(summed kernel milliseconds, timed calls) since the last reset."""
+        ms, calls = ctypes.c_double(), ctypes.c_int()
+        N.check(N.lib().bpf_resampler_timing_read(self._h, int(reset), ctypes.byref(ms), ctypes.byref(calls)),
+                "bpf_resampler_timing_read")
+        return ms.value, calls.value
+
     def reduce(self, lws):
         """ESS and lW = log mean exp(lws): Resampler::reduce -> ess_reduce."""
         lW, ess = ctypes.c_double(), ctypes.c_double()
