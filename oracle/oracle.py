@@ -1,7 +1,9 @@
 """ORACLE — test infrastructure only (tests/, the smoke check and the bench's
 CPU-baseline leg).  ctypes binding of the C restatement (bpf_oracle.c ->
-_build/liboracle.so) and of the reference's own resampler code compiled from
-its sources (ref/ref_resampler.cpp -> _ref/libbiref.so, when built)."""
+_build/liboracle.so) and of the reference's own code compiled from its
+sources, when built: the resampler code (ref/ref_resampler.cpp) and the host
+updaters on hand-rendered model classes (ref/model_l96.cpp, ref/model_pz.cpp)
+-> _ref/libbiref.so, and the L96 model with real = float -> _ref/libbiref_f32.so."""
 from __future__ import annotations
 
 import ctypes
@@ -14,6 +16,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libbiref.so")
+REF_F32_SO = os.path.join(HERE, "_ref", "libbiref_f32.so")
 REF_TREE = "/root/reference/share/src"
 
 
@@ -49,6 +52,7 @@ class Oracle:
                                      c_void_p, c_double, c_double, c_uint64, c_int, c_double]
         L.orc_filter.argtypes = [c_void_p, c_void_p, c_int, c_double, c_double, c_void_p, c_void_p, c_void_p,
                                  c_void_p, POINTER(c_double), c_void_p, c_void_p]
+        L.orc_noise_normals.argtypes = [c_uint64, ctypes.c_uint32, c_int, c_int, c_int, c_void_p]
         L.orc_simulate.argtypes = [c_void_p, c_uint64, c_int, c_double, c_double, c_void_p, c_void_p]
         self.L = L
 
@@ -139,6 +143,13 @@ class Oracle:
                                ctypes.byref(ll), _p(x), _p(lw))
         return dict(rc=rc, ll=ll.value, inc=inc, ess=ess, resampled=res, x=x, lw=lw)
 
+    def noise_normals(self, seed, p, step, n, f32):
+        """The n standard normals of particle p's process noise at step, in
+        the order the transition consumes them (include/bpf_philox.h)."""
+        z = np.zeros(n)
+        self.L.orc_noise_normals(c_uint64(seed), int(p), int(step), int(n), 0 if f32 else 1, _p(z))
+        return z
+
     def simulate(self, desc, seed, T, t0, dt):
         dtp = np.float32 if desc.precision == 0 else np.float64
         nobs = desc.dim if desc.kind == 1 else 1
@@ -208,3 +219,50 @@ class RefResampler:
         a = np.ascontiguousarray(as_, dtype=np.int32)
         self.L.ref_gather_rows(_p(a), _p(X), n, d)
         return X
+
+
+class RefModels:
+    """The reference's own host updaters (RK4IntegratorHost,
+    RK43IntegratorHost, StaticSamplerHost, StaticUpdaterHost,
+    SparseStaticLogDensityHost) on hand-rendered L96 (d = 40) and PZ model
+    classes (oracle/ref/model_l96.cpp, model_pz.cpp), draws from a tape of
+    standard normals.  f32 selects the L96 build with real = float."""
+
+    L96_DIM = 40
+
+    def __init__(self, f32: bool = False):
+        path = REF_F32_SO if f32 else REF_SO
+        if not os.path.exists(path):
+            raise OSError(f"reference build missing: {path}")
+        L = ctypes.CDLL(path)
+        sig = [c_void_p, c_int, c_void_p, c_double, c_double, c_void_p, c_void_p]
+        L.ref_l96_transition.argtypes = sig
+        if not f32:
+            L.ref_pz_transition.argtypes = sig
+        self.L = L
+        self.f32 = f32
+
+    def l96_transition(self, x, z, t1, t2, y=None, lp=None):
+        """x: (P, 40) particle-major state; z: (P, 40) standard normals in the
+        sampler's draw order; returns (x_out, lp_out)."""
+        x = np.ascontiguousarray(x, np.float64).copy()
+        P = x.shape[0]
+        z = np.ascontiguousarray(z, np.float64)
+        lp = np.zeros(P) if lp is None else np.ascontiguousarray(lp, np.float64).copy()
+        y = None if y is None else np.ascontiguousarray(y, np.float64)
+        rc = self.L.ref_l96_transition(_p(x), P, _p(z), float(t1), float(t2), _p(y), _p(lp))
+        if rc:
+            raise RuntimeError("reference L96 transition did not consume its draws exactly")
+        return x, lp
+
+    def pz_transition(self, x, z, t1, t2, y=None, lp=None):
+        """x: (P, 2) state (P, Z); z: P standard normals (the alpha draws)."""
+        x = np.ascontiguousarray(x, np.float64).copy()
+        P = x.shape[0]
+        z = np.ascontiguousarray(z, np.float64)
+        lp = np.zeros(P) if lp is None else np.ascontiguousarray(lp, np.float64).copy()
+        y = None if y is None else np.ascontiguousarray(np.atleast_1d(y), np.float64)
+        rc = self.L.ref_pz_transition(_p(x), P, _p(z), float(t1), float(t2), _p(y), _p(lp))
+        if rc:
+            raise RuntimeError("reference PZ transition did not consume its draws exactly")
+        return x, lp
