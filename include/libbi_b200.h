@@ -252,6 +252,62 @@ int bpf_gather_rows(const int* as, const void* X, void* Y, int n, int d, int ld,
 int bpf_systematic_ancestors_static(const double* lw, int n, const double* a, int permute, int* as, int* Os,
                                     void* stream);
 
+/* ---- batched filters --------------------------------------------------- */
+/* Many independent filters of one model advanced together: one launch per
+ * phase (resample, transition) for the whole batch, and bpf_filter_batch runs
+ * init + T steps as one captured CUDA graph.  The reference runs such filters
+ * one Filter<BootstrapPF>::filter at a time, e.g. per iteration of
+ * MarginalMH (share/src/bi/sampler/MarginalMH.hpp:230-271) or per parameter
+ * particle of MarginalSIR (share/src/bi/sampler/MarginalSIR.hpp:283-420).
+ * Filter f of a batch draws exactly what a single filter (bpf_create) with
+ * the same particle count, resampler, seed and theta draws, so it reproduces
+ * that filter's log-likelihood increments. */
+#define BPF_BATCH_MAX_PARTICLES 32768
+
+typedef struct {
+  int nparticles;        /* N of this filter, 1 .. BPF_BATCH_MAX_PARTICLES */
+  int resampler;         /* BPF_RESAMPLER_* */
+  int metropolis_steps;  /* B, Metropolis only */
+  uint64_t seed;
+  double theta[BPF_MAX_THETA];  /* this filter's model constants (bpf_model_desc.theta) */
+} bpf_batch_filter;
+
+typedef struct bpf_batch bpf_batch;
+
+/* model gives kind, dim, precision, integrator and h/atoler/rtoler shared by
+ * every filter; filters[nfilters] the per-filter settings; ess_rel as in
+ * bpf_config.  stream: cudaStream_t, or NULL for a library-owned blocking
+ * stream.  Draws the initial particles (bpf_batch_init). */
+int bpf_batch_create(const bpf_model_desc* model, int nfilters, const bpf_batch_filter* filters, double ess_rel,
+                     void* stream, bpf_batch** out);
+int bpf_batch_destroy(bpf_batch* b);
+/* Simulator::init for every filter of the batch (see bpf_init). */
+int bpf_batch_init(bpf_batch* b);
+/* Replace every filter's theta (host, nfilters x BPF_MAX_THETA), e.g. a PMMH
+ * proposal; takes effect from the next step or filter run. */
+int bpf_batch_set_theta(bpf_batch* b, const double* theta);
+/* One BootstrapPF::step of every filter (see bpf_step); y_device: device
+ * observations, nfilters x (dim for L96, 1 for PZ), filter-major, in the
+ * model precision, or NULL for an unobserved step.  Does not synchronise. */
+int bpf_batch_step_device(bpf_batch* b, double t1, double t2, const void* y_device);
+/* Host copies of every filter's logLikelihood (-inf after a degenerate
+ * resample), ESS and status; returns the first non-OK status, if any. */
+int bpf_batch_stats(bpf_batch* b, double* log_likelihoods, double* ess, int* status);
+/* Device pointers of the shared buffers: filter f's particle p, component j
+ * at x[j*ld + offsets[f] + p]; log-weights lw[offsets[f] + p]; ancestors
+ * (filter-local indices) as[offsets[f] + p].  offsets: host, nfilters. */
+int bpf_batch_state_ptrs(bpf_batch* b, void** x, double** lw, int** as, int* ld, int* offsets);
+/* Filter<BootstrapPF>::filter for every filter over T observations at
+ * t0+dt, ..., t0+T*dt: bpf_batch_init and T steps.  y: host, T x nfilters x
+ * (dim or 1) in the model precision, step-major then filter-major.  Outputs
+ * (host, may be NULL): log_likelihoods[nfilters] (BootstrapPF::term),
+ * log_increments[T*nfilters] and ess[T*nfilters] (step-major),
+ * status[nfilters].  The init and steps run as one CUDA graph, captured on
+ * the first call and replayed while T, t0 and dt stay the same.  Returns the
+ * first non-OK filter status, if any (the other filters' outputs are valid). */
+int bpf_filter_batch(bpf_batch* b, int T, double t0, double dt, const void* y, double* log_likelihoods,
+                     double* log_increments, double* ess, int* status);
+
 /* ---- checkpoint (BootstrapPFState save/load,
  *      share/src/bi/state/BootstrapPFState.hpp:216-231) ------------------- */
 

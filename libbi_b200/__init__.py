@@ -7,8 +7,8 @@ reference's filter/resampler classes.
 from ._native import (BpfError, ParticleFilterDegeneratedException, load_library,  # noqa: F401
                       LIB_PATH, EXPORTS)
 from .filter import (BootstrapPF, ModelL96, ModelPZ, Resampler, SystematicResampler,  # noqa: F401
-                     MultinomialResampler, MetropolisResampler, gather_rows, StepResult)
+                     MultinomialResampler, MetropolisResampler, gather_rows, StepResult, BatchedBootstrapPF)
 from . import configs  # noqa: F401
 
 __all__ = ["BootstrapPF", "ModelL96", "ModelPZ", "Resampler", "SystematicResampler", "MultinomialResampler",
-           "MetropolisResampler", "gather_rows", "BpfError", "ParticleFilterDegeneratedException", "configs"]
+           "MetropolisResampler", "BatchedBootstrapPF", "gather_rows", "BpfError", "ParticleFilterDegeneratedException", "configs"]

@@ -21,6 +21,7 @@ BPF_E_TIMEOUT = 4
 BPF_E_NOMEM = 5
 BPF_E_TOO_LARGE = 6
 BPF_STATIC_MAX_PARTICLES = 65536
+BPF_BATCH_MAX_PARTICLES = 32768
 
 BPF_MODEL_L96 = 1
 BPF_MODEL_PZ = 2
@@ -42,6 +43,8 @@ EXPORTS = (
     "bpf_snapshot_size", "bpf_snapshot", "bpf_restore", "bpf_version",
     "bpf_status_string", "bpf_timing_enable", "bpf_timing_read", "bpf_systematic_ancestors_static",
     "bpf_resampler_timing_enable", "bpf_resampler_timing_read",
+    "bpf_batch_create", "bpf_batch_destroy", "bpf_batch_init", "bpf_batch_set_theta", "bpf_batch_step_device",
+    "bpf_batch_stats", "bpf_batch_state_ptrs", "bpf_filter_batch",
 )
 
 
@@ -57,6 +60,13 @@ class Config(ctypes.Structure):
     _fields_ = [
         ("nparticles", c_int), ("resampler", c_int), ("metropolis_steps", c_int),
         ("ess_rel", c_double), ("seed", c_uint64), ("stream", c_void_p),
+    ]
+
+
+class BatchFilter(ctypes.Structure):
+    _fields_ = [
+        ("nparticles", c_int), ("resampler", c_int), ("metropolis_steps", c_int), ("seed", c_uint64),
+        ("theta", c_double * BPF_MAX_THETA),
     ]
 
 
@@ -106,6 +116,17 @@ def _declare(L):
         "bpf_restore": (c_int, [H, c_void_p, c_uint64]),
         "bpf_timing_enable": (c_int, [H, c_int]),
         "bpf_timing_read": (c_int, [H, c_int, POINTER(c_double), POINTER(c_double), POINTER(c_int)]),
+        "bpf_batch_create": (c_int, [POINTER(ModelDesc), c_int, POINTER(BatchFilter), c_double, c_void_p,
+                                     POINTER(H)]),
+        "bpf_batch_destroy": (c_int, [H]),
+        "bpf_batch_init": (c_int, [H]),
+        "bpf_batch_set_theta": (c_int, [H, c_void_p]),
+        "bpf_batch_step_device": (c_int, [H, c_double, c_double, c_void_p]),
+        "bpf_batch_stats": (c_int, [H, c_void_p, c_void_p, c_void_p]),
+        "bpf_batch_state_ptrs": (c_int, [H, POINTER(c_void_p), POINTER(c_void_p), POINTER(c_void_p), POINTER(c_int),
+                                         c_void_p]),
+        "bpf_filter_batch": (c_int, [H, c_int, c_double, c_double, c_void_p, c_void_p, c_void_p, c_void_p,
+                                     c_void_p]),
         "bpf_resampler_timing_enable": (c_int, [H, c_int]),
         "bpf_resampler_timing_read": (c_int, [H, c_int, POINTER(c_double), POINTER(c_int)]),
         "bpf_systematic_ancestors_static": (c_int, [c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p,

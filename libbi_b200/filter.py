@@ -357,3 +357,104 @@ class BootstrapPF:
     def restore(self, blob: bytes):
         buf = ctypes.create_string_buffer(blob, len(blob))
         N.check(N.lib().bpf_restore(self._h, buf, len(blob)), "bpf_restore")
+
+
+# ---------------------------------------------------------------------------
+# batched filters
+# ---------------------------------------------------------------------------
+class BatchedBootstrapPF:
+    """Many independent BootstrapPF filters of one model kind advanced together
+    (bpf_batch_*).  models[f] gives filter f's constants (all of one kind,
+    dimension, precision and integrator settings); nparticles, resamplers,
+    seeds and metropolis_steps are per filter (scalars broadcast)."""
+
+    def __init__(self, models, nparticles, resamplers="systematic", seeds=0, ess_rel: float = 0.5,
+                 metropolis_steps=0, stream=None):
+        models = list(models)
+        F = len(models)
+        bc = lambda v: list(v) if isinstance(v, (list, tuple, np.ndarray)) else [v] * F  # noqa: E731
+        nparticles, resamplers, seeds, msteps = bc(nparticles), bc(resamplers), bc(seeds), bc(metropolis_steps)
+        if not (len(nparticles) == len(resamplers) == len(seeds) == len(msteps) == F):
+            raise ValueError("per-filter settings must have one entry per model")
+        self.model = models[0]
+        self.models = models
+        self.nf = F
+        self.n = [int(v) for v in nparticles]
+        self._desc = self.model.desc()
+        arr = (N.BatchFilter * F)()
+        for f, m in enumerate(models):
+            d = m.desc()
+            if (d.kind, d.dim, d.precision, d.integrator) != (self._desc.kind, self._desc.dim, self._desc.precision,
+                                                              self._desc.integrator):
+                raise ValueError("all filters of a batch share the model kind, dimension and precision")
+            arr[f].nparticles = int(nparticles[f])
+            arr[f].resampler = RESAMPLERS[resamplers[f]] if isinstance(resamplers[f], str) else int(resamplers[f])
+            arr[f].metropolis_steps = int(msteps[f])
+            arr[f].seed = int(seeds[f])
+            for i in range(N.BPF_MAX_THETA):
+                arr[f].theta[i] = d.theta[i]
+        self._filters = arr
+        self._h = ctypes.c_void_p()
+        N.check(N.lib().bpf_batch_create(ctypes.byref(self._desc), F, arr, ess_rel, stream, ctypes.byref(self._h)),
+                "bpf_batch_create")
+
+    def close(self):
+        if self._h:
+            N.load_library().bpf_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def init(self):
+        N.check(N.lib().bpf_batch_init(self._h), "bpf_batch_init")
+
+    def set_theta(self, theta):
+        """theta: (nfilters, k <= BPF_MAX_THETA) model constants per filter."""
+        t = np.zeros((self.nf, N.BPF_MAX_THETA))
+        th = np.asarray(theta, dtype=np.float64)
+        t[:, :th.shape[1]] = th
+        N.check(N.lib().bpf_batch_set_theta(self._h, t.ctypes.data_as(ctypes.c_void_p)), "bpf_batch_set_theta")
+
+    def step_device(self, t1: float, t2: float, y_dev=None):
+        """One step of every filter; y_dev: (nfilters, nobs) device tensor or None."""
+        N.check(N.lib().bpf_batch_step_device(self._h, t1, t2, _ptr(y_dev)), "bpf_batch_step_device")
+
+    def stats(self):
+        """(logLikelihood[F], ess[F], status[F]) on the host; no exception for
+        degenerate filters (their logLikelihood is -inf)."""
+        ll, ess, st = np.zeros(self.nf), np.zeros(self.nf), np.zeros(self.nf, np.int32)
+        N.lib().bpf_batch_stats(self._h, ll.ctypes.data_as(ctypes.c_void_p), ess.ctypes.data_as(ctypes.c_void_p),
+                                st.ctypes.data_as(ctypes.c_void_p))
+        return ll, ess, st
+
+    def filter(self, y, t0: float = 0.0, dt: float = 1.0):
+        """Filter<BootstrapPF>::filter for every filter; y: (T, nfilters,
+        nobs) host observations.  Returns (logLikelihood[F],
+        logIncrements[T, F], ess[T, F], status[F])."""
+        arr = np.ascontiguousarray(np.asarray(y, dtype=self.model.np_dtype))
+        T = arr.size // (self.nf * self.model.nobs)
+        if arr.size != T * self.nf * self.model.nobs:
+            raise ValueError("y must hold T x nfilters x nobs values")
+        ll, st = np.zeros(self.nf), np.zeros(self.nf, np.int32)
+        inc, ess = np.zeros((T, self.nf)), np.zeros((T, self.nf))
+        rc = N.lib().bpf_filter_batch(self._h, T, t0, dt, arr.ctypes.data_as(ctypes.c_void_p),
+                                      ll.ctypes.data_as(ctypes.c_void_p), inc.ctypes.data_as(ctypes.c_void_p),
+                                      ess.ctypes.data_as(ctypes.c_void_p), st.ctypes.data_as(ctypes.c_void_p))
+        if rc not in (N.BPF_OK, N.BPF_E_DEGENERATE):
+            N.check(rc, "bpf_filter_batch")
+        return ll, inc, ess, st
+
+    def state(self):
+        """Device views (x[dim, ld], lws[ld], as[ld]) and per-filter offsets."""
+        x, lw, as_, ld = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_int()
+        offs = np.zeros(self.nf, np.int32)
+        N.check(N.lib().bpf_batch_state_ptrs(self._h, ctypes.byref(x), ctypes.byref(lw), ctypes.byref(as_),
+                                             ctypes.byref(ld), offs.ctypes.data_as(ctypes.c_void_p)),
+                "bpf_batch_state_ptrs")
+        dt = "f4" if self.model.precision == "f32" else "f8"
+        return (_view(x.value, (self.model.dim, ld.value), dt), _view(lw.value, (ld.value,), "f8"),
+                _view(as_.value, (ld.value,), "i4"), offs)
