@@ -232,6 +232,131 @@ def large_n_kernels(sizes=(1 << 22, 1 << 24), reps=5):
     return out
 
 
+def batched_workload(rng_seed=3, nf=256, T=100):
+    """256 independent Lorenz-96 d = 40 filters: forcing F_i ~ U(6, 10),
+    particle counts log-uniform in [512, 32768] rounded to 32, seeds
+    1000 + i, systematic resampling for even i and multinomial for odd i,
+    T = 100 observations of all 40 components every 0.05 with N(0, 1) noise."""
+    import numpy as np
+    from libbi_b200 import ModelL96
+
+    rng = np.random.default_rng(rng_seed)
+    Fs = rng.uniform(6.0, 10.0, nf)
+    ns = np.floor(np.exp(rng.uniform(np.log(512), np.log(32768), nf))).astype(int)
+    ns = np.clip((ns + 31) // 32 * 32, 512, 32768)
+    models = [ModelL96(dim=DIM, F=float(F)) for F in Fs]
+    res = ["systematic" if i % 2 == 0 else "multinomial" for i in range(nf)]
+    seeds = [1000 + i for i in range(nf)]
+    return models, [int(n) for n in ns], res, seeds, T
+
+
+def batched_truth(models, T, seed0=5000):
+    """Each filter's synthetic observations: one run of its own model (the
+    library's transition and noise, N = 1, seed seed0 + i) observed with
+    N(0, sigma_y^2) noise."""
+    import numpy as np
+    from libbi_b200 import BatchedBootstrapPF
+
+    nf = len(models)
+    truth = BatchedBootstrapPF(models, [1] * nf, "systematic", [seed0 + i for i in range(nf)])
+    xs = np.zeros((T, nf, DIM), np.float32)
+    for k in range(T):
+        truth.step_device(k * DT, (k + 1) * DT, None)
+        x, _, _, offs = truth.state()
+        xs[k] = x[:, offs.tolist()].cpu().numpy().T
+    truth.close()
+    return observe(xs.reshape(T * nf, DIM), models[0].sigma_y).reshape(T, nf, DIM)
+
+
+def batched_filters(runs=5):
+    """The batched workload through bpf_filter_batch: device time of the
+    captured init + T steps (CUDA events around the graph launch), and end to
+    end (observations uploaded from host memory, log-likelihoods and
+    increments read back) by the host clock.  The state (2 x 40 x sum N x 4 B,
+    ~640 MB) exceeds L2, so no flush is needed between runs."""
+    import numpy as np
+    from libbi_b200 import BatchedBootstrapPF
+
+    models, ns, res, seeds, T = batched_workload()
+    y = batched_truth(models, T)
+    b = BatchedBootstrapPF(models, ns, res, seeds, ess_rel=ESS_REL)
+    b.filter(y, 0.0, DT)  # capture the graph
+    b.timing(True)
+    b.timing_read(reset=True)
+    walls = []
+    for _ in range(runs):
+        t0 = time.perf_counter()
+        ll, inc, ess, st = b.filter(y, 0.0, DT)
+        walls.append(time.perf_counter() - t0)
+    ms, steps = b.timing_read(reset=True)
+    b.close()
+    total = int(np.sum(ns))
+    dev_s = ms / 1e3 / runs
+    hbm, how, _ = peaks()
+    # algorithmic bytes per particle-step of the transition (+ resample
+    # bytes on resample steps are not counted)
+    bps = TRANSITION_BYTES_PER_PARTICLE * total * T / dev_s / 1e9
+    return {
+        "workload": "l96_d40_256filters_n512_32768_loguniform_t100",
+        "filters": len(ns), "total_particles": total, "T": T, "runs": runs,
+        "particle_steps_per_s": total * T / dev_s,
+        "ms_per_filter_run": dev_s * 1e3,
+        "e2e_particle_steps_per_s": total * T / float(np.median(walls)),
+        "e2e_ms_per_filter_run": float(np.median(walls)) * 1e3,
+        "h2d_bytes_per_run": int(y.size * 4), "d2h_bytes_per_run": int(3 * T * len(ns) * 8),
+        "degenerate_filters": int(np.sum(st != 0)),
+        "gpu_launches_per_run": 1 + 2 * T,
+        "roofline": {"bound": "hbm", "achieved": bps, "peak": hbm, "unit": "GB/s", "frac": bps / hbm,
+                     "peak_source": how, "bytes": "336 B per particle-step (transition state + log-weight)"},
+        "l2": "state larger than L2 (~640 MB), no flush",
+    }
+
+
+def pmmh_chains(iterations=20, nchains=128, nparticles=2048, T=100):
+    """Particle-marginal Metropolis-Hastings on the plankton model: 128
+    chains over (c, e, m, q) with priors c, e ~ U(0, 1), m, q ~
+    LogN(ln 0.1, 0.5^2), Gaussian random walk of 0.02 per coordinate; every
+    iteration filters all chains' proposals (N particles each, systematic
+    resampling every step) over T = 100 daily observations log P + N(0, 0.2^2)
+    of one seeded model run (seed 4).  A bounded number of iterations is
+    timed (host clock around bpf_pmmh_run; each iteration is one graph
+    launch plus the proposal and accept/reject arithmetic on the host)."""
+    import math
+
+    import numpy as np
+    from libbi_b200 import BootstrapPF, MarginalMH, ModelPZ, Prior
+
+    model = ModelPZ()
+    truth = BootstrapPF(model, 1, seed=4)
+    ps = np.zeros(T)
+    for k in range(T):
+        truth.step(float(k), float(k + 1), None)
+        x, _, _ = truth.state()
+        ps[k] = float(x[0, 0].item())
+    truth.close()
+    rng = np.random.default_rng(4)
+    y = (np.log(ps) + model.sigma_y * rng.standard_normal(T)).astype(np.float64)
+    priors = [Prior(0, "uniform", 0.0, 1.0, 0.02), Prior(1, "uniform", 0.0, 1.0, 0.02),
+              Prior(2, "log_normal", math.log(0.1), 0.5, 0.02), Prior(3, "log_normal", math.log(0.1), 0.5, 0.02)]
+    mh = MarginalMH(model, priors, y, 0.0, 1.0, nchains=nchains, nparticles=nparticles, resampler="systematic",
+                    ess_rel=1.0, seed=4)
+    mh.run(2)  # graph capture and warm-up
+    t0 = time.perf_counter()
+    out = mh.run(iterations)
+    wall = time.perf_counter() - t0
+    mh.close()
+    acc = (out["accepted"] - 1) / (iterations + 2)
+    return {
+        "workload": f"pz_pmmh_{nchains}chains_n{nparticles}_t{T}",
+        "chains": nchains, "nparticles": nparticles, "T": T, "iterations_timed": iterations,
+        "iterations_per_s": iterations / wall,
+        "particle_steps_per_s": nchains * nparticles * T * iterations / wall,
+        "seconds_for_2000_iterations": 2000 * wall / iterations,
+        "mean_acceptance": float(np.mean(acc)),
+        "timer": "host wall clock around bpf_pmmh_run",
+    }
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -265,6 +390,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-large-n", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -396,6 +522,9 @@ def main():
     }
     if rank == 0 and not args.no_large_n:
         line["kernels_large_n"] = large_n_kernels()
+    if rank == 0 and not args.no_batched:
+        line["batched"] = batched_filters()
+        line["pmmh"] = pmmh_chains()
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(y_host)
     pf.close()

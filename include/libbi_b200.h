@@ -286,6 +286,9 @@ int bpf_batch_init(bpf_batch* b);
 /* Replace every filter's theta (host, nfilters x BPF_MAX_THETA), e.g. a PMMH
  * proposal; takes effect from the next step or filter run. */
 int bpf_batch_set_theta(bpf_batch* b, const double* theta);
+/* Replace every filter's seed (host, nfilters), e.g. fresh randomness for
+ * each filter run of a PMMH iteration; takes effect from the next init. */
+int bpf_batch_set_seeds(bpf_batch* b, const uint64_t* seeds);
 /* One BootstrapPF::step of every filter (see bpf_step); y_device: device
  * observations, nfilters x (dim for L96, 1 for PZ), filter-major, in the
  * model precision, or NULL for an unobserved step.  Does not synchronise. */
@@ -307,6 +310,64 @@ int bpf_batch_state_ptrs(bpf_batch* b, void** x, double** lw, int** as, int* ld,
  * first non-OK filter status, if any (the other filters' outputs are valid). */
 int bpf_filter_batch(bpf_batch* b, int T, double t0, double dt, const void* y, double* log_likelihoods,
                      double* log_increments, double* ess, int* status);
+
+/* Device timing of a batch: when enabled, bpf_batch_step_device times its
+ * kernels and bpf_filter_batch its graph launch (init + T steps; not the
+ * observation upload or the read-back) with CUDA events; these calls then
+ * wait for the timed work.  bpf_batch_timing_read returns the summed
+ * milliseconds and steps since the last reset. */
+int bpf_batch_timing_enable(bpf_batch* b, int enable);
+int bpf_batch_timing_read(bpf_batch* b, int reset, double* ms, int* steps);
+
+/* ---- particle-marginal Metropolis-Hastings over many chains ------------ */
+/* MarginalMH (share/src/bi/sampler/MarginalMH.hpp:190-271) for C chains at
+ * once: every iteration proposes a Gaussian random-walk move of the sampled
+ * entries of theta for each chain, filters all C proposals as one batch
+ * (bpf_filter_batch) and accepts or rejects each chain with
+ * min(1, exp(loglr + logpr)).  Proposals outside the prior's support are
+ * rejected without a filter run for them; a degenerate filter gives
+ * logLikelihood -inf (MarginalMH::propose). */
+enum { BPF_PRIOR_UNIFORM = 0, BPF_PRIOR_LOG_NORMAL = 1, BPF_PRIOR_GAUSSIAN = 2 };
+
+typedef struct {
+  int index;    /* the entry of theta this parameter is */
+  int prior;    /* BPF_PRIOR_UNIFORM (a, b = bounds), _LOG_NORMAL or _GAUSSIAN (a, b = mu, sigma) */
+  double a, b;
+  double step;  /* standard deviation of the random-walk proposal */
+} bpf_pmmh_param;
+
+typedef struct {
+  int nchains;
+  int nparticles;        /* per filter, at most BPF_BATCH_MAX_PARTICLES */
+  int resampler;         /* BPF_RESAMPLER_* */
+  int metropolis_steps;
+  double ess_rel;
+  uint64_t seed;         /* proposals, acceptance and filter seeds derive from it */
+  int nparams;
+  bpf_pmmh_param params[BPF_MAX_THETA];
+} bpf_pmmh_config;
+
+typedef struct bpf_pmmh bpf_pmmh;
+
+/* y: host, T observations (dim values for L96, 1 for PZ) at t0+dt, ...,
+ * t0+T*dt, the same for every chain.  theta0: host, nchains x nparams
+ * initial values, or NULL to draw them from the priors; the other entries of
+ * theta come from model->theta.  Runs the initial filter of every chain
+ * (MarginalMH::init). */
+int bpf_pmmh_create(const bpf_model_desc* model, const bpf_pmmh_config* cfg, int T, double t0, double dt,
+                    const void* y, const double* theta0, void* stream, bpf_pmmh** out);
+int bpf_pmmh_destroy(bpf_pmmh* s);
+/* Run `iterations` MH iterations of every chain.  Outputs (host, may be
+ * NULL), per iteration i and chain c: samples[(i*C + c)*nparams + j] (the
+ * chain's state after the iteration), log_likelihoods[i*C + c],
+ * log_priors[i*C + c], proposal_log_likelihoods[i*C + c] (the proposal's
+ * filter estimate, -inf when not filtered); accepted[c]: accepted moves so
+ * far, counting the initial state as MarginalMH does. */
+int bpf_pmmh_run(bpf_pmmh* s, int iterations, double* samples, double* log_likelihoods, double* log_priors,
+                 double* proposal_log_likelihoods, int* accepted);
+/* Current state: theta[c*nparams + j], logLikelihood and logPrior per chain,
+ * and the number of filter runs so far (the next run index). */
+int bpf_pmmh_state(bpf_pmmh* s, double* theta, double* log_likelihoods, double* log_priors, int* runs);
 
 /* ---- checkpoint (BootstrapPFState save/load,
  *      share/src/bi/state/BootstrapPFState.hpp:216-231) ------------------- */

@@ -44,7 +44,9 @@ EXPORTS = (
     "bpf_status_string", "bpf_timing_enable", "bpf_timing_read", "bpf_systematic_ancestors_static",
     "bpf_resampler_timing_enable", "bpf_resampler_timing_read",
     "bpf_batch_create", "bpf_batch_destroy", "bpf_batch_init", "bpf_batch_set_theta", "bpf_batch_step_device",
-    "bpf_batch_stats", "bpf_batch_state_ptrs", "bpf_filter_batch",
+    "bpf_batch_stats", "bpf_batch_state_ptrs", "bpf_filter_batch", "bpf_batch_timing_enable",
+    "bpf_batch_timing_read", "bpf_batch_set_seeds",
+    "bpf_pmmh_create", "bpf_pmmh_destroy", "bpf_pmmh_run", "bpf_pmmh_state",
 )
 
 
@@ -67,6 +69,20 @@ class BatchFilter(ctypes.Structure):
     _fields_ = [
         ("nparticles", c_int), ("resampler", c_int), ("metropolis_steps", c_int), ("seed", c_uint64),
         ("theta", c_double * BPF_MAX_THETA),
+    ]
+
+
+BPF_PRIOR_UNIFORM, BPF_PRIOR_LOG_NORMAL, BPF_PRIOR_GAUSSIAN = 0, 1, 2
+
+
+class PmmhParam(ctypes.Structure):
+    _fields_ = [("index", c_int), ("prior", c_int), ("a", c_double), ("b", c_double), ("step", c_double)]
+
+
+class PmmhConfig(ctypes.Structure):
+    _fields_ = [
+        ("nchains", c_int), ("nparticles", c_int), ("resampler", c_int), ("metropolis_steps", c_int),
+        ("ess_rel", c_double), ("seed", c_uint64), ("nparams", c_int), ("params", PmmhParam * BPF_MAX_THETA),
     ]
 
 
@@ -127,6 +143,14 @@ def _declare(L):
                                          c_void_p]),
         "bpf_filter_batch": (c_int, [H, c_int, c_double, c_double, c_void_p, c_void_p, c_void_p, c_void_p,
                                      c_void_p]),
+        "bpf_batch_timing_enable": (c_int, [H, c_int]),
+        "bpf_batch_set_seeds": (c_int, [H, c_void_p]),
+        "bpf_pmmh_create": (c_int, [POINTER(ModelDesc), POINTER(PmmhConfig), c_int, c_double, c_double, c_void_p,
+                                    c_void_p, c_void_p, POINTER(H)]),
+        "bpf_pmmh_destroy": (c_int, [H]),
+        "bpf_pmmh_run": (c_int, [H, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+        "bpf_pmmh_state": (c_int, [H, c_void_p, c_void_p, c_void_p, POINTER(c_int)]),
+        "bpf_batch_timing_read": (c_int, [H, c_int, POINTER(c_double), POINTER(c_int)]),
         "bpf_resampler_timing_enable": (c_int, [H, c_int]),
         "bpf_resampler_timing_read": (c_int, [H, c_int, POINTER(c_double), POINTER(c_int)]),
         "bpf_systematic_ancestors_static": (c_int, [c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p,

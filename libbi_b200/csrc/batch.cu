@@ -504,6 +504,12 @@ struct bpf_batch {
   double g_t0 = 0.0, g_dt = 0.0;
   const void* g_y = nullptr;
   const void* g_hist = nullptr;
+  // optional device timing: events around every step_device call's kernels
+  // and around every filter run's graph launch
+  bool timing = false;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  double timed_ms = 0.0;
+  int timed_steps = 0;
 };
 
 namespace {
@@ -542,6 +548,8 @@ int batch_check_theta(const bpf_model_desc* m, const double* th) {
 
 void batch_free(bpf_batch* b) {
   if (b->graph) cudaGraphExecDestroy(b->graph);
+  for (cudaEvent_t e : b->ev)
+    if (e) cudaEventDestroy(e);
   void* ptrs[] = {b->x[0], b->x[1], b->lw, b->as, b->stats, b->partials, b->counters, b->filt_dev,
                   b->prm_dev, b->blk2f, b->order, b->lu, b->os, b->y_dev, b->hist};
   for (void* p : ptrs)
@@ -734,9 +742,56 @@ int bpf_batch_set_theta(bpf_batch* b, const double* theta) {
   return batch_upload_params(b);
 }
 
+// events around enqueued work; the elapsed time is collected at the next
+// synchronising read (bpf_batch_timing_read)
+static int batch_timing_begin(bpf_batch* b) {
+  if (b->timing) BPF_TRY(cudaEventRecord(b->ev[0], b->stream));
+  return BPF_OK;
+}
+
+static int batch_timing_end(bpf_batch* b, int steps) {
+  if (!b->timing) return BPF_OK;
+  BPF_TRY(cudaEventRecord(b->ev[1], b->stream));
+  BPF_TRY(cudaEventSynchronize(b->ev[1]));
+  float ms = 0.0f;
+  BPF_TRY(cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]));
+  b->timed_ms += ms;
+  b->timed_steps += steps;
+  return BPF_OK;
+}
+
+int bpf_batch_set_seeds(bpf_batch* b, const uint64_t* seeds) {
+  if (!b || !seeds) return BPF_E_INVALID;
+  for (int f = 0; f < b->nf; ++f) b->filt[f].seed = seeds[f];
+  BPF_TRY(cudaMemcpyAsync(b->filt_dev, b->filt.data(), b->filt.size() * sizeof(bpf::BatchFilter),
+                          cudaMemcpyHostToDevice, b->stream));
+  BPF_TRY(cudaStreamSynchronize(b->stream));
+  return BPF_OK;
+}
+
 int bpf_batch_step_device(bpf_batch* b, double t1, double t2, const void* y_device) {
   if (!b || !(t1 < t2)) return BPF_E_INVALID;
-  return batch_enqueue_step(b, t1, t2, y_device, nullptr, 0);
+  int rc = batch_timing_begin(b);
+  if (!rc) rc = batch_enqueue_step(b, t1, t2, y_device, nullptr, 0);
+  if (!rc) rc = batch_timing_end(b, 1);
+  return rc;
+}
+
+int bpf_batch_timing_enable(bpf_batch* b, int enable) {
+  if (!b) return BPF_E_INVALID;
+  if (enable)
+    for (cudaEvent_t& e : b->ev)
+      if (!e) BPF_TRY(cudaEventCreate(&e));
+  b->timing = enable != 0;
+  return BPF_OK;
+}
+
+int bpf_batch_timing_read(bpf_batch* b, int reset, double* ms, int* steps) {
+  if (!b) return BPF_E_INVALID;
+  if (ms) *ms = b->timed_ms;
+  if (steps) *steps = b->timed_steps;
+  if (reset) { b->timed_ms = 0.0; b->timed_steps = 0; }
+  return BPF_OK;
 }
 
 int bpf_batch_stats(bpf_batch* b, double* log_likelihoods, double* ess, int* status) {
@@ -801,7 +856,11 @@ int bpf_filter_batch(bpf_batch* b, int T, double t0, double dt, const void* y, d
     if (e != cudaSuccess) { b->graph = nullptr; bpf_set_last_cuda_error(e); return BPF_E_CUDA; }
     b->g_T = T; b->g_t0 = t0; b->g_dt = dt; b->g_y = b->y_dev; b->g_hist = b->hist;
   }
+  int rc = batch_timing_begin(b);
+  if (rc) return rc;
   BPF_TRY(cudaGraphLaunch(b->graph, b->stream));
+  rc = batch_timing_end(b, T);
+  if (rc) return rc;
   // the host-side state the captured steps advanced
   b->cur = T & 1;
   b->step = T;

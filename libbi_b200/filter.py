@@ -47,6 +47,11 @@ def _view(ptr: int, shape, dtype: str):
     return torch.as_tensor(_DeviceArray(ptr, shape, typestr), device="cuda")
 
 
+def _ptr_np(a):
+    """Host pointer of a contiguous numpy array (or None)."""
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
 def _ptr(t) -> Optional[int]:
     if t is None:
         return None
@@ -422,6 +427,16 @@ class BatchedBootstrapPF:
     def step_device(self, t1: float, t2: float, y_dev=None):
         """One step of every filter; y_dev: (nfilters, nobs) device tensor or None."""
         N.check(N.lib().bpf_batch_step_device(self._h, t1, t2, _ptr(y_dev)), "bpf_batch_step_device")
+
+    def timing(self, enable: bool = True):
+        N.check(N.lib().bpf_batch_timing_enable(self._h, int(enable)), "bpf_batch_timing_enable")
+
+    def timing_read(self, reset: bool = True):
+        """(device milliseconds, steps) timed since the last reset."""
+        ms, k = ctypes.c_double(), ctypes.c_int()
+        N.check(N.lib().bpf_batch_timing_read(self._h, int(reset), ctypes.byref(ms), ctypes.byref(k)),
+                "bpf_batch_timing_read")
+        return ms.value, k.value
 
     def stats(self):
         """(logLikelihood[F], ess[F], status[F]) on the host; no exception for

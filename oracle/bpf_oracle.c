@@ -664,3 +664,18 @@ void orc_noise_normals(uint64_t seed, uint32_t p, int step, int n, int prec, dou
     }
   }
 }
+
+/* PMMH draws of chain c at filter run r (the scheme documented in
+ * libbi_b200/csrc/pmmh.cu): the proposal normal of parameter j from block
+ * j/2, word pair j%2 (Box-Muller, double); the acceptance uniform from block
+ * 64; tag BPF_RNG_PMMH. */
+void orc_pmmh_draws(uint64_t seed, int c, int r, int nparams, double* z, double* u) {
+  for (int j = 0; j < nparams; ++j) {
+    bpf_u32x4 w = bpf_draw(seed, (uint32_t)c, (uint32_t)r, (uint32_t)(j / 2), BPF_RNG_PMMH);
+    double z0, z1;
+    bpf_normal_pair_d(w.v[0], w.v[1], &z0, &z1);
+    z[j] = (j & 1) ? z1 : z0;
+  }
+  bpf_u32x4 w = bpf_draw(seed, (uint32_t)c, (uint32_t)r, 64u, BPF_RNG_PMMH);
+  *u = bpf_u01d(w.v[0], w.v[1]);
+}

@@ -53,6 +53,7 @@ class Oracle:
         L.orc_filter.argtypes = [c_void_p, c_void_p, c_int, c_double, c_double, c_void_p, c_void_p, c_void_p,
                                  c_void_p, POINTER(c_double), c_void_p, c_void_p]
         L.orc_noise_normals.argtypes = [c_uint64, ctypes.c_uint32, c_int, c_int, c_int, c_void_p]
+        L.orc_pmmh_draws.argtypes = [c_uint64, c_int, c_int, c_int, c_void_p, POINTER(c_double)]
         L.orc_simulate.argtypes = [c_void_p, c_uint64, c_int, c_double, c_double, c_void_p, c_void_p]
         self.L = L
 
@@ -149,6 +150,14 @@ class Oracle:
         z = np.zeros(n)
         self.L.orc_noise_normals(c_uint64(seed), int(p), int(step), int(n), 0 if f32 else 1, _p(z))
         return z
+
+    def pmmh_draws(self, seed, c, r, nparams):
+        """(proposal normals[nparams], acceptance uniform) of PMMH chain c at
+        filter run r."""
+        z = np.zeros(nparams)
+        u = c_double()
+        self.L.orc_pmmh_draws(c_uint64(seed), int(c), int(r), int(nparams), _p(z), ctypes.byref(u))
+        return z, u.value
 
     def simulate(self, desc, seed, T, t0, dt):
         dtp = np.float32 if desc.precision == 0 else np.float64
