@@ -369,6 +369,19 @@ int bpf_pmmh_run(bpf_pmmh* s, int iterations, double* samples, double* log_likel
  * and the number of filter runs so far (the next run index). */
 int bpf_pmmh_state(bpf_pmmh* s, double* theta, double* log_likelihoods, double* log_priors, int* runs);
 
+/* ---- tensor-core dense layer (the learned proposal's arithmetic) ------- */
+/* No counterpart in the reference.  D[m, n] = act(sum_k A(m,k) B(n,k) +
+ * bias[n]) for m < M, n < N <= 256, on the sm_100a tensor cores (tcgen05,
+ * BF16 operands, FP32 accumulation in tensor memory).  A(m,k) =
+ * A[m*a_rs + k*a_cs] and B(n,k) = B[n*b_rs + k*b_cs] (device, BF16), so
+ * transposed operands need no copy; bias: device, N floats, or NULL; relu:
+ * 0 or 1; Df (FP32, row stride df_rs) and/or Dh (BF16, row stride dh_rs)
+ * receive D; err: device int set to 1 if a bounded wait gave up.  Enqueued
+ * on `stream`; does not synchronise. */
+int bpf_dense_bf16(const void* A, long long a_rs, long long a_cs, const void* B, long long b_rs, long long b_cs,
+                   int M, int N, int K, const float* bias, int relu, float* Df, long long df_rs, void* Dh,
+                   long long dh_rs, int* err, void* stream);
+
 /* ---- checkpoint (BootstrapPFState save/load,
  *      share/src/bi/state/BootstrapPFState.hpp:216-231) ------------------- */
 

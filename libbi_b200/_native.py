@@ -8,7 +8,7 @@ from __future__ import annotations
 
 import ctypes
 import os
-from ctypes import POINTER, c_double, c_int, c_uint64, c_void_p, c_char_p
+from ctypes import c_longlong, POINTER, c_double, c_int, c_uint64, c_void_p, c_char_p
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_lib", "libbi_b200.so")
@@ -46,7 +46,7 @@ EXPORTS = (
     "bpf_batch_create", "bpf_batch_destroy", "bpf_batch_init", "bpf_batch_set_theta", "bpf_batch_step_device",
     "bpf_batch_stats", "bpf_batch_state_ptrs", "bpf_filter_batch", "bpf_batch_timing_enable",
     "bpf_batch_timing_read", "bpf_batch_set_seeds",
-    "bpf_pmmh_create", "bpf_pmmh_destroy", "bpf_pmmh_run", "bpf_pmmh_state",
+    "bpf_pmmh_create", "bpf_pmmh_destroy", "bpf_pmmh_run", "bpf_pmmh_state", "bpf_dense_bf16",
 )
 
 
@@ -148,6 +148,9 @@ def _declare(L):
         "bpf_pmmh_create": (c_int, [POINTER(ModelDesc), POINTER(PmmhConfig), c_int, c_double, c_double, c_void_p,
                                     c_void_p, c_void_p, POINTER(H)]),
         "bpf_pmmh_destroy": (c_int, [H]),
+        "bpf_dense_bf16": (c_int, [c_void_p, c_longlong, c_longlong, c_void_p, c_longlong, c_longlong, c_int, c_int,
+                                   c_int, c_void_p, c_int, c_void_p, c_longlong, c_void_p, c_longlong, c_void_p,
+                                   c_void_p]),
         "bpf_pmmh_run": (c_int, [H, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
         "bpf_pmmh_state": (c_int, [H, c_void_p, c_void_p, c_void_p, POINTER(c_int)]),
         "bpf_batch_timing_read": (c_int, [H, c_int, POINTER(c_double), POINTER(c_int)]),

@@ -1,0 +1,170 @@
+// Dense layers on the fifth-generation tensor cores, the arithmetic of the
+// learned proposal (forward inference inside the guided filter, forward and
+// backward passes of its training).
+//
+// k_dense_tc computes, for one 128-row tile of A per CTA,
+//   D[m, n] = act( sum_k A(m, k) * B(n, k) + bias[n] ),   n < N <= 256,
+// with A and B read through arbitrary element strides (so transposed
+// operands cost nothing extra), BF16 operands and FP32 accumulation in
+// tensor memory.  The K dimension streams through shared memory in chunks of
+// 64: the 128 threads stage a chunk in the canonical K-major layout, one
+// thread issues four 128 x N x 16 MMAs and commits them to an mbarrier, and
+// the chunk buffer is reused once that barrier's phase completes.  The
+// epilogue reads each thread's accumulator row from tensor memory (warp w
+// owns lanes 32w..32w+31), adds the bias, applies the activation and writes
+// FP32 and/or BF16 results.
+#include "internal.cuh"
+#include "tc.cuh"
+
+#include <cuda_bf16.h>
+
+namespace bpf {
+
+struct DenseArgs {
+  const __nv_bfloat16* A;
+  long long a_rs, a_cs;  // A(m, k) = A[m*a_rs + k*a_cs]
+  const __nv_bfloat16* B;
+  long long b_rs, b_cs;  // B(n, k) = B[n*b_rs + k*b_cs]
+  int M, N, K;
+  const float* bias;     // N values, or null
+  int relu;
+  float* Df;             // D(m, n) = Df[m*df_rs + n], or null
+  long long df_rs;
+  __nv_bfloat16* Dh;     // BF16 copy, or null
+  long long dh_rs;
+  int* err;              // set when a bounded wait gives up
+};
+
+constexpr int kTcKC = 64;                         // K per staged chunk
+constexpr long long kTcWaitCycles = 2000000000ll;  // ~1 s at 2 GHz
+
+template <int BN>
+__global__ void __launch_bounds__(128) k_dense_tc(DenseArgs g) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned char* sA = smem;                     // 128 x KC
+  unsigned char* sB = smem + 128 * kTcKC * 2;   // BN x KC
+  __shared__ uint64_t mbar;
+  __shared__ uint32_t s_taddr;
+  constexpr uint32_t NCOLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.x * 128;
+  if (warp == 0) tc::tmem_alloc(&s_taddr, NCOLS);
+  if (tid == 0) tc::mbar_init(&mbar, 1);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t taddr = s_taddr;
+  constexpr uint32_t idesc = tc::idesc_bf16(128, BN);
+  const __nv_bfloat16 zero = __float2bfloat16(0.0f);
+  bool ok = true;
+  const int nchunks = (g.K + kTcKC - 1) / kTcKC;
+  for (int c = 0; c < nchunks; ++c) {
+    const int k0 = c * kTcKC;
+    for (int e = tid; e < 128 * kTcKC; e += 128) {
+      const int r = e / kTcKC, k = e % kTcKC;
+      const int m = m0 + r, kk = k0 + k;
+      const __nv_bfloat16 v = (m < g.M && kk < g.K) ? g.A[m * g.a_rs + kk * g.a_cs] : zero;
+      *reinterpret_cast<__nv_bfloat16*>(sA + tc::kmajor_off(r, k, kTcKC)) = v;
+    }
+    for (int e = tid; e < BN * kTcKC; e += 128) {
+      const int r = e / kTcKC, k = e % kTcKC;
+      const int kk = k0 + k;
+      const __nv_bfloat16 v = (r < g.N && kk < g.K) ? g.B[r * g.b_rs + kk * g.b_cs] : zero;
+      *reinterpret_cast<__nv_bfloat16*>(sB + tc::kmajor_off(r, k, kTcKC)) = v;
+    }
+    tc::fence_proxy_async();
+    __syncthreads();
+    if (tid == 0) {
+      tc::fence_after_sync();
+#pragma unroll
+      for (int ks = 0; ks < kTcKC / 16; ++ks) {
+        const uint64_t ad = tc::smem_desc(tc::smem_u32(sA) + ks * 256, 128, kTcKC * 16);
+        const uint64_t bd = tc::smem_desc(tc::smem_u32(sB) + ks * 256, 128, kTcKC * 16);
+        tc::mma_bf16(taddr, ad, bd, idesc, (c > 0 || ks > 0) ? 1u : 0u);
+      }
+      tc::mma_commit(&mbar);
+    }
+    // the chunk buffers are reused once the MMAs that read them are done
+    const bool done = tc::mbar_wait(&mbar, (uint32_t)(c & 1), kTcWaitCycles);
+    ok = __syncthreads_and(done && ok) != 0;
+    if (!ok) break;
+  }
+  tc::fence_after_sync();
+  if (ok) {
+    const int m = m0 + warp * 32 + lane;
+#pragma unroll 1
+    for (int n0 = 0; n0 < BN; n0 += 16) {
+      float v[16];
+      tc::tmem_ld16(taddr + ((uint32_t)(warp * 32) << 16) + (uint32_t)n0, v);
+      if (m < g.M) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int n = n0 + j;
+          if (n < g.N) {
+            float x = v[j] + (g.bias ? __ldg(g.bias + n) : 0.0f);
+            if (g.relu) x = fmaxf(x, 0.0f);
+            if (g.Df) g.Df[m * g.df_rs + n] = x;
+            if (g.Dh) g.Dh[m * g.dh_rs + n] = __float2bfloat16(x);
+          }
+        }
+      }
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(taddr, NCOLS);
+  if (!ok && tid == 0) atomicExch(g.err, 1);
+}
+
+template <int BN>
+static int launch_dense_bn(const DenseArgs& g, cudaStream_t st) {
+  constexpr uint32_t NCOLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
+  // staging buffers, and at least enough shared memory that the CTAs
+  // resident on one SM never ask for more than its 512 TMEM columns
+  const size_t staging = (size_t)(128 + BN) * kTcKC * 2;
+  const size_t tmem_cap = 233472 / (512 / NCOLS + 1) + 1024;
+  const size_t smem = staging > tmem_cap ? staging : tmem_cap;
+  static bool configured = false;
+  if (!configured) {
+    BPF_TRY(cudaFuncSetAttribute(k_dense_tc<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    configured = true;
+  }
+  const int grid = (g.M + 127) / 128;
+  k_dense_tc<BN><<<grid, 128, smem, st>>>(g);
+  BPF_TRY(cudaGetLastError());
+  return BPF_OK;
+}
+
+int launch_dense(const DenseArgs& g, cudaStream_t st) {
+  if (g.M <= 0 || g.N <= 0 || g.K <= 0 || !g.A || !g.B || !g.err || (!g.Df && !g.Dh)) return BPF_E_INVALID;
+  const int bn = (g.N + 15) / 16 * 16;
+  switch (bn) {
+    case 16: return launch_dense_bn<16>(g, st);
+    case 32: return launch_dense_bn<32>(g, st);
+    case 48: return launch_dense_bn<48>(g, st);
+    case 64: return launch_dense_bn<64>(g, st);
+    case 80: return launch_dense_bn<80>(g, st);
+    case 96: return launch_dense_bn<96>(g, st);
+    case 128: return launch_dense_bn<128>(g, st);
+    case 160: return launch_dense_bn<160>(g, st);
+    case 192: return launch_dense_bn<192>(g, st);
+    case 256: return launch_dense_bn<256>(g, st);
+    default: return BPF_E_INVALID;
+  }
+}
+
+}  // namespace bpf
+
+extern "C" int bpf_dense_bf16(const void* A, long long a_rs, long long a_cs, const void* B, long long b_rs,
+                              long long b_cs, int M, int N, int K, const float* bias, int relu, float* Df,
+                              long long df_rs, void* Dh, long long dh_rs, int* err, void* stream) {
+  bpf::DenseArgs g;
+  g.A = (const __nv_bfloat16*)A; g.a_rs = a_rs; g.a_cs = a_cs;
+  g.B = (const __nv_bfloat16*)B; g.b_rs = b_rs; g.b_cs = b_cs;
+  g.M = M; g.N = N; g.K = K;
+  g.bias = bias; g.relu = relu;
+  g.Df = Df; g.df_rs = df_rs;
+  g.Dh = (__nv_bfloat16*)Dh; g.dh_rs = dh_rs;
+  g.err = err;
+  return bpf::launch_dense(g, (cudaStream_t)stream);
+}
