@@ -382,6 +382,51 @@ int bpf_dense_bf16(const void* A, long long a_rs, long long a_cs, const void* B,
                    int M, int N, int K, const float* bias, int relu, float* Df, long long df_rs, void* Dh,
                    long long dh_rs, int* err, void* stream);
 
+/* ---- learned proposal (Lorenz-96, d = 40, FP32) ------------------------ */
+/* No counterpart in the reference, whose bootstrap filter proposes from the
+ * transition.  A small network proposes
+ *   x_{t+1} ~ N(m(x_t) + delta, diag(exp(2 s))),  (delta, s) = MLP([x_t, y_{t+1} - m(x_t)]),
+ * m the model's deterministic RK4 step over dt (the observation enters
+ * through its innovation); input standardised with the training data's
+ * statistics, two hidden layers of 128 ReLU units, BF16
+ * weights and activations on the tensor cores (bpf_dense_bf16), FP32
+ * accumulation, FP32 master weights trained by Adam on the Gaussian negative
+ * log-likelihood of x_{t+1}.  A filter with a proposal attached
+ * (bpf_set_proposal) weights each particle by p(y|x') p(x'|x) / q(x'|x, y),
+ * so its likelihood estimate stays unbiased. */
+typedef struct bpf_proposal bpf_proposal;
+
+/* model: L96, dim 40, BPF_F32 (F = theta[0], sigma_eta = theta[1], h); dt: the
+ * observation interval; max_batch: the largest training batch (>= 128).
+ * The untrained proposal is close to the transition itself. */
+int bpf_proposal_create(const bpf_model_desc* model, double dt, int max_batch, uint64_t seed, void* stream,
+                        bpf_proposal** out);
+int bpf_proposal_destroy(bpf_proposal* p);
+/* Training triples (device, n x 40 each, row-major, kept by the caller while
+ * training): x_t, x_{t+1} simulated from x_t by the model, y_{t+1} observed
+ * from x_{t+1}.  Computes the RK4 means and the input standardisation. */
+int bpf_proposal_set_data(bpf_proposal* p, const float* x_t, const float* x_t1, const float* y_t1, int n);
+/* `steps` Adam steps on minibatches of `batch` rows drawn with replacement
+ * (counter-based stream of the seed), learning rate lr after a linear
+ * warm-up over 5% of the steps and decaying by a cosine to lr/10;
+ * loss_trace (host, may be NULL) gets each step's mean loss. */
+int bpf_proposal_train(bpf_proposal* p, int steps, int batch, double lr, float* loss_trace);
+/* Loss and gradient (device, nparams floats, the parameter layout of
+ * bpf_proposal_params) on one given minibatch: U (device BF16, batch x 80,
+ * standardised [x_t, y - m(x_t)]) and r0 (device FP32, batch x 40,
+ * x_{t+1} - m(x_t)). */
+int bpf_proposal_loss_grad(bpf_proposal* p, const void* U, const float* r0, int batch, double* loss, float* grads);
+/* Host copies of the FP32 parameters W1 [128 x 80], b1, W2 [128 x 128], b2,
+ * W3 [80 x 128], b3 and of the input shift and scale (80 each); any pointer
+ * may be NULL.  bpf_proposal_set_params loads them. */
+int bpf_proposal_params(bpf_proposal* p, float* params, float* shift, float* scale, int* nparams);
+int bpf_proposal_set_params(bpf_proposal* p, const float* params, const float* shift, const float* scale);
+/* Attach a proposal to a filter (L96, dim 40, FP32) or detach it (p = NULL).
+ * Observed steps of exactly the proposal's dt then propose from it and weight
+ * by p(y|x') p(x'|x) / q(x'|x, y); unobserved steps use the transition.  The
+ * proposal must outlive its use by the handle. */
+int bpf_set_proposal(bpf_handle* h, bpf_proposal* p);
+
 /* ---- checkpoint (BootstrapPFState save/load,
  *      share/src/bi/state/BootstrapPFState.hpp:216-231) ------------------- */
 

@@ -47,6 +47,8 @@ EXPORTS = (
     "bpf_batch_stats", "bpf_batch_state_ptrs", "bpf_filter_batch", "bpf_batch_timing_enable",
     "bpf_batch_timing_read", "bpf_batch_set_seeds",
     "bpf_pmmh_create", "bpf_pmmh_destroy", "bpf_pmmh_run", "bpf_pmmh_state", "bpf_dense_bf16",
+    "bpf_proposal_create", "bpf_proposal_destroy", "bpf_proposal_set_data", "bpf_proposal_train",
+    "bpf_proposal_loss_grad", "bpf_proposal_params", "bpf_proposal_set_params", "bpf_set_proposal",
 )
 
 
@@ -148,6 +150,14 @@ def _declare(L):
         "bpf_pmmh_create": (c_int, [POINTER(ModelDesc), POINTER(PmmhConfig), c_int, c_double, c_double, c_void_p,
                                     c_void_p, c_void_p, POINTER(H)]),
         "bpf_pmmh_destroy": (c_int, [H]),
+        "bpf_proposal_create": (c_int, [POINTER(ModelDesc), c_double, c_int, c_uint64, c_void_p, POINTER(H)]),
+        "bpf_proposal_destroy": (c_int, [H]),
+        "bpf_proposal_set_data": (c_int, [H, c_void_p, c_void_p, c_void_p, c_int]),
+        "bpf_proposal_train": (c_int, [H, c_int, c_int, c_double, c_void_p]),
+        "bpf_proposal_loss_grad": (c_int, [H, c_void_p, c_void_p, c_int, POINTER(c_double), c_void_p]),
+        "bpf_proposal_params": (c_int, [H, c_void_p, c_void_p, c_void_p, POINTER(c_int)]),
+        "bpf_proposal_set_params": (c_int, [H, c_void_p, c_void_p, c_void_p]),
+        "bpf_set_proposal": (c_int, [H, H]),
         "bpf_dense_bf16": (c_int, [c_void_p, c_longlong, c_longlong, c_void_p, c_longlong, c_longlong, c_int, c_int,
                                    c_int, c_void_p, c_int, c_void_p, c_longlong, c_void_p, c_longlong, c_void_p,
                                    c_void_p]),

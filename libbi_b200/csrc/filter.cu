@@ -8,6 +8,7 @@
 // the counter-based RNG.  One BootstrapPF::step is a short, fixed sequence of
 // kernels on the handle's stream; nothing returns to the host unless asked.
 #include "internal.cuh"
+#include "proposal.cuh"
 
 #include <cstdio>
 #include <cstring>
@@ -38,6 +39,11 @@ struct bpf_handle {
   bool timing = false;
   std::vector<cudaEvent_t> ev;
   int ev_steps = 0;
+  // learned proposal (bpf_set_proposal) and its per-particle scratch
+  bpf_proposal* prop = nullptr;
+  float* g_M = nullptr;
+  __nv_bfloat16 *g_U = nullptr, *g_H1 = nullptr, *g_H2 = nullptr;
+  float* g_O = nullptr;
 };
 
 struct bpf_resampler {
@@ -131,6 +137,44 @@ int enqueue_step(bpf_handle* h, double t1, double t2, const void* y_dev) {
   if (h->timing) {
     rc = timing_event(h, 1);
     if (rc) return rc;
+  }
+  if (h->prop && y_dev) {
+    // guided step: the learned proposal instead of the transition
+    const double dt = bpf::proposal_dt(h->prop);
+    if (std::fabs((t2 - t1) - dt) > 1e-9 * dt) return BPF_E_INVALID;
+    bpf::GuidedArgs ga;
+    ga.x_in = h->x[h->cur];
+    ga.x_out = h->x[h->cur ^ 1];
+    ga.ld = h->ld;
+    ga.n = h->n;
+    ga.as = h->as;
+    ga.lw = h->lw;
+    ga.y = y_dev;
+    ga.t1 = t1;
+    ga.t2 = t2;
+    ga.seed = h->cfg.seed;
+    ga.step = k;
+    for (int i = 0; i < BPF_MAX_THETA; ++i) ga.theta[i] = h->model.theta[i];
+    ga.h = h->model.h;
+    ga.stats = h->rs.stats;
+    ga.partials = h->rs.partials;
+    ga.max_partials = h->rs.max_partials;
+    ga.counter = h->rs.counters + 4;
+    ga.M = h->g_M;
+    ga.U = h->g_U;
+    ga.H1 = h->g_H1;
+    ga.H2 = h->g_H2;
+    ga.O = h->g_O;
+    rc = bpf::launch_guided(*bpf::proposal_net(h->prop), ga, h->stream);
+    if (rc) return rc;
+    if (h->timing) {
+      rc = timing_event(h, 2);
+      if (rc) return rc;
+      h->ev_steps += 1;
+    }
+    h->cur ^= 1;
+    h->step = k;
+    return BPF_OK;
   }
   bpf::TransitionArgs ta;
   ta.x_in = h->x[h->cur];
@@ -247,8 +291,38 @@ int bpf_destroy(bpf_handle* h) {
   if (h->y_dev) cudaFree(h->y_dev);
   if (h->hist) cudaFree(h->hist);
   for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
+  void* g[] = {h->g_M, h->g_U, h->g_H1, h->g_H2, h->g_O};
+  for (void* p : g)
+    if (p) cudaFree(p);
   bpf::scratch_free(h->rs);
   delete h;
+  return BPF_OK;
+}
+
+int bpf_set_proposal(bpf_handle* h, bpf_proposal* p) {
+  if (!h) return BPF_E_INVALID;
+  if (p) {
+    if (h->model.kind != BPF_MODEL_L96 || h->model.dim != 40 || h->model.precision != BPF_F32) return BPF_E_INVALID;
+    const bpf::ProposalNet& net = *bpf::proposal_net(p);
+    if (net.dim != h->dim) return BPF_E_INVALID;
+    if (!h->g_M) {
+      const size_t L = (size_t)h->ld;
+      bool ok = cudaMalloc((void**)&h->g_M, (size_t)net.dim * L * 4) == cudaSuccess &&
+                cudaMalloc((void**)&h->g_U, L * net.din * 2) == cudaSuccess &&
+                cudaMalloc((void**)&h->g_H1, L * net.hidden * 2) == cudaSuccess &&
+                cudaMalloc((void**)&h->g_H2, L * net.hidden * 2) == cudaSuccess &&
+                cudaMalloc((void**)&h->g_O, (size_t)net.dout * L * 4) == cudaSuccess;
+      if (!ok) {
+        cudaGetLastError();
+        void* g[] = {h->g_M, h->g_U, h->g_H1, h->g_H2, h->g_O};
+        for (void* q : g)
+          if (q) cudaFree(q);
+        h->g_M = nullptr; h->g_U = nullptr; h->g_H1 = nullptr; h->g_H2 = nullptr; h->g_O = nullptr;
+        return BPF_E_NOMEM;
+      }
+    }
+  }
+  h->prop = p;
   return BPF_OK;
 }
 

@@ -15,25 +15,11 @@
 // FP32 and/or BF16 results.
 #include "internal.cuh"
 #include "tc.cuh"
+#include "mlp.cuh"
 
 #include <cuda_bf16.h>
 
 namespace bpf {
-
-struct DenseArgs {
-  const __nv_bfloat16* A;
-  long long a_rs, a_cs;  // A(m, k) = A[m*a_rs + k*a_cs]
-  const __nv_bfloat16* B;
-  long long b_rs, b_cs;  // B(n, k) = B[n*b_rs + k*b_cs]
-  int M, N, K;
-  const float* bias;     // N values, or null
-  int relu;
-  float* Df;             // D(m, n) = Df[m*df_rs + n], or null
-  long long df_rs;
-  __nv_bfloat16* Dh;     // BF16 copy, or null
-  long long dh_rs;
-  int* err;              // set when a bounded wait gives up
-};
 
 constexpr int kTcKC = 64;                         // K per staged chunk
 constexpr long long kTcWaitCycles = 2000000000ll;  // ~1 s at 2 GHz
@@ -103,7 +89,7 @@ __global__ void __launch_bounds__(128) k_dense_tc(DenseArgs g) {
           if (n < g.N) {
             float x = v[j] + (g.bias ? __ldg(g.bias + n) : 0.0f);
             if (g.relu) x = fmaxf(x, 0.0f);
-            if (g.Df) g.Df[m * g.df_rs + n] = x;
+            if (g.Df) g.Df[m * g.df_rs + n * g.df_cs] = x;
             if (g.Dh) g.Dh[m * g.dh_rs + n] = __float2bfloat16(x);
           }
         }
@@ -163,7 +149,7 @@ extern "C" int bpf_dense_bf16(const void* A, long long a_rs, long long a_cs, con
   g.B = (const __nv_bfloat16*)B; g.b_rs = b_rs; g.b_cs = b_cs;
   g.M = M; g.N = N; g.K = K;
   g.bias = bias; g.relu = relu;
-  g.Df = Df; g.df_rs = df_rs;
+  g.Df = Df; g.df_rs = df_rs; g.df_cs = 1;
   g.Dh = (__nv_bfloat16*)Dh; g.dh_rs = dh_rs;
   g.err = err;
   return bpf::launch_dense(g, (cudaStream_t)stream);

@@ -1,0 +1,27 @@
+// Declarations of the tensor-core dense layer (mlp.cu).
+#pragma once
+#include "internal.cuh"
+
+#include <cuda_bf16.h>
+
+namespace bpf {
+
+struct DenseArgs {
+  const __nv_bfloat16* A;
+  long long a_rs, a_cs;  // A(m, k) = A[m*a_rs + k*a_cs]
+  const __nv_bfloat16* B;
+  long long b_rs, b_cs;  // B(n, k) = B[n*b_rs + k*b_cs]
+  int M, N, K;
+  const float* bias;     // N values, or null
+  int relu;
+  float* Df;             // D(m, n) = Df[m*df_rs + n*df_cs], or null
+  long long df_rs;
+  long long df_cs = 1;
+  __nv_bfloat16* Dh;     // BF16 copy, or null
+  long long dh_rs;
+  int* err;              // set when a bounded wait gives up
+};
+
+int launch_dense(const DenseArgs& g, cudaStream_t st);
+
+}  // namespace bpf

@@ -1,0 +1,77 @@
+// The learned proposal's network and buffers (proposal.cu), shared with the
+// guided filter step (guided.cu).
+#pragma once
+#include "internal.cuh"
+
+#include <cuda_bf16.h>
+
+namespace bpf {
+
+constexpr int kProposalHidden = 128;
+// clamp of the proposal's log-scale s
+constexpr float kSMin = -7.0f, kSMax = 3.0f;
+
+struct ProposalNet {
+  int dim = 0, din = 0, dout = 0, hidden = 0;
+  // parameter vector: W1 [hidden x din], b1, W2 [hidden x hidden], b2,
+  // W3 [dout x hidden], b3 (offsets in floats)
+  int o_w1 = 0, o_b1 = 0, o_w2 = 0, o_b2 = 0, o_w3 = 0, o_b3 = 0, nparams = 0;
+  float* params = nullptr;            // FP32 master copy
+  __nv_bfloat16* params_h = nullptr;  // BF16 copy the dense layers read
+  float *grads = nullptr, *m1 = nullptr, *m2 = nullptr;
+  float *shift = nullptr, *scale = nullptr;  // input standardisation
+  int* err = nullptr;
+  double* loss = nullptr;
+  // minibatch buffers (cap rows)
+  int cap = 0;
+  __nv_bfloat16 *U = nullptr, *H1 = nullptr, *H2 = nullptr, *dO = nullptr, *dZ = nullptr;
+  float *O = nullptr, *dH = nullptr, *r0 = nullptr;
+  float* mt = nullptr;  // RK4 means of the training inputs
+
+  const __nv_bfloat16* w1h() const { return params_h + o_w1; }
+  const __nv_bfloat16* w2h() const { return params_h + o_w2; }
+  const __nv_bfloat16* w3h() const { return params_h + o_w3; }
+  const float* b1() const { return params + o_b1; }
+  const float* b2() const { return params + o_b2; }
+  const float* b3() const { return params + o_b3; }
+
+  int alloc(int d, int hid, int cap_batch);
+  void release();
+};
+
+// O [B x dout] = MLP(U [B x din]); H1, H2 [B x hidden] hold the activations
+int proposal_forward(ProposalNet& p, const __nv_bfloat16* U, int B, __nv_bfloat16* H1, __nv_bfloat16* H2, float* O,
+                     cudaStream_t st);
+
+// one guided filter step (guided.cu)
+struct GuidedArgs {
+  const void* x_in;  // state before the step (FP32 SoA, ld)
+  void* x_out;
+  int ld, n;
+  const int* as;
+  double* lw;
+  const void* y;     // device observation (required)
+  double t1, t2;
+  uint64_t seed;
+  int step;
+  double theta[BPF_MAX_THETA];
+  double h;
+  StepStats* stats;
+  LwPartial* partials;
+  int max_partials;
+  unsigned* counter;
+  // scratch: M [dim x ld] FP32, U [ld x din] BF16, H1/H2 [ld x hidden] BF16,
+  // O [dout x ld] FP32
+  float* M;
+  __nv_bfloat16 *U, *H1, *H2;
+  float* O;
+};
+int launch_guided(ProposalNet& net, const GuidedArgs& a, cudaStream_t st);
+
+}  // namespace bpf
+
+struct bpf_proposal;
+namespace bpf {
+ProposalNet* proposal_net(bpf_proposal* q);
+double proposal_dt(bpf_proposal* q);
+}  // namespace bpf

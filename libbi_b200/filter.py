@@ -321,6 +321,12 @@ class BootstrapPF:
                                    ctypes.byref(ll)), "bpf_filter")
         return ll.value, inc, ess
 
+    def set_proposal(self, proposal):
+        """Attach a LearnedProposal (or None to detach): observed steps then
+        propose from it and correct the weights by importance sampling."""
+        N.check(N.lib().bpf_set_proposal(self._h, None if proposal is None else proposal.handle), "bpf_set_proposal")
+        self._proposal = proposal
+
     def reduce(self):
         lW, ess = ctypes.c_double(), ctypes.c_double()
         N.check(N.lib().bpf_reduce(self._h, ctypes.byref(lW), ctypes.byref(ess)), "bpf_reduce")
