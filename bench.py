@@ -357,6 +357,73 @@ def pmmh_chains(iterations=20, nchains=128, nparticles=2048, T=100):
     }
 
 
+def guided_vs_bootstrap(y_host, seeds=64, n_guided=4096, n_boot=65536, n_data=1 << 20, train_steps=3000):
+    """The learned proposal on the Lorenz-96 workload: trained on 2^20
+    (x_t, x_{t+1}, y_{t+1}) triples simulated by the model (2^20 particles
+    spun up for 100 intervals from the initial distribution, one more
+    interval, observations with N(0, 1) noise), then the guided filter at
+    N = 4096 against the bootstrap filter at N = 65536 on the bench's T = 200
+    observations over 64 seeds: standard deviation of the log-likelihood
+    estimate and device time per filter run (CUDA events around each step's
+    kernels).  Monte Carlo variance falls as 1/N, so the guided filter
+    reaches the bootstrap's deviation in t_g * (sd_g / sd_b)^2."""
+    import numpy as np
+    import torch
+    from libbi_b200 import BootstrapPF, LearnedProposal, configs
+
+    model = configs.L96_D40_N65536["model"]
+    sim = BootstrapPF(model, n_data, seed=3)
+    for k in range(100):
+        sim.step_device(k * DT, (k + 1) * DT, None, sync=False)
+    x, _, _ = sim.state()
+    xt = x[:, :n_data].T.contiguous().clone()
+    sim.step_device(100 * DT, 101 * DT, None, sync=False)
+    x, _, _ = sim.state()
+    xt1 = x[:, :n_data].T.contiguous().clone()
+    g = torch.Generator(device="cuda")
+    g.manual_seed(3)
+    yt1 = (xt1 + model.sigma_y * torch.randn(xt1.shape, generator=g, device="cuda")).contiguous()
+    sim.close()
+    prop = LearnedProposal(model, DT, max_batch=8192, seed=3)
+    prop.set_data(xt, xt1, yt1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    trace = prop.train(train_steps, 8192, 2e-3)
+    train_s = time.perf_counter() - t0
+    del xt, xt1, yt1
+
+    def run(n, use_prop):
+        lls, ms = [], 0.0
+        for s in range(seeds):
+            pf = BootstrapPF(model, n, resampler="systematic", ess_rel=ESS_REL, seed=10_000 + s)
+            if use_prop:
+                pf.set_proposal(prop)
+            pf.timing(True)
+            ll, _, _ = pf.filter(y_host, 0.0, DT)
+            r, t, _ = pf.timing_read(reset=True)
+            ms += r + t
+            lls.append(ll)
+            pf.close()
+        return np.array(lls), ms / seeds
+
+    llg, msg = run(n_guided, True)
+    llb, msb = run(n_boot, False)
+    prop.close()
+    sdg, sdb = float(llg.std(ddof=1)), float(llb.std(ddof=1))
+    t_match = msg * (sdg / sdb) ** 2 if sdb > 0 else float("nan")
+    return {
+        "workload": "l96_d40_t200_guided_n4096_vs_bootstrap_n65536_64seeds",
+        "train": {"triples": n_data, "steps": train_steps, "batch": 8192, "seconds": train_s,
+                  "loss_first": float(trace[:10].mean()), "loss_last": float(trace[-50:].mean()),
+                  "loss_optimal_approx": float(40 * (np.log(0.1 / np.sqrt(1.01)) + 0.5))},
+        "guided": {"n": n_guided, "ll_mean": float(llg.mean()), "ll_sd": sdg, "ms_per_run": msg},
+        "bootstrap": {"n": n_boot, "ll_mean": float(llb.mean()), "ll_sd": sdb, "ms_per_run": msb},
+        "guided_ms_to_bootstrap_sd": t_match,
+        "gpu_time_ratio_bootstrap_over_guided_at_equal_sd": msb / t_match if t_match > 0 else None,
+        "timer": "CUDA events around each step's kernels, summed per filter run",
+    }
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -391,6 +458,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-large-n", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-guided", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -525,6 +593,8 @@ def main():
     if rank == 0 and not args.no_batched:
         line["batched"] = batched_filters()
         line["pmmh"] = pmmh_chains()
+    if rank == 0 and not args.no_guided:
+        line["guided"] = guided_vs_bootstrap(y_host)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(y_host)
     pf.close()
