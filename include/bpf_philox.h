@@ -35,7 +35,8 @@ enum {
   BPF_RNG_MULTINOMIAL = 3,  /* the n uniforms of a multinomial resample */
   BPF_RNG_METROPOLIS = 4,   /* the 2*B uniforms per particle of a Metropolis resample */
   BPF_RNG_DATA = 5,         /* synthetic data generation */
-  BPF_RNG_PMMH = 6          /* PMMH proposals, acceptance draws and initial parameters */
+  BPF_RNG_PMMH = 6,         /* PMMH proposals, acceptance draws and initial parameters */
+  BPF_RNG_PATH = 7          /* the particle a sampled path ends in */
 };
 
 typedef struct { uint32_t v[4]; } bpf_u32x4;

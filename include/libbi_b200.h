@@ -178,6 +178,24 @@ int bpf_resample(bpf_handle* h, const double* uniforms, int* ancestors_out);
 int bpf_timing_enable(bpf_handle* h, int enable);
 int bpf_timing_read(bpf_handle* h, int reset, double* resample_ms, double* transition_ms, int* steps);
 
+/* Path output (BootstrapPFCache::writeState + AncestryCache,
+ * share/src/bi/cache/BootstrapPFCache.hpp:182-210; BootstrapPF::samplePath,
+ * share/src/bi/filter/BootstrapPF.hpp:148-154).  bpf_path_cache reserves
+ * room for max_steps steps (0 frees it) and records the current state; every
+ * later step (and bpf_init, which restarts the record) appends its state and
+ * ancestors.  The whole history is kept in device memory (no pruning):
+ * (max_steps + 1) x dim x ld values plus max_steps x ld ancestors. */
+int bpf_path_cache(bpf_handle* h, int max_steps);
+/* samplePath: p ~ multinomial(exp(lw)) over the current log-weights
+ * (RngHost::multinomial, share/src/bi/host/random/RngHost.hpp:120-139) from
+ * one uniform (u: device pointer, or NULL for the handle's own draw), then
+ * the state path of p back through the recorded ancestors
+ * (AncestryCache::readPath, share/src/bi/cache/AncestryCache.hpp:294-311).
+ * path: host, len x dim in the model precision, oldest first; particle and
+ * len: host.  BPF_E_TOO_LARGE when more steps were taken than the cache
+ * holds. */
+int bpf_sample_path(bpf_handle* h, const double* u, void* path, int* particle, int* len);
+
 /* ---- stand-alone primitives (the Resampler<R> and gather APIs) -------- */
 
 typedef struct bpf_resampler bpf_resampler;

@@ -9,6 +9,7 @@
 // kernels on the handle's stream; nothing returns to the host unless asked.
 #include "internal.cuh"
 #include "proposal.cuh"
+#include "resample_common.cuh"
 
 #include <cstdio>
 #include <cstring>
@@ -44,6 +45,14 @@ struct bpf_handle {
   float* g_M = nullptr;
   __nv_bfloat16 *g_U = nullptr, *g_H1 = nullptr, *g_H2 = nullptr;
   float* g_O = nullptr;
+  // path cache (bpf_path_cache): pc_len states of dim x ld in the model
+  // precision (slot 0 the state the recording started from, slot t the state
+  // after t more steps) and the ancestors of each recorded step
+  void* pc_x = nullptr;
+  int* pc_a = nullptr;
+  int pc_cap = 0;   // steps that fit
+  int pc_len = 0;   // states recorded
+  bool pc_full = false;
 };
 
 struct bpf_resampler {
@@ -112,6 +121,32 @@ int timing_event(bpf_handle* h, int which) {
   return BPF_OK;
 }
 
+// ancestors of the step just taken, in the previous state's indexing
+__global__ void k_record_ancestors(const bpf::StepStats* st, const int* as, int* out, int n) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < n) out[p] = st->resampled ? as[p] : p;
+}
+
+// append the handle's current state (and, after a step, its ancestors) to
+// the path cache
+int path_record(bpf_handle* h, bool after_step) {
+  if (!h->pc_x || h->pc_full) return BPF_OK;
+  if (h->pc_len > h->pc_cap) {
+    h->pc_full = true;
+    return BPF_OK;
+  }
+  const size_t slot = (size_t)h->dim * h->ld * h->esz;
+  BPF_TRY(cudaMemcpyAsync((char*)h->pc_x + (size_t)h->pc_len * slot, h->x[h->cur], slot, cudaMemcpyDeviceToDevice,
+                          h->stream));
+  if (after_step && h->pc_len > 0) {
+    k_record_ancestors<<<(h->n + 255) / 256, 256, 0, h->stream>>>(h->rs.stats, h->as,
+                                                                  h->pc_a + (size_t)(h->pc_len - 1) * h->ld, h->n);
+    BPF_TRY(cudaGetLastError());
+  }
+  ++h->pc_len;
+  return BPF_OK;
+}
+
 int enqueue_step(bpf_handle* h, double t1, double t2, const void* y_dev) {
   const int k = h->step + 1;
   if (h->timing) {
@@ -174,7 +209,7 @@ int enqueue_step(bpf_handle* h, double t1, double t2, const void* y_dev) {
     }
     h->cur ^= 1;
     h->step = k;
-    return BPF_OK;
+    return path_record(h, true);
   }
   bpf::TransitionArgs ta;
   ta.x_in = h->x[h->cur];
@@ -201,7 +236,7 @@ int enqueue_step(bpf_handle* h, double t1, double t2, const void* y_dev) {
   }
   h->cur ^= 1;
   h->step = k;
-  return BPF_OK;
+  return path_record(h, true);
 }
 
 __global__ void k_record(const bpf::StepStats* st, double* hist, int k) {
@@ -291,11 +326,140 @@ int bpf_destroy(bpf_handle* h) {
   if (h->y_dev) cudaFree(h->y_dev);
   if (h->hist) cudaFree(h->hist);
   for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
-  void* g[] = {h->g_M, h->g_U, h->g_H1, h->g_H2, h->g_O};
+  void* g[] = {h->g_M, h->g_U, h->g_H1, h->g_H2, h->g_O, h->pc_x, h->pc_a};
   for (void* p : g)
     if (p) cudaFree(p);
   bpf::scratch_free(h->rs);
   delete h;
+  return BPF_OK;
+}
+
+// ---- path cache and samplePath --------------------------------------------
+
+}  // extern "C"
+
+namespace {
+
+constexpr int kPathThreads = 1024;
+
+// p ~ multinomial(exp(lw)) from one uniform u, as RngHost::multinomial
+// (share/src/bi/host/random/RngHost.hpp:120-139): Ps = inclusive scan of
+// exp(lw - max) (here exact fixed-point sums rounded once), x = Ps_last * u,
+// p = first index with Ps_p >= x; p = 0 when the weights sum to zero.
+__global__ void __launch_bounds__(kPathThreads)
+k_sample_index(const double* __restrict__ lw, int n, const double* u_in, uint64_t seed, int step, int* out) {
+  __shared__ double s_max[kPathThreads / 32];
+  __shared__ int s_best;
+  const int IT = (n + kPathThreads - 1) / kPathThreads;
+  const int i0 = min(n, (int)threadIdx.x * IT), i1 = min(n, i0 + IT);
+  double m = -INFINITY;
+  for (int i = i0; i < i1; ++i) m = bpf::nan_max(m, lw[i]);
+  for (int d = 16; d > 0; d >>= 1) m = bpf::nan_max(m, __shfl_xor_sync(0xffffffffu, m, d));
+  if ((threadIdx.x & 31) == 0) s_max[threadIdx.x >> 5] = m;
+  if (threadIdx.x == 0) s_best = n;
+  __syncthreads();
+  double mx = -INFINITY;
+  for (int w = 0; w < kPathThreads / 32; ++w) mx = bpf::nan_max(mx, s_max[w]);
+  bpf::u128 acc = bpf::u128_zero();
+  for (int i = i0; i < i1; ++i) {
+    bpf::u128 q; q.lo = bpf::weight_to_fixed(bpf::nanexp(__dsub_rn(lw[i], mx))); q.hi = 0;
+    acc = bpf::u128_add(acc, q);
+  }
+  bpf::u128 tot;
+  bpf::u128 Q = bpf::block_exclusive_scan_u128_nt<kPathThreads>(acc, &tot);
+  const double W = bpf::u128_to_weight(tot);
+  double u;
+  if (u_in) {
+    u = *u_in;
+  } else {
+    bpf_u32x4 r = bpf_draw(seed, 0u, (uint32_t)step, 0u, BPF_RNG_PATH);
+    u = bpf_u01d(r.v[0], r.v[1]);
+  }
+  if (!(W > 0.0)) {
+    if (threadIdx.x == 0) *out = 0;
+    return;
+  }
+  const double x = __dmul_rn(W, u);
+  for (int i = i0; i < i1; ++i) {
+    bpf::u128 q; q.lo = bpf::weight_to_fixed(bpf::nanexp(__dsub_rn(lw[i], mx))); q.hi = 0;
+    Q = bpf::u128_add(Q, q);
+    if (bpf::u128_to_weight(Q) >= x) {
+      atomicMin(&s_best, i);
+      break;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *out = s_best < n ? s_best : n - 1;
+}
+
+// AncestryCache::readPath (share/src/bi/cache/AncestryCache.hpp:294-311):
+// from the final particle back through the recorded ancestors
+template <class T>
+__global__ void k_trace_path(const T* __restrict__ X, const int* __restrict__ A, int len, int dim, int ld,
+                             const int* p_in, T* path) {
+  int a = *p_in;
+  for (int t = len - 1; t >= 0; --t) {
+    for (int i = threadIdx.x; i < dim; i += blockDim.x)
+      path[(size_t)t * dim + i] = X[((size_t)t * dim + i) * ld + a];
+    if (t > 0) a = A[(size_t)(t - 1) * ld + a];
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int bpf_path_cache(bpf_handle* h, int max_steps) {
+  if (!h || max_steps < 0) return BPF_E_INVALID;
+  BPF_TRY(cudaStreamSynchronize(h->stream));
+  if (h->pc_x) cudaFree(h->pc_x);
+  if (h->pc_a) cudaFree(h->pc_a);
+  h->pc_x = nullptr;
+  h->pc_a = nullptr;
+  h->pc_cap = 0;
+  h->pc_len = 0;
+  h->pc_full = false;
+  if (max_steps == 0) return BPF_OK;
+  const size_t slot = (size_t)h->dim * h->ld * h->esz;
+  if (cudaMalloc(&h->pc_x, (size_t)(max_steps + 1) * slot) != cudaSuccess ||
+      cudaMalloc((void**)&h->pc_a, (size_t)max_steps * h->ld * sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    if (h->pc_x) cudaFree(h->pc_x);
+    h->pc_x = nullptr;
+    return BPF_E_NOMEM;
+  }
+  h->pc_cap = max_steps;
+  return path_record(h, false);  // the current state opens the record
+}
+
+int bpf_sample_path(bpf_handle* h, const double* u, void* path, int* particle, int* len) {
+  if (!h || !h->pc_x || h->pc_len == 0) return BPF_E_INVALID;
+  if (h->pc_full) return BPF_E_TOO_LARGE;
+  if (len) *len = h->pc_len;
+  int* d_p = nullptr;
+  void* d_path = nullptr;
+  const size_t pb = (size_t)h->pc_len * h->dim * h->esz;
+  if (cudaMalloc((void**)&d_p, sizeof(int)) != cudaSuccess || cudaMalloc(&d_path, pb) != cudaSuccess) {
+    cudaGetLastError();
+    if (d_p) cudaFree(d_p);
+    return BPF_E_NOMEM;
+  }
+  k_sample_index<<<1, kPathThreads, 0, h->stream>>>(h->lw, h->n, u, h->cfg.seed, h->step, d_p);
+  if (h->esz == 4)
+    k_trace_path<float><<<1, 64, 0, h->stream>>>((const float*)h->pc_x, h->pc_a, h->pc_len, h->dim, h->ld, d_p,
+                                                 (float*)d_path);
+  else
+    k_trace_path<double><<<1, 64, 0, h->stream>>>((const double*)h->pc_x, h->pc_a, h->pc_len, h->dim, h->ld, d_p,
+                                                  (double*)d_path);
+  int p = 0;
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&p, d_p, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess && path) e = cudaMemcpyAsync(path, d_path, pb, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(d_p);
+  cudaFree(d_path);
+  if (e != cudaSuccess) { bpf_set_last_cuda_error(e); return BPF_E_CUDA; }
+  if (particle) *particle = p;
   return BPF_OK;
 }
 
@@ -339,8 +503,12 @@ int bpf_init(bpf_handle* h) {
   if (!h) return BPF_E_INVALID;
   h->cur = 0;
   h->step = 0;
-  return bpf::launch_init(h->model, h->x[0], h->ld, h->n, h->lw, h->cfg.seed, h->rs.stats, h->cfg.ess_rel,
-                          h->stream);
+  int rc = bpf::launch_init(h->model, h->x[0], h->ld, h->n, h->lw, h->cfg.seed, h->rs.stats, h->cfg.ess_rel,
+                            h->stream);
+  if (rc) return rc;
+  h->pc_len = 0;
+  h->pc_full = false;
+  return path_record(h, false);
 }
 
 static void fill_out(const bpf::StepStats& s, bpf_step_out* out) {

@@ -321,6 +321,22 @@ class BootstrapPF:
                                    ctypes.byref(ll)), "bpf_filter")
         return ll.value, inc, ess
 
+    def path_cache(self, max_steps: int):
+        """Record states and ancestors of up to max_steps steps (0: stop)."""
+        N.check(N.lib().bpf_path_cache(self._h, max_steps), "bpf_path_cache")
+        self._path_steps = max_steps
+
+    def sample_path(self, u=None):
+        """BootstrapPF::samplePath: (particle, path[len, dim]) with the path of
+        a particle drawn from the current weights (u: device tensor with one
+        uniform, or None for the handle's own draw)."""
+        cap = getattr(self, "_path_steps", 0)
+        buf = np.zeros((cap + 1, self.model.dim), dtype=self.model.np_dtype)
+        p, n = ctypes.c_int(), ctypes.c_int()
+        N.check(N.lib().bpf_sample_path(self._h, _ptr(u), buf.ctypes.data_as(ctypes.c_void_p), ctypes.byref(p),
+                                        ctypes.byref(n)), "bpf_sample_path")
+        return p.value, buf[:n.value]
+
     def set_proposal(self, proposal):
         """Attach a LearnedProposal (or None to detach): observed steps then
         propose from it and correct the weights by importance sampling."""
