@@ -143,6 +143,15 @@ int bpf_init(bpf_handle* h);
  * step.  out may be NULL (no sync). */
 int bpf_step(bpf_handle* h, double t1, double t2, const void* y, bpf_step_out* out);
 
+/* bpf_step with only some components observed: the observation Mask of
+ * Observer::getMask / SparseStaticLogDensity (share/src/bi/state/Mask.hpp:26-203,
+ * share/src/bi/simulator/Observer.hpp:97-126).  y: host, nidx values in the
+ * model precision for the components idx[0..nidx) (distinct, < 64); nidx = 0
+ * is an unobserved step.  A filter with a learned proposal proposes from the
+ * transition on such steps. */
+int bpf_step_sparse(bpf_handle* h, double t1, double t2, const void* y, const int* idx, int nidx,
+                    bpf_step_out* out);
+
 /* bpf_step with the observation already in device memory (or NULL): no
  * host-to-device copy is enqueued. */
 int bpf_step_device(bpf_handle* h, double t1, double t2, const void* y_device, bpf_step_out* out);

@@ -49,7 +49,7 @@ EXPORTS = (
     "bpf_pmmh_create", "bpf_pmmh_destroy", "bpf_pmmh_run", "bpf_pmmh_state", "bpf_dense_bf16",
     "bpf_proposal_create", "bpf_proposal_destroy", "bpf_proposal_set_data", "bpf_proposal_train",
     "bpf_proposal_loss_grad", "bpf_proposal_params", "bpf_proposal_set_params", "bpf_set_proposal",
-    "bpf_path_cache", "bpf_sample_path",
+    "bpf_path_cache", "bpf_sample_path", "bpf_step_sparse",
 )
 
 
@@ -160,6 +160,7 @@ def _declare(L):
         "bpf_proposal_set_params": (c_int, [H, c_void_p, c_void_p, c_void_p]),
         "bpf_set_proposal": (c_int, [H, H]),
         "bpf_path_cache": (c_int, [H, c_int]),
+        "bpf_step_sparse": (c_int, [H, c_double, c_double, c_void_p, c_void_p, c_int, POINTER(StepOut)]),
         "bpf_sample_path": (c_int, [H, c_void_p, c_void_p, POINTER(c_int), POINTER(c_int)]),
         "bpf_dense_bf16": (c_int, [c_void_p, c_longlong, c_longlong, c_void_p, c_longlong, c_longlong, c_int, c_int,
                                    c_int, c_void_p, c_int, c_void_p, c_longlong, c_void_p, c_longlong, c_void_p,

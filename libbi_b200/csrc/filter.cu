@@ -147,7 +147,7 @@ int path_record(bpf_handle* h, bool after_step) {
   return BPF_OK;
 }
 
-int enqueue_step(bpf_handle* h, double t1, double t2, const void* y_dev) {
+int enqueue_step(bpf_handle* h, double t1, double t2, const void* y_dev, uint64_t mask = ~0ull) {
   const int k = h->step + 1;
   if (h->timing) {
     int rc = timing_event(h, 0);
@@ -173,8 +173,9 @@ int enqueue_step(bpf_handle* h, double t1, double t2, const void* y_dev) {
     rc = timing_event(h, 1);
     if (rc) return rc;
   }
-  if (h->prop && y_dev) {
-    // guided step: the learned proposal instead of the transition
+  if (h->prop && y_dev && (mask | ~((h->dim >= 64 ? 0ull : (1ull << h->dim)) - 1ull)) == ~0ull) {
+    // guided step (every component observed): the learned proposal instead
+    // of the transition
     const double dt = bpf::proposal_dt(h->prop);
     if (std::fabs((t2 - t1) - dt) > 1e-9 * dt) return BPF_E_INVALID;
     bpf::GuidedArgs ga;
@@ -227,6 +228,7 @@ int enqueue_step(bpf_handle* h, double t1, double t2, const void* y_dev) {
   ta.partials = h->rs.partials;
   ta.max_partials = h->rs.max_partials;
   ta.counter = h->rs.counters + 4;
+  ta.obs_mask = mask;
   rc = bpf::launch_transition(h->model, ta, h->stream);
   if (rc) return rc;
   if (h->timing) {
@@ -531,6 +533,38 @@ int bpf_step(bpf_handle* h, double t1, double t2, const void* y, bpf_step_out* o
     yd = h->y_dev;
   }
   int rc = enqueue_step(h, t1, t2, yd);
+  if (rc) return rc;
+  if (out) {
+    bpf::StepStats s;
+    rc = read_stats(h, &s);
+    if (rc) return rc;
+    fill_out(s, out);
+    return s.status;
+  }
+  return BPF_OK;
+}
+
+int bpf_step_sparse(bpf_handle* h, double t1, double t2, const void* y, const int* idx, int nidx, bpf_step_out* out) {
+  if (!h || !(t1 < t2) || nidx < 0 || (nidx > 0 && (!y || !idx))) return BPF_E_INVALID;
+  const int nob = nobs(h);
+  if (nob > 64) return BPF_E_INVALID;
+  uint64_t mask = 0;
+  std::vector<unsigned char> dense((size_t)nob * h->esz, 0);
+  for (int j = 0; j < nidx; ++j) {
+    const int i = idx[j];
+    if (i < 0 || i >= nob || ((mask >> i) & 1ull)) return BPF_E_INVALID;
+    mask |= 1ull << i;
+    std::memcpy(&dense[(size_t)i * h->esz], (const unsigned char*)y + (size_t)j * h->esz, h->esz);
+  }
+  const void* yd = nullptr;
+  if (nidx > 0) {
+    int rc = ensure_y(h, dense.size());
+    if (rc) return rc;
+    BPF_TRY(cudaMemcpyAsync(h->y_dev, dense.data(), dense.size(), cudaMemcpyHostToDevice, h->stream));
+    BPF_TRY(cudaStreamSynchronize(h->stream));  // dense is a temporary
+    yd = h->y_dev;
+  }
+  int rc = enqueue_step(h, t1, t2, yd, mask);
   if (rc) return rc;
   if (out) {
     bpf::StepStats s;

@@ -261,6 +261,7 @@ struct TransitionArgs {
   LwPartial* partials;
   int max_partials;   // capacity of partials (one per block)
   unsigned* counter;
+  uint64_t obs_mask = ~0ull;  // bit i: component i observed (when y is given)
 };
 int launch_transition(const ModelArgs& m, const TransitionArgs& a, cudaStream_t st);
 int launch_init(const ModelArgs& m, void* x, int ld, int n, double* lw, uint64_t seed,

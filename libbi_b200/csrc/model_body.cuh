@@ -115,12 +115,15 @@ __device__ __forceinline__ void l96_rk4(T (&x0)[D], double t1d, double t2d, T F,
 // lp += -0.5*((y - x)/sigma)^2 - BI_HALF_LOG_TWO_PI - log(sigma), four
 // components per Philox block, in component order.  The integrated state is
 // staged in sx[.][threadIdx.x]; the new state goes to x_out[i*ld + p_out];
-// prng is the particle's index in its filter's random stream.  Returns l plus
-// the observation terms.
+// prng is the particle's index in its filter's random stream; bit i of mask
+// says whether component i is observed (the observation Mask of
+// SparseStaticLogDensity, share/src/bi/state/Mask.hpp).  Returns l plus the
+// observation terms.
 template <class T, int D>
 __device__ __forceinline__ double l96_noise_obs(const T (&sx)[D][kL96Block], T* __restrict__ x_out, size_t ld,
                                                 int p_out, const T* __restrict__ y, uint64_t seed, uint32_t prng,
-                                                int step, const L96Params& prm, double l) {
+                                                int step, const L96Params& prm, double l,
+                                                uint64_t mask = ~0ull) {
   const T se = (T)prm.sigma_eta;
   const T sy = (T)prm.sigma_y, isy = (T)prm.inv_sigma_y;
   const T c2 = (T)prm.c_half_log_2pi, ls = (T)prm.log_sigma_y;
@@ -136,7 +139,7 @@ __device__ __forceinline__ double l96_noise_obs(const T (&sx)[D][kL96Block], T* 
       if (i < D) {
         const T xi = Prec<T>::add_(sx[i][threadIdx.x], Prec<T>::mul_(se, z[j]));
         x_out[(size_t)i * ld + p_out] = xi;
-        if (y) {
+        if (y && ((mask >> i) & 1ull)) {
           T dz = __ldg(y + i) - xi;
           dz = isy != (T)0 ? dz * isy : dz / sy;
           T term = Prec<T>::fma_((T)-0.5, dz * dz, -c2) - ls;

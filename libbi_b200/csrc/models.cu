@@ -22,7 +22,7 @@ __global__ void __launch_bounds__(kL96Block, (sizeof(T) == 4 && D <= 40 ? 8 : 4)
 k_l96_transition(const T* __restrict__ x_in, T* __restrict__ x_out, int ld, int n,
                  int* __restrict__ as, double* __restrict__ lw, const T* __restrict__ y,
                  double t1d, double t2d, uint64_t seed, int step, L96Params prm,
-                 StepStats* st, LwPartial* partials, unsigned* counter) {
+                 StepStats* st, LwPartial* partials, unsigned* counter, uint64_t mask) {
   // state staged here for the rolled noise/observation epilogue
   __shared__ T sx[D][kL96Block];
   const int p = blockIdx.x * kL96Block + threadIdx.x;
@@ -39,7 +39,7 @@ k_l96_transition(const T* __restrict__ x_in, T* __restrict__ x_out, int ld, int 
 #pragma unroll
     for (int i = 0; i < D; ++i) sx[i][threadIdx.x] = x0[i];
     const double l = l96_noise_obs<T, D>(sx, x_out, (size_t)ld, p, y, seed, (uint32_t)p, step, prm,
-                                         resampled ? ll : lw[p]);
+                                         resampled ? ll : lw[p], mask);
     lw[p] = l;
     if (resampled) as[p] = src;
     lw_push(part, l);
@@ -52,7 +52,7 @@ __global__ void __launch_bounds__(kPZBlock)
 k_pz_transition(const T* __restrict__ x_in, T* __restrict__ x_out, int ld, int n,
                 int* __restrict__ as, double* __restrict__ lw, const T* __restrict__ y,
                 double t1d, double t2d, uint64_t seed, int step, PZParams prm,
-                StepStats* st, LwPartial* partials, unsigned* counter) {
+                StepStats* st, LwPartial* partials, unsigned* counter, uint64_t mask) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   const int resampled = st->resample;
   const bool ok = st->status == BPF_OK;
@@ -63,7 +63,7 @@ k_pz_transition(const T* __restrict__ x_in, T* __restrict__ x_out, int ld, int n
     const T alpha = pz_alpha<T>(seed, (uint32_t)p, step, prm);
     pz_advance<T>(P, Z, alpha, t1d, t2d, prm);
     double l = resampled ? st->ll : lw[p];
-    if (y) l += pz_obs_term<T>(P, __ldg(y), prm);
+    if (y && (mask & 1ull)) l += pz_obs_term<T>(P, __ldg(y), prm);
     x_out[p] = P;
     x_out[(size_t)ld + p] = Z;
     lw[p] = l;
@@ -115,7 +115,8 @@ __global__ void k_stats_init(StepStats* st, int n, double ess_rel) {
 #define L96_CASE(DD)                                                                                   \
   case DD:                                                                                             \
     k_l96_transition<T, DD><<<blocks, kL96Block, 0, st>>>((const T*)a.x_in, (T*)a.x_out, a.ld, a.n,          \
-        (int*)a.as, a.lw, (const T*)a.y, a.t1, a.t2, a.seed, a.step, prm, a.stats, a.partials, a.counter); \
+        (int*)a.as, a.lw, (const T*)a.y, a.t1, a.t2, a.seed, a.step, prm, a.stats, a.partials, a.counter,     \
+        a.obs_mask);                                                                                   \
     break;
 
 template <class T>
@@ -140,7 +141,7 @@ static int transition_t(const ModelArgs& m, const TransitionArgs& a, cudaStream_
     PZParams prm = pz_params<T>(m.theta, m.h, m.atoler, m.rtoler);
     k_pz_transition<T><<<blocks, kPZBlock, 0, st>>>((const T*)a.x_in, (T*)a.x_out, a.ld, a.n, (int*)a.as, a.lw,
                                                (const T*)a.y, a.t1, a.t2, a.seed, a.step, prm, a.stats,
-                                               a.partials, a.counter);
+                                               a.partials, a.counter, a.obs_mask);
   } else {
     return BPF_E_INVALID;
   }

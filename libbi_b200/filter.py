@@ -299,6 +299,18 @@ class BootstrapPF:
         N.check(N.lib().bpf_step(self._h, t1, t2, p, ctypes.byref(out)), "bpf_step")
         return StepResult(out.ess, out.log_weight_sum, out.log_increment, out.log_likelihood, bool(out.resampled))
 
+    def step_sparse(self, t1: float, t2: float, y, idx) -> StepResult:
+        """BootstrapPF::step to an observation of the components idx only."""
+        vals = np.ascontiguousarray(np.asarray(y, dtype=self.model.np_dtype).reshape(-1))
+        ix = np.ascontiguousarray(np.asarray(idx, dtype=np.int32).reshape(-1))
+        if vals.size != ix.size:
+            raise ValueError("one value per observed component")
+        out = N.StepOut()
+        N.check(N.lib().bpf_step_sparse(self._h, t1, t2, vals.ctypes.data_as(ctypes.c_void_p),
+                                        ix.ctypes.data_as(ctypes.c_void_p), ix.size, ctypes.byref(out)),
+                "bpf_step_sparse")
+        return StepResult(out.ess, out.log_weight_sum, out.log_increment, out.log_likelihood, bool(out.resampled))
+
     def step_device(self, t1: float, t2: float, y_dev=None, sync: bool = True) -> Optional[StepResult]:
         """BootstrapPF::step with the observation already on the device."""
         if not sync:

@@ -261,7 +261,7 @@ static int is_pow2(double v) {
 /* L96 transition of one particle in float: x (d values) in/out; returns the
  * observation log-density added to base (FP64) when y != NULL. */
 static double l96_particle_f(const bpf_model_desc* m, float* x, const float* y, double t1d, double t2d,
-                             uint64_t seed, int step, uint32_t p, double base) {
+                             uint64_t seed, int step, uint32_t p, double base, uint64_t mask) {
   const int D = m->dim;
   const float F = (float)m->theta[0], h0 = (float)m->h;
   const float b1 = (float)(1.0 / 6.0), b2 = (float)(1.0 / 3.0), b3 = (float)(1.0 / 3.0), b4 = (float)(1.0 / 6.0);
@@ -303,7 +303,7 @@ static double l96_particle_f(const bpf_model_desc* m, float* x, const float* y, 
       int i = 4 * b + j;
       if (i < D) {
         x[i] = x[i] + se * z[j];
-        if (y) {
+        if (y && ((mask >> i) & 1u)) {
           float dz = y[i] - x[i];
           dz = isy != 0.0f ? dz * isy : dz / sy;
           float term = fmaf(-0.5f, dz * dz, -c2) - ls;
@@ -316,7 +316,7 @@ static double l96_particle_f(const bpf_model_desc* m, float* x, const float* y, 
 }
 
 static double l96_particle_d(const bpf_model_desc* m, double* x, const double* y, double t1d, double t2d,
-                             uint64_t seed, int step, uint32_t p, double base) {
+                             uint64_t seed, int step, uint32_t p, double base, uint64_t mask) {
   const int D = m->dim;
   const double F = m->theta[0], h0 = m->h;
   const double b1 = 1.0 / 6.0, b2 = 1.0 / 3.0, b3 = 1.0 / 3.0, b4 = 1.0 / 6.0;
@@ -358,7 +358,7 @@ static double l96_particle_d(const bpf_model_desc* m, double* x, const double* y
       int i = 4 * b + j;
       if (i < D) {
         x[i] = x[i] + se * z[j];
-        if (y) {
+        if (y && ((mask >> i) & 1u)) {
           double dz = y[i] - x[i];
           dz = isy != 0.0 ? dz * isy : dz / sy;
           double term = fma(-0.5, dz * dz, -c2) - ls;
@@ -372,7 +372,7 @@ static double l96_particle_d(const bpf_model_desc* m, double* x, const double* y
 
 /* PZ transition of one particle in FP64 (RK4(3) adaptive) */
 static double pz_particle_d(const bpf_model_desc* m, double* x, const double* y, double t1d, double t2d,
-                            uint64_t seed, int step, uint32_t p, double base) {
+                            uint64_t seed, int step, uint32_t p, double base, uint64_t mask) {
   const double c = m->theta[0], e = m->theta[1], mm = m->theta[2], q = m->theta[3];
   const double mu = m->theta[4], sigma = m->theta[5], sy = m->theta[6];
   bpf_u32x4 r = bpf_draw(seed, p, (uint32_t)step, 0u, BPF_RNG_NOISE);
@@ -454,7 +454,7 @@ static double pz_particle_d(const bpf_model_desc* m, double* x, const double* y,
   x[0] = r1P;
   x[1] = r1Z;
   double l = base;
-  if (y) {
+  if (y && (mask & 1u)) {
     double dz = y[0] - bpf_log(x[0]);
     dz = is_pow2(sy) ? dz * (1.0 / sy) : dz / sy;
     double term = fma(-0.5, dz * dz, -HALF_LOG_TWO_PI) - log(sy);
@@ -502,8 +502,10 @@ void orc_init(const bpf_model_desc* m, void* x, int ld, int n, double* lw, uint6
 
 /* One fused transition over all particles (gather from as when resampled).
  * x_in/x_out: SoA, ld; lw updated in place; base_ll used when resampled. */
-void orc_transition(const bpf_model_desc* m, const void* x_in, void* x_out, int ld, int n, int* as, int resampled,
-                    double* lw, const void* y, double t1, double t2, uint64_t seed, int step, double ll) {
+/* orc_transition with observation mask (bit i: component i observed) */
+void orc_transition_mask(const bpf_model_desc* m, const void* x_in, void* x_out, int ld, int n, int* as,
+                         int resampled, double* lw, const void* y, double t1, double t2, uint64_t seed, int step,
+                         double ll, uint64_t mask) {
   const int D = m->dim;
 #pragma omp parallel for schedule(static)
   for (int p = 0; p < n; ++p) {
@@ -512,18 +514,25 @@ void orc_transition(const bpf_model_desc* m, const void* x_in, void* x_out, int 
     if (m->precision == BPF_F32) {
       float xp[64];
       for (int i = 0; i < D; ++i) xp[i] = ((const float*)x_in)[(size_t)i * ld + src];
-      lw[p] = l96_particle_f(m, xp, (const float*)y, t1, t2, seed, step, (uint32_t)p, base);
+      lw[p] = l96_particle_f(m, xp, (const float*)y, t1, t2, seed, step, (uint32_t)p, base, mask);
       for (int i = 0; i < D; ++i) ((float*)x_out)[(size_t)i * ld + p] = xp[i];
     } else {
       double xp[64];
       for (int i = 0; i < D; ++i) xp[i] = ((const double*)x_in)[(size_t)i * ld + src];
       if (m->kind == BPF_MODEL_L96)
-        lw[p] = l96_particle_d(m, xp, (const double*)y, t1, t2, seed, step, (uint32_t)p, base);
+        lw[p] = l96_particle_d(m, xp, (const double*)y, t1, t2, seed, step, (uint32_t)p, base, mask);
       else
-        lw[p] = pz_particle_d(m, xp, (const double*)y, t1, t2, seed, step, (uint32_t)p, base);
+        lw[p] = pz_particle_d(m, xp, (const double*)y, t1, t2, seed, step, (uint32_t)p, base, mask);
       for (int i = 0; i < D; ++i) ((double*)x_out)[(size_t)i * ld + p] = xp[i];
     }
   }
+}
+
+/* One fused transition over all particles (gather from as when resampled).
+ * x_in/x_out: SoA, ld; lw updated in place; base_ll used when resampled. */
+void orc_transition(const bpf_model_desc* m, const void* x_in, void* x_out, int ld, int n, int* as, int resampled,
+                    double* lw, const void* y, double t1, double t2, uint64_t seed, int step, double ll) {
+  orc_transition_mask(m, x_in, x_out, ld, n, as, resampled, lw, y, t1, t2, seed, step, ll, ~(uint64_t)0);
 }
 
 /* ---------------------------------------------------------------- filter */
@@ -590,11 +599,11 @@ void orc_simulate(const bpf_model_desc* m, uint64_t seed, int T, double t0, doub
   for (int k = 1; k <= T; ++k) {
     /* the filter's transition with its own noise, no observation */
     if (m->precision == BPF_F32) {
-      l96_particle_f(m, (float*)xbuf, NULL, t0 + (k - 1) * dt, t0 + k * dt, seed, k, 0u, 0.0);
+      l96_particle_f(m, (float*)xbuf, NULL, t0 + (k - 1) * dt, t0 + k * dt, seed, k, 0u, 0.0, 0u);
     } else if (m->kind == BPF_MODEL_L96) {
-      l96_particle_d(m, (double*)xbuf, NULL, t0 + (k - 1) * dt, t0 + k * dt, seed, k, 0u, 0.0);
+      l96_particle_d(m, (double*)xbuf, NULL, t0 + (k - 1) * dt, t0 + k * dt, seed, k, 0u, 0.0, 0u);
     } else {
-      pz_particle_d(m, (double*)xbuf, NULL, t0 + (k - 1) * dt, t0 + k * dt, seed, k, 0u, 0.0);
+      pz_particle_d(m, (double*)xbuf, NULL, t0 + (k - 1) * dt, t0 + k * dt, seed, k, 0u, 0.0, 0u);
     }
     if (xtrue) memcpy((char*)xtrue + (size_t)(k - 1) * D * esz, xbuf, (size_t)D * esz);
     /* observation noise */

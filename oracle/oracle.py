@@ -52,6 +52,8 @@ class Oracle:
                                      c_void_p, c_double, c_double, c_uint64, c_int, c_double]
         L.orc_filter.argtypes = [c_void_p, c_void_p, c_int, c_double, c_double, c_void_p, c_void_p, c_void_p,
                                  c_void_p, POINTER(c_double), c_void_p, c_void_p]
+        L.orc_transition_mask.argtypes = [c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p, c_int, c_void_p,
+                                          c_void_p, c_double, c_double, c_uint64, c_int, c_double, c_uint64]
         L.orc_noise_normals.argtypes = [c_uint64, ctypes.c_uint32, c_int, c_int, c_int, c_void_p]
         L.orc_pmmh_draws.argtypes = [c_uint64, c_int, c_int, c_int, c_void_p, POINTER(c_double)]
         L.orc_simulate.argtypes = [c_void_p, c_uint64, c_int, c_double, c_double, c_void_p, c_void_p]
@@ -129,6 +131,16 @@ class Oracle:
         y = None if y is None else np.ascontiguousarray(y, x_in.dtype)
         self.L.orc_transition(ctypes.byref(desc), _p(x_in), _p(x_out), x_in.shape[1], n, _p(as_), int(resampled),
                               _p(lw), _p(y), t1, t2, seed, step, ll)
+        return x_out, lw
+
+    def transition_mask(self, desc, x_in, n, as_, resampled, lw, y, t1, t2, seed, step, ll, mask):
+        """transition with only the components of bitmask `mask` observed"""
+        x_out = np.zeros_like(x_in)
+        lw = lw.copy()
+        as_ = None if as_ is None else np.ascontiguousarray(as_, np.int32)
+        y = None if y is None else np.ascontiguousarray(y, x_in.dtype)
+        self.L.orc_transition_mask(ctypes.byref(desc), _p(x_in), _p(x_out), x_in.shape[1], n, _p(as_),
+                                   int(resampled), _p(lw), _p(y), t1, t2, seed, step, ll, mask)
         return x_out, lw
 
     def filter(self, desc, cfg, y, T, t0, dt):
