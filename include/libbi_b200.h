@@ -396,6 +396,39 @@ int bpf_pmmh_run(bpf_pmmh* s, int iterations, double* samples, double* log_likel
  * and the number of filter runs so far (the next run index). */
 int bpf_pmmh_state(bpf_pmmh* s, double* theta, double* log_likelihoods, double* log_priors, int* runs);
 
+/* ---- SMC^2 over the batched filter -------------------------------------- */
+/* MarginalSIR (share/src/bi/sampler/MarginalSIR.hpp:283-480): ntheta
+ * parameter particles from the priors, each with a filter of nparticles; at
+ * every observation the filters step together and each parameter particle's
+ * log-weight grows by its filter's log-likelihood increment; when the
+ * weights' ESS falls below theta_ess_rel * ntheta they are resampled
+ * (systematic) and each makes `moves` PMMH moves (a random-walk proposal
+ * filtered over the observations so far, MarginalMH's accept/reject).
+ * After a resample-move round the filters replay the observations so far
+ * from their (parameters, seed) pairs, which reproduces every
+ * log-likelihood exactly.  Seeds: see libbi_b200/csrc/smc2.cu. */
+typedef struct {
+  int ntheta;             /* parameter particles */
+  int nparticles;         /* per filter, at most BPF_BATCH_MAX_PARTICLES */
+  int resampler;          /* the filters' BPF_RESAMPLER_* */
+  int metropolis_steps;
+  double ess_rel;         /* the filters' essRel */
+  double theta_ess_rel;   /* resample the parameter particles when ESS < theta_ess_rel * ntheta */
+  int moves;              /* PMMH moves per parameter particle after a resample */
+  uint64_t seed;
+  int nparams;
+  bpf_pmmh_param params[BPF_MAX_THETA];  /* priors and random-walk steps */
+} bpf_smc2_config;
+
+/* y: host, T observations (dim values for L96, 1 for PZ) at t0+dt, ...,
+ * t0+T*dt.  Outputs (host, may be NULL): theta_out[ntheta*nparams] and
+ * log_weights[ntheta] after the last observation,
+ * log_evidence_increments[T] (the marginal likelihood's log increments),
+ * resample_steps (parameter resamples), acceptance (of the PMMH moves). */
+int bpf_smc2_run(const bpf_model_desc* model, const bpf_smc2_config* cfg, int T, double t0, double dt,
+                 const void* y, void* stream, double* theta_out, double* log_weights,
+                 double* log_evidence_increments, int* resample_steps, double* acceptance);
+
 /* ---- tensor-core dense layer (the learned proposal's arithmetic) ------- */
 /* No counterpart in the reference.  D[m, n] = act(sum_k A(m,k) B(n,k) +
  * bias[n]) for m < M, n < N <= 256, on the sm_100a tensor cores (tcgen05,

@@ -8,9 +8,9 @@ from ._native import (BpfError, ParticleFilterDegeneratedException, load_library
                       LIB_PATH, EXPORTS)
 from .filter import (BootstrapPF, ModelL96, ModelPZ, Resampler, SystematicResampler,  # noqa: F401
                      MultinomialResampler, MetropolisResampler, gather_rows, StepResult, BatchedBootstrapPF)
-from .sampler import MarginalMH, Prior  # noqa: F401
+from .sampler import MarginalMH, Prior, smc2  # noqa: F401
 from .proposal import LearnedProposal  # noqa: F401
 from . import configs  # noqa: F401
 
 __all__ = ["BootstrapPF", "ModelL96", "ModelPZ", "Resampler", "SystematicResampler", "MultinomialResampler",
-           "MetropolisResampler", "BatchedBootstrapPF", "MarginalMH", "Prior", "LearnedProposal", "gather_rows", "BpfError", "ParticleFilterDegeneratedException", "configs"]
+           "MetropolisResampler", "BatchedBootstrapPF", "MarginalMH", "Prior", "smc2", "LearnedProposal", "gather_rows", "BpfError", "ParticleFilterDegeneratedException", "configs"]

@@ -49,7 +49,7 @@ EXPORTS = (
     "bpf_pmmh_create", "bpf_pmmh_destroy", "bpf_pmmh_run", "bpf_pmmh_state", "bpf_dense_bf16",
     "bpf_proposal_create", "bpf_proposal_destroy", "bpf_proposal_set_data", "bpf_proposal_train",
     "bpf_proposal_loss_grad", "bpf_proposal_params", "bpf_proposal_set_params", "bpf_set_proposal",
-    "bpf_path_cache", "bpf_sample_path", "bpf_step_sparse",
+    "bpf_path_cache", "bpf_sample_path", "bpf_step_sparse", "bpf_smc2_run",
 )
 
 
@@ -86,6 +86,14 @@ class PmmhConfig(ctypes.Structure):
     _fields_ = [
         ("nchains", c_int), ("nparticles", c_int), ("resampler", c_int), ("metropolis_steps", c_int),
         ("ess_rel", c_double), ("seed", c_uint64), ("nparams", c_int), ("params", PmmhParam * BPF_MAX_THETA),
+    ]
+
+
+class Smc2Config(ctypes.Structure):
+    _fields_ = [
+        ("ntheta", c_int), ("nparticles", c_int), ("resampler", c_int), ("metropolis_steps", c_int),
+        ("ess_rel", c_double), ("theta_ess_rel", c_double), ("moves", c_int), ("seed", c_uint64),
+        ("nparams", c_int), ("params", PmmhParam * BPF_MAX_THETA),
     ]
 
 
@@ -160,6 +168,8 @@ def _declare(L):
         "bpf_proposal_set_params": (c_int, [H, c_void_p, c_void_p, c_void_p]),
         "bpf_set_proposal": (c_int, [H, H]),
         "bpf_path_cache": (c_int, [H, c_int]),
+        "bpf_smc2_run": (c_int, [POINTER(ModelDesc), POINTER(Smc2Config), c_int, c_double, c_double, c_void_p,
+                                 c_void_p, c_void_p, c_void_p, c_void_p, POINTER(c_int), POINTER(c_double)]),
         "bpf_step_sparse": (c_int, [H, c_double, c_double, c_void_p, c_void_p, c_int, POINTER(StepOut)]),
         "bpf_sample_path": (c_int, [H, c_void_p, c_void_p, POINTER(c_int), POINTER(c_int)]),
         "bpf_dense_bf16": (c_int, [c_void_p, c_longlong, c_longlong, c_void_p, c_longlong, c_longlong, c_int, c_int,

@@ -85,3 +85,27 @@ class MarginalMH:
         N.check(N.lib().bpf_pmmh_state(self._h, _ptr_np(th), _ptr_np(ll), _ptr_np(lp), ctypes.byref(runs)),
                 "bpf_pmmh_state")
         return th, ll, lp, runs.value
+
+
+def smc2(model, priors, y, t0: float = 0.0, dt: float = 1.0, ntheta: int = 64, nparticles: int = 1024,
+         resampler: str = "systematic", ess_rel: float = 1.0, theta_ess_rel: float = 0.5, moves: int = 1,
+         seed: int = 0, metropolis_steps: int = 0, stream=None):
+    """SMC^2 (MarginalSIR) over the batched filter: returns dict(theta[P, k],
+    log_weights[P], log_evidence_increments[T], resample_steps, acceptance)."""
+    cfg = N.Smc2Config()
+    cfg.ntheta, cfg.nparticles = ntheta, nparticles
+    cfg.resampler, cfg.metropolis_steps = RESAMPLERS[resampler], metropolis_steps
+    cfg.ess_rel, cfg.theta_ess_rel, cfg.moves, cfg.seed = ess_rel, theta_ess_rel, moves, seed
+    cfg.nparams = len(priors)
+    for j, q in enumerate(priors):
+        cfg.params[j].index, cfg.params[j].prior = q.index, _KINDS[q.kind]
+        cfg.params[j].a, cfg.params[j].b, cfg.params[j].step = q.a, q.b, q.step
+    desc = model.desc()
+    yy = np.ascontiguousarray(np.asarray(y, dtype=model.np_dtype))
+    T = yy.size // model.nobs
+    th, lw, ev = np.zeros((ntheta, len(priors))), np.zeros(ntheta), np.zeros(T)
+    nres, acc = ctypes.c_int(), ctypes.c_double()
+    N.check(N.lib().bpf_smc2_run(ctypes.byref(desc), ctypes.byref(cfg), T, t0, dt, _ptr_np(yy), stream, _ptr_np(th),
+                                 _ptr_np(lw), _ptr_np(ev), ctypes.byref(nres), ctypes.byref(acc)), "bpf_smc2_run")
+    return dict(theta=th, log_weights=lw, log_evidence_increments=ev, resample_steps=nres.value,
+                acceptance=acc.value)
