@@ -48,14 +48,25 @@ k_lw_reduce(const double* __restrict__ lw, int n, int chunk, LwPartial* partials
   const bool vec = ((reinterpret_cast<uintptr_t>(lw + begin) & 15) == 0);
   int i = begin + threadIdx.x * K;
   if (vec) {
-    for (; i + K <= end; i += blockDim.x * K) {
-      const double2* p = reinterpret_cast<const double2*>(lw + i);
+    // the next batch's loads are issued before the current batch's exps, so
+    // the memory latency overlaps the arithmetic
+    const int stride = blockDim.x * K;
+    double2 nxt[K / 2];
+    if (i + K <= end) {
+#pragma unroll
+      for (int k = 0; k < K / 2; ++k) nxt[k] = __ldg(reinterpret_cast<const double2*>(lw + i) + k);
+    }
+    while (i + K <= end) {
       double x[K];
 #pragma unroll
       for (int k = 0; k < K / 2; ++k) {
-        const double2 t = __ldg(p + k);
-        x[2 * k] = t.x;
-        x[2 * k + 1] = t.y;
+        x[2 * k] = nxt[k].x;
+        x[2 * k + 1] = nxt[k].y;
+      }
+      i += stride;
+      if (i + K <= end) {
+#pragma unroll
+        for (int k = 0; k < K / 2; ++k) nxt[k] = __ldg(reinterpret_cast<const double2*>(lw + i) + k);
       }
       lw_push_batch<K>(v, x);
     }
