@@ -24,6 +24,43 @@ namespace bpf {
 constexpr int kTcKC = 64;                         // K per staged chunk
 constexpr long long kTcWaitCycles = 2000000000ll;  // ~1 s at 2 GHz
 
+// Stage rows [r0, r0 + ROWS) x columns [k0, k0 + KC) of an operand into the
+// canonical K-major layout (zero outside rows < R, columns < K).  A
+// K-contiguous operand with 16-byte aligned rows moves 8 elements per
+// 16-byte load and store (a core-matrix row); any other goes element-wise.
+template <int ROWS>
+__device__ __forceinline__ void stage_tile(unsigned char* sdst, const __nv_bfloat16* __restrict__ src, long long rs,
+                                           long long cs, int r0, int R, int k0, int K, int vec,
+                                           __nv_bfloat16 zero) {
+  constexpr int C8 = kTcKC / 8;
+  if (vec) {
+#pragma unroll 4
+    for (int e = threadIdx.x; e < ROWS * C8; e += 128) {
+      const int r = e / C8, c = e % C8;
+      const int row = r0 + r, kk = k0 + 8 * c;
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (row < R) {
+        if (kk + 8 <= K) {
+          v = __ldg(reinterpret_cast<const uint4*>(src + row * rs + kk));
+        } else if (kk < K) {
+          __nv_bfloat16 t[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) t[j] = kk + j < K ? src[row * rs + kk + j] : zero;
+          v = *reinterpret_cast<const uint4*>(t);
+        }
+      }
+      *reinterpret_cast<uint4*>(sdst + tc::kmajor_off(r, 8 * c, kTcKC)) = v;
+    }
+  } else {
+    for (int e = threadIdx.x; e < ROWS * kTcKC; e += 128) {
+      const int r = e / kTcKC, k = e % kTcKC;
+      const int row = r0 + r, kk = k0 + k;
+      const __nv_bfloat16 v = (row < R && kk < K) ? src[row * rs + kk * cs] : zero;
+      *reinterpret_cast<__nv_bfloat16*>(sdst + tc::kmajor_off(r, k, kTcKC)) = v;
+    }
+  }
+}
+
 template <int BN>
 __global__ void __launch_bounds__(128) k_dense_tc(DenseArgs g) {
   extern __shared__ __align__(1024) unsigned char smem[];
@@ -46,18 +83,8 @@ __global__ void __launch_bounds__(128) k_dense_tc(DenseArgs g) {
   const int nchunks = (g.K + kTcKC - 1) / kTcKC;
   for (int c = 0; c < nchunks; ++c) {
     const int k0 = c * kTcKC;
-    for (int e = tid; e < 128 * kTcKC; e += 128) {
-      const int r = e / kTcKC, k = e % kTcKC;
-      const int m = m0 + r, kk = k0 + k;
-      const __nv_bfloat16 v = (m < g.M && kk < g.K) ? g.A[m * g.a_rs + kk * g.a_cs] : zero;
-      *reinterpret_cast<__nv_bfloat16*>(sA + tc::kmajor_off(r, k, kTcKC)) = v;
-    }
-    for (int e = tid; e < BN * kTcKC; e += 128) {
-      const int r = e / kTcKC, k = e % kTcKC;
-      const int kk = k0 + k;
-      const __nv_bfloat16 v = (r < g.N && kk < g.K) ? g.B[r * g.b_rs + kk * g.b_cs] : zero;
-      *reinterpret_cast<__nv_bfloat16*>(sB + tc::kmajor_off(r, k, kTcKC)) = v;
-    }
+    stage_tile<128>(sA, g.A, g.a_rs, g.a_cs, m0, g.M, k0, g.K, g.a_vec, zero);
+    stage_tile<BN>(sB, g.B, g.b_rs, g.b_cs, 0, g.N, k0, g.K, g.b_vec, zero);
     tc::fence_proxy_async();
     __syncthreads();
     if (tid == 0) {
@@ -121,8 +148,15 @@ static int launch_dense_bn(const DenseArgs& g, cudaStream_t st) {
   return BPF_OK;
 }
 
-int launch_dense(const DenseArgs& g, cudaStream_t st) {
+static int k_contiguous(const __nv_bfloat16* p, long long rs, long long cs) {
+  return cs == 1 && rs % 8 == 0 && (reinterpret_cast<uintptr_t>(p) & 15) == 0;
+}
+
+int launch_dense(const DenseArgs& g0, cudaStream_t st) {
+  DenseArgs g = g0;
   if (g.M <= 0 || g.N <= 0 || g.K <= 0 || !g.A || !g.B || !g.err || (!g.Df && !g.Dh)) return BPF_E_INVALID;
+  g.a_vec = k_contiguous(g.A, g.a_rs, g.a_cs);
+  g.b_vec = k_contiguous(g.B, g.b_rs, g.b_cs);
   const int bn = (g.N + 15) / 16 * 16;
   switch (bn) {
     case 16: return launch_dense_bn<16>(g, st);

@@ -20,6 +20,9 @@ struct DenseArgs {
   __nv_bfloat16* Dh;     // BF16 copy, or null
   long long dh_rs;
   int* err;              // set when a bounded wait gives up
+  // set by launch_dense: the operand is K-contiguous with 16-byte aligned
+  // rows, so a chunk is staged with one 16-byte load per 8 elements
+  int a_vec = 0, b_vec = 0;
 };
 
 int launch_dense(const DenseArgs& g, cudaStream_t st);
