@@ -40,11 +40,8 @@ struct bpf_handle {
   bool timing = false;
   std::vector<cudaEvent_t> ev;
   int ev_steps = 0;
-  // learned proposal (bpf_set_proposal) and its per-particle scratch
+  // learned proposal (bpf_set_proposal), owned by the caller
   bpf_proposal* prop = nullptr;
-  float* g_M = nullptr;
-  __nv_bfloat16 *g_U = nullptr, *g_H1 = nullptr, *g_H2 = nullptr;
-  float* g_O = nullptr;
   // path cache (bpf_path_cache): pc_len states of dim x ld in the model
   // precision (slot 0 the state the recording started from, slot t the state
   // after t more steps) and the ancestors of each recorded step
@@ -196,11 +193,6 @@ int enqueue_step(bpf_handle* h, double t1, double t2, const void* y_dev, uint64_
     ga.partials = h->rs.partials;
     ga.max_partials = h->rs.max_partials;
     ga.counter = h->rs.counters + 4;
-    ga.M = h->g_M;
-    ga.U = h->g_U;
-    ga.H1 = h->g_H1;
-    ga.H2 = h->g_H2;
-    ga.O = h->g_O;
     rc = bpf::launch_guided(*bpf::proposal_net(h->prop), ga, h->stream);
     if (rc) return rc;
     if (h->timing) {
@@ -328,7 +320,7 @@ int bpf_destroy(bpf_handle* h) {
   if (h->y_dev) cudaFree(h->y_dev);
   if (h->hist) cudaFree(h->hist);
   for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
-  void* g[] = {h->g_M, h->g_U, h->g_H1, h->g_H2, h->g_O, h->pc_x, h->pc_a};
+  void* g[] = {h->pc_x, h->pc_a};
   for (void* p : g)
     if (p) cudaFree(p);
   bpf::scratch_free(h->rs);
@@ -470,23 +462,7 @@ int bpf_set_proposal(bpf_handle* h, bpf_proposal* p) {
   if (p) {
     if (h->model.kind != BPF_MODEL_L96 || h->model.dim != 40 || h->model.precision != BPF_F32) return BPF_E_INVALID;
     const bpf::ProposalNet& net = *bpf::proposal_net(p);
-    if (net.dim != h->dim) return BPF_E_INVALID;
-    if (!h->g_M) {
-      const size_t L = (size_t)h->ld;
-      bool ok = cudaMalloc((void**)&h->g_M, (size_t)net.dim * L * 4) == cudaSuccess &&
-                cudaMalloc((void**)&h->g_U, L * net.din * 2) == cudaSuccess &&
-                cudaMalloc((void**)&h->g_H1, L * net.hidden * 2) == cudaSuccess &&
-                cudaMalloc((void**)&h->g_H2, L * net.hidden * 2) == cudaSuccess &&
-                cudaMalloc((void**)&h->g_O, (size_t)net.dout * L * 4) == cudaSuccess;
-      if (!ok) {
-        cudaGetLastError();
-        void* g[] = {h->g_M, h->g_U, h->g_H1, h->g_H2, h->g_O};
-        for (void* q : g)
-          if (q) cudaFree(q);
-        h->g_M = nullptr; h->g_U = nullptr; h->g_H1 = nullptr; h->g_H2 = nullptr; h->g_O = nullptr;
-        return BPF_E_NOMEM;
-      }
-    }
+    if (net.dim != h->dim || net.hidden != bpf::kProposalHidden) return BPF_E_INVALID;
   }
   h->prop = p;
   return BPF_OK;

@@ -65,7 +65,7 @@ __global__ void k_gather_batch(const float* __restrict__ xt, const float* __rest
 }
 
 __global__ void k_loss_grad(const float* __restrict__ O, const float* __restrict__ r0, int B, int D,
-                            __nv_bfloat16* dO, double* loss) {
+                            __nv_bfloat16* dO, double* loss_part) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   double l = 0.0;
   if (b < B) {
@@ -82,7 +82,7 @@ __global__ void k_loss_grad(const float* __restrict__ O, const float* __restrict
       dO[(size_t)b * 2 * D + D + i] = __float2bfloat16(inside ? (1.0f - r * r * e) * invB : 0.0f);
     }
   }
-  // block sum, one atomic per block
+  // block sum into this block's slot; k_loss_finish adds the slots in order
   __shared__ double s_l[8];
   for (int d = 16; d > 0; d >>= 1) l += __shfl_xor_sync(0xffffffffu, l, d);
   if ((threadIdx.x & 31) == 0) s_l[threadIdx.x >> 5] = l;
@@ -90,8 +90,14 @@ __global__ void k_loss_grad(const float* __restrict__ O, const float* __restrict
   if (threadIdx.x == 0) {
     double t = 0.0;
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_l[w];
-    atomicAdd(loss, t / (double)B);
+    loss_part[blockIdx.x] = t;
   }
+}
+
+__global__ void k_loss_finish(const double* __restrict__ part, int nblocks, int B, double* loss) {
+  double t = 0.0;
+  for (int b = 0; b < nblocks; ++b) t += part[b];
+  *loss = t / (double)B;
 }
 
 // dZ = dH where the layer's ReLU output is positive
@@ -101,14 +107,31 @@ __global__ void k_relu_back(const float* __restrict__ dH, const __nv_bfloat16* _
   if (i < n) dZ[i] = __float2bfloat16(__bfloat162float(H[i]) > 0.0f ? dH[i] : 0.0f);
 }
 
-// out[j] += sum_b X[b, j] over a chunk of rows per block (out zeroed first)
-__global__ void k_colsum(const __nv_bfloat16* __restrict__ X, int B, int N, float* out) {
+// column sums out[j] = sum_b X[b, j] (the bias gradients) in a fixed order,
+// so that training is reproducible: each block sums a chunk of kColChunk
+// rows into part[block][j], then one block adds the chunks in block order
+constexpr int kColChunk = 64;
+__global__ void k_colsum(const __nv_bfloat16* __restrict__ X, int B, int N, float* __restrict__ part) {
   const int j = threadIdx.x;
   if (j >= N) return;
-  const int r0 = blockIdx.x * 64, r1 = min(B, r0 + 64);
+  const int r0 = blockIdx.x * kColChunk, r1 = min(B, r0 + kColChunk);
   float s = 0.0f;
   for (int r = r0; r < r1; ++r) s += __bfloat162float(X[(size_t)r * N + j]);
-  atomicAdd(out + j, s);
+  part[(size_t)blockIdx.x * N + j] = s;
+}
+
+__global__ void k_colsum_finish(const float* __restrict__ part, int nchunks, int N, float* __restrict__ out) {
+  const int j = threadIdx.x;
+  if (j >= N) return;
+  float s = 0.0f;
+  for (int c = 0; c < nchunks; ++c) s += part[(size_t)c * N + j];
+  out[j] = s;
+}
+
+static void colsum(const __nv_bfloat16* X, int B, int N, float* part, float* out, cudaStream_t st) {
+  const int nchunks = (B + kColChunk - 1) / kColChunk;
+  k_colsum<<<nchunks, 256, 0, st>>>(X, B, N, part);
+  k_colsum_finish<<<1, 256, 0, st>>>(part, nchunks, N, out);
 }
 
 __global__ void k_adam(float* __restrict__ P, const float* __restrict__ G, float* __restrict__ M1,
@@ -162,30 +185,30 @@ static int loss_and_grad(ProposalNet& p, int B, cudaStream_t st) {
   int rc = proposal_forward(p, p.U, B, p.H1, p.H2, p.O, st);
   if (rc) return rc;
   BPF_TRY(cudaMemsetAsync(p.grads, 0, (size_t)p.nparams * sizeof(float), st));
-  BPF_TRY(cudaMemsetAsync(p.loss, 0, sizeof(double), st));
-  k_loss_grad<<<(B + 255) / 256, 256, 0, st>>>(p.O, p.r0, B, D, p.dO, p.loss);
+  const int lblocks = (B + 255) / 256;
+  k_loss_grad<<<lblocks, 256, 0, st>>>(p.O, p.r0, B, D, p.dO, p.loss_part);
+  k_loss_finish<<<1, 1, 0, st>>>(p.loss_part, lblocks, B, p.loss);
   float* g = p.grads;
   float *gW1 = g + p.o_w1, *gb1 = g + p.o_b1, *gW2 = g + p.o_w2, *gb2 = g + p.o_b2, *gW3 = g + p.o_w3,
         *gb3 = g + p.o_b3;
-  const int cs_blocks = (B + 63) / 64;
   // layer 3: O = H2 W3^T + b3
   rc = launch_dense(dense(p.dO, 1, dout, p.H2, 1, H, dout, H, B, nullptr, 0, gW3, nullptr, p.err), st);
   if (rc) return rc;
-  k_colsum<<<cs_blocks, 256, 0, st>>>(p.dO, B, dout, gb3);
+  colsum(p.dO, B, dout, p.colpart, gb3, st);
   rc = launch_dense(dense(p.dO, dout, 1, p.w3h(), 1, H, B, H, dout, nullptr, 0, p.dH, nullptr, p.err), st);
   if (rc) return rc;
   k_relu_back<<<(unsigned)(((size_t)B * H + 255) / 256), 256, 0, st>>>(p.dH, p.H2, p.dZ, (size_t)B * H);
   // layer 2: H2 = relu(H1 W2^T + b2)
   rc = launch_dense(dense(p.dZ, 1, H, p.H1, 1, H, H, H, B, nullptr, 0, gW2, nullptr, p.err), st);
   if (rc) return rc;
-  k_colsum<<<cs_blocks, 256, 0, st>>>(p.dZ, B, H, gb2);
+  colsum(p.dZ, B, H, p.colpart, gb2, st);
   rc = launch_dense(dense(p.dZ, H, 1, p.w2h(), 1, H, B, H, H, nullptr, 0, p.dH, nullptr, p.err), st);
   if (rc) return rc;
   k_relu_back<<<(unsigned)(((size_t)B * H + 255) / 256), 256, 0, st>>>(p.dH, p.H1, p.dZ, (size_t)B * H);
   // layer 1: H1 = relu(U W1^T + b1)
   rc = launch_dense(dense(p.dZ, 1, H, p.U, 1, din, H, din, B, nullptr, 0, gW1, nullptr, p.err), st);
   if (rc) return rc;
-  k_colsum<<<cs_blocks, 256, 0, st>>>(p.dZ, B, H, gb1);
+  colsum(p.dZ, B, H, p.colpart, gb1, st);
   BPF_TRY(cudaGetLastError());
   return BPF_OK;
 }
@@ -221,12 +244,15 @@ int ProposalNet::alloc(int d, int hid, int cap_batch) {
   if (!rc) rc = A((void**)&dH, (size_t)cap * hidden * 4);
   if (!rc) rc = A((void**)&dZ, (size_t)cap * hidden * 2);
   if (!rc) rc = A((void**)&r0, (size_t)cap * dim * 4);
+  if (!rc) rc = A((void**)&colpart, (size_t)((cap + kColChunk - 1) / kColChunk) * (hidden > dout ? hidden : dout) * 4);
+  if (!rc) rc = A((void**)&loss_part, (size_t)((cap + 255) / 256) * sizeof(double));
   if (rc) cudaGetLastError();
   return rc;
 }
 
 void ProposalNet::release() {
-  void* ps[] = {params, params_h, grads, m1, m2, shift, scale, err, loss, U, H1, H2, O, dO, dH, dZ, r0, mt};
+  void* ps[] = {params, params_h, grads, m1, m2, shift, scale, err, loss, U, H1, H2, O, dO, dH, dZ, r0, mt,
+                 colpart, loss_part};
   for (void* q : ps)
     if (q) cudaFree(q);
 }

@@ -27,6 +27,8 @@ struct ProposalNet {
   __nv_bfloat16 *U = nullptr, *H1 = nullptr, *H2 = nullptr, *dO = nullptr, *dZ = nullptr;
   float *O = nullptr, *dH = nullptr, *r0 = nullptr;
   float* mt = nullptr;  // RK4 means of the training inputs
+  float* colpart = nullptr;  // per-chunk column sums of the bias gradients
+  double* loss_part = nullptr;  // per-block loss sums
 
   const __nv_bfloat16* w1h() const { return params_h + o_w1; }
   const __nv_bfloat16* w2h() const { return params_h + o_w2; }
@@ -60,11 +62,6 @@ struct GuidedArgs {
   LwPartial* partials;
   int max_partials;
   unsigned* counter;
-  // scratch: M [dim x ld] FP32, U [ld x din] BF16, H1/H2 [ld x hidden] BF16,
-  // O [dout x ld] FP32
-  float* M;
-  __nv_bfloat16 *U, *H1, *H2;
-  float* O;
 };
 int launch_guided(ProposalNet& net, const GuidedArgs& a, cudaStream_t st);
 

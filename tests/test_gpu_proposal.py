@@ -63,6 +63,49 @@ def test_loss_and_gradient_match_oracle(cuda, B):
     N.lib().bpf_proposal_destroy(h)
 
 
+def _triples(model, n, dt):
+    """(x_t, x_{t+1}, y_{t+1}) simulated by the library's own model."""
+    import torch
+    from libbi_b200 import BootstrapPF
+
+    pf = BootstrapPF(model, n, seed=9)
+    for k in range(40):  # onto the attractor
+        pf.step(k * dt, (k + 1) * dt, None)
+    x, _, _ = pf.state()
+    xt = x[:, :n].T.contiguous().clone()
+    pf.step(40 * dt, 41 * dt, None)
+    x, _, _ = pf.state()
+    xt1 = x[:, :n].T.contiguous().clone()
+    g = torch.Generator(device="cuda")
+    g.manual_seed(1)
+    y = (xt1 + model.sigma_y * torch.randn(xt1.shape, generator=g, device="cuda")).contiguous()
+    pf.close()
+    return xt, xt1, y
+
+
+def test_training_is_reproducible(cuda):
+    """The same seed, data and schedule give the same loss trace and the same
+    parameters, bit for bit (no atomics in the gradient sums)."""
+    from libbi_b200 import ModelL96
+    from libbi_b200 import _native as N
+
+    model = ModelL96(dim=40, sigma_eta=0.5, sigma_y=0.1)
+    n = 1 << 14
+    xt, xt1, y = _triples(model, n, 0.05)
+    out = []
+    for _ in range(2):
+        h = _make(model, max_batch=2048)
+        N.check(N.lib().bpf_proposal_set_data(h, xt.data_ptr(), xt1.data_ptr(), y.data_ptr(), n),
+                "bpf_proposal_set_data")
+        trace = np.zeros(200, np.float32)
+        N.check(N.lib().bpf_proposal_train(h, 200, 2048, 2e-3, trace.ctypes.data), "bpf_proposal_train")
+        out.append((trace, _params(h)))
+        N.lib().bpf_proposal_destroy(h)
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+    assert out[0][0][-20:].mean() < out[0][0][:5].mean()
+
+
 def test_training_learns_the_observation_update(cuda):
     """With an informative observation (sigma_y = 0.1 against sigma_eta = 0.5)
     the optimal proposal moves most of the way to y; training from the
