@@ -7,23 +7,28 @@
 // and q = N(m(x) + delta, diag(exp(2 s))).  No counterpart in the reference;
 // the resampling before it is the bootstrap filter's.
 //
-// One launch per step, one CTA per tile of 128 particles (thread r owns
-// particle m0 + r, which is also TMEM lane r of the accumulator):
-//   1. the layer-1 weights start streaming into shared memory; each thread
+// One launch per step.  A CTA holds TILES tiles of 128 particles (thread
+// 128 j + r owns particle r of tile j, which is TMEM lane r of that tile's
+// accumulator, columns [128 j, 128 j + 128)):
+//   1. one thread starts the bulk copy of the layer-1 weight image (packed
+//      once in the canonical K-major layout) into shared memory; each thread
 //      gathers its ancestor, runs the RK4 mean m (kept in registers) and
-//      writes its network input row [x, y - m] (standardised, BF16) into the
-//      canonical K-major A tile
+//      writes its network input row [x, y - m] (standardised, BF16) into its
+//      tile's A operand
 //   2. three tcgen05 MMA chains 128 x 128 x 80, 128 x 128 x 128 and
-//      128 x 80 x 128 into one 128-column FP32 accumulator; between them the
-//      epilogue (bias, ReLU, BF16) moves the accumulator row of each thread
-//      back into shared memory as the next layer's A tile while the next
-//      layer's weights are staged
-//   3. the last epilogue reads (delta, s) from tensor memory, draws
-//      x' = m + delta + exp(s) z, writes x' and the weight, and pushes the
-//      weight into the block partial of the log-weight reduction; the last
-//      block finalises ESS, lW and the log-likelihood.
-// Shared memory: three 32 KB tiles (weights, two activations), so two CTAs
-// (256 TMEM columns) share an SM.
+//      128 x 80 x 128 per tile; as soon as a layer's MMAs are done the next
+//      layer's weights start copying, and the epilogue (bias, ReLU, BF16)
+//      moves each thread's accumulator row back into its tile as the next
+//      layer's A operand
+//   3. the last epilogue reads (delta, s) from tensor memory eight
+//      components at a time, draws x' = m + delta + exp(s) z, writes x' and
+//      the weight, and pushes the weight into the block partial of the
+//      log-weight reduction; the last block finalises ESS, lW and the
+//      log-likelihood.
+// Shared memory: the weight buffer and one 32 KB activation tile per 128
+// particles.  TILES = 2 (256 threads, 96 KB, 256 TMEM columns, at most 128
+// registers) puts 512 particles on an SM, so 65536 particles run in one wave
+// on 148 SMs; TILES = 1 spreads small filters over more SMs.
 #include "internal.cuh"
 #include "reduce.cuh"
 #include "model_body.cuh"
@@ -34,23 +39,12 @@ namespace bpf {
 
 namespace {
 
-constexpr int kGTile = 128;                        // particles per CTA
-constexpr int kGTileBytes = 128 * 128 * 2;         // one BF16 tile
-constexpr int kGSmem = 3 * kGTileBytes + 1024;     // + alignment slack
-constexpr long long kGWaitCycles = 2000000000ll;   // ~1 s at 2 GHz
+constexpr int kGTile = 128;                     // particles per tile
+constexpr int kGTileBytes = 128 * 128 * 2;      // one BF16 activation tile
+constexpr long long kGWaitCycles = 2000000000ll;  // ~1 s at 2 GHz
 
-// rows x K BF16 matrix (K-contiguous rows, 16-byte aligned) into the
-// canonical K-major layout with K columns
-template <int ROWS, int K>
-__device__ __forceinline__ void stage_weights(unsigned char* s, const __nv_bfloat16* __restrict__ w) {
-  constexpr int C8 = K / 8;
-#pragma unroll 2
-  for (int e = threadIdx.x; e < ROWS * C8; e += kGTile) {
-    const int r = e / C8, c = e % C8;
-    const uint4 v = __ldg(reinterpret_cast<const uint4*>(w + r * K + 8 * c));
-    *reinterpret_cast<uint4*>(s + tc::kmajor_off(r, 8 * c, K)) = v;
-  }
-}
+template <int TILES>
+constexpr int guided_smem() { return (1 + TILES) * kGTileBytes + 1024; }  // + alignment slack
 
 // 8 FP32 values rounded to BF16, one 16-byte core-matrix row
 __device__ __forceinline__ uint4 pack8(const float* v) {
@@ -63,24 +57,27 @@ __device__ __forceinline__ uint4 pack8(const float* v) {
   return u;
 }
 
-// one thread issues the MMA chain D = A * B^T over K (multiple of 16) and
-// commits it to the mbarrier
-template <int K, int N>
-__device__ __forceinline__ void issue_layer(uint32_t taddr, const unsigned char* sA, const unsigned char* sB,
+// one thread issues, for every tile, the MMA chain D_j = A_j * W^T over K
+// (a multiple of 16) and commits them all to the mbarrier
+template <int TILES, int K, int N>
+__device__ __forceinline__ void issue_layer(uint32_t taddr, const unsigned char* sA, const unsigned char* sW,
                                             uint64_t* mbar) {
   constexpr uint32_t idesc = tc::idesc_bf16(128, N);
   tc::fence_after_sync();
 #pragma unroll
-  for (int ks = 0; ks < K / 16; ++ks) {
-    const uint64_t ad = tc::smem_desc(tc::smem_u32(sA) + ks * 256, 128, K * 16);
-    const uint64_t bd = tc::smem_desc(tc::smem_u32(sB) + ks * 256, 128, K * 16);
-    tc::mma_bf16(taddr, ad, bd, idesc, ks > 0 ? 1u : 0u);
+  for (int j = 0; j < TILES; ++j) {
+#pragma unroll
+    for (int ks = 0; ks < K / 16; ++ks) {
+      const uint64_t ad = tc::smem_desc(tc::smem_u32(sA + j * kGTileBytes) + ks * 256, 128, K * 16);
+      const uint64_t bd = tc::smem_desc(tc::smem_u32(sW) + ks * 256, 128, K * 16);
+      tc::mma_bf16(taddr + (uint32_t)(128 * j), ad, bd, idesc, ks > 0 ? 1u : 0u);
+    }
   }
   tc::mma_commit(mbar);
 }
 
 // hidden-layer epilogue: this thread's accumulator row + bias, ReLU, BF16,
-// into row r of the next layer's A tile (K = 128)
+// into row r of its tile (K = 128)
 __device__ __forceinline__ void hidden_epilogue(uint32_t trow, const float* __restrict__ bias, unsigned char* sOut,
                                                 int r) {
 #pragma unroll 1
@@ -94,6 +91,17 @@ __device__ __forceinline__ void hidden_epilogue(uint32_t trow, const float* __re
   }
 }
 
+// thread 0 waits for the weight copy, then everyone agrees that the layer
+// can be issued (the A operands written by all threads are visible to the
+// tensor core once this returns true)
+__device__ __forceinline__ bool weights_ready(uint64_t* wbar, uint32_t parity, bool ok) {
+  tc::fence_before_sync();
+  tc::fence_proxy_async();
+  bool mine = ok;
+  if (threadIdx.x == 0 && ok) mine = tc::mbar_wait(wbar, parity, kGWaitCycles);
+  return __syncthreads_and(mine) != 0;
+}
+
 // wait for the MMA chain's commit; all threads agree on the outcome
 __device__ __forceinline__ bool layer_done(uint64_t* mbar, uint32_t parity, bool ok) {
   const bool done = ok && tc::mbar_wait(mbar, parity, kGWaitCycles);
@@ -102,39 +110,51 @@ __device__ __forceinline__ bool layer_done(uint64_t* mbar, uint32_t parity, bool
   return ok;
 }
 
-template <int D>
-__global__ void __launch_bounds__(kGTile, 2)
+struct GuidedWeights {
+  const unsigned char* packed;  // shared-memory images of W1, W2, W3
+  int pk_w1, pk_w2, pk_w3;
+  const float *b1, *b2, *b3, *shift, *scale;
+};
+
+template <int D, int TILES>
+__global__ void __launch_bounds__(kGTile * TILES, TILES == 1 ? 3 : 2)
 k_guided_fused(const float* __restrict__ x_in, float* __restrict__ x_out, int ld, int n,
                const int* __restrict__ as, double* __restrict__ lw, const float* __restrict__ y, double t1,
                double t2, uint64_t seed, int step, L96Params prm, StepStats* st, LwPartial* partials,
-               unsigned* counter, const __nv_bfloat16* __restrict__ w1, const __nv_bfloat16* __restrict__ w2,
-               const __nv_bfloat16* __restrict__ w3, const float* __restrict__ b1, const float* __restrict__ b2,
-               const float* __restrict__ b3, const float* __restrict__ shift, const float* __restrict__ scale,
-               int* err) {
+               unsigned* counter, GuidedWeights w, int* err) {
   constexpr int DIN = 2 * D, DOUT = 2 * D, H = kProposalHidden;
-  static_assert(DIN % 16 == 0 && DOUT % 16 == 0 && DIN <= H && DOUT <= H, "tile shapes");
+  constexpr uint32_t W1B = H * DIN * 2, W2B = H * H * 2, W3B = DOUT * H * 2;
+  static_assert(DIN % 16 == 0 && DOUT % 16 == 0 && DIN <= H && DOUT <= H && D % 8 == 0, "tile shapes");
   extern __shared__ unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  unsigned char* sW = smem;                    // weights of the current layer
-  unsigned char* sX = smem + kGTileBytes;      // network input, then layer-2 output
-  unsigned char* sY = smem + 2 * kGTileBytes;  // layer-1 output
-  __shared__ uint64_t mbar;
+  unsigned char* sW = smem;                // weights of the current layer
+  unsigned char* sA = smem + kGTileBytes;  // TILES activation tiles
+  __shared__ uint64_t mbar, wbar;
   __shared__ uint32_t s_taddr;
   const int tid = threadIdx.x, warp = tid >> 5;
-  const int p = blockIdx.x * kGTile + tid;
+  const int tile = tid / kGTile, r = tid % kGTile;
+  unsigned char* sT = sA + tile * kGTileBytes;  // this thread's tile
+  const int p = (blockIdx.x * TILES + tile) * kGTile + r;
   const int resampled = st->resample;
   const bool ok_in = st->status == BPF_OK;
-  if (warp == 0) tc::tmem_alloc(&s_taddr, H);
-  if (tid == 0) tc::mbar_init(&mbar, 1);
+  if (warp == 0) tc::tmem_alloc(&s_taddr, 128 * TILES);
+  if (tid == 0) {
+    tc::mbar_init(&mbar, 1);
+    tc::mbar_init(&wbar, 1);
+  }
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
   const uint32_t taddr = s_taddr;
-  const uint32_t trow = taddr + ((uint32_t)(warp * 32) << 16);  // this warp's 32 lanes
+  // this warp's 32 lanes of its tile's accumulator
+  const uint32_t trow = taddr + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(128 * tile);
   LwPartial part = lw_empty();
   bool ok = ok_in;
   if (ok) {
-    stage_weights<H, DIN>(sW, w1);
+    if (tid == 0) {
+      tc::mbar_expect_tx(&wbar, W1B);
+      tc::bulk_g2s(sW, w.packed + w.pk_w1, W1B, &wbar);
+    }
     // 1. ancestor, RK4 mean, network input row
     const bool live = p < n;
     const int src = live ? (resampled ? min(max(as[p], 0), n - 1) : p) : 0;
@@ -144,8 +164,8 @@ k_guided_fused(const float* __restrict__ x_in, float* __restrict__ x_out, int ld
 #pragma unroll
     for (int c = 0; c < D / 8; ++c) {
 #pragma unroll
-      for (int j = 0; j < 8; ++j) u[j] = (m[8 * c + j] - __ldg(shift + 8 * c + j)) * __ldg(scale + 8 * c + j);
-      *reinterpret_cast<uint4*>(sX + tc::kmajor_off(tid, 8 * c, DIN)) = pack8(u);
+      for (int j = 0; j < 8; ++j) u[j] = (m[8 * c + j] - __ldg(w.shift + 8 * c + j)) * __ldg(w.scale + 8 * c + j);
+      *reinterpret_cast<uint4*>(sT + tc::kmajor_off(r, 8 * c, DIN)) = pack8(u);
     }
     l96_rk4<float, D>(m, t1, t2, (float)prm.F, (float)prm.h);
 #pragma unroll
@@ -153,61 +173,58 @@ k_guided_fused(const float* __restrict__ x_in, float* __restrict__ x_out, int ld
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
         const int i = 8 * c + j;
-        u[j] = ((__ldg(y + i) - m[i]) - __ldg(shift + D + i)) * __ldg(scale + D + i);
+        u[j] = ((__ldg(y + i) - m[i]) - __ldg(w.shift + D + i)) * __ldg(w.scale + D + i);
       }
-      *reinterpret_cast<uint4*>(sX + tc::kmajor_off(tid, D + 8 * c, DIN)) = pack8(u);
+      *reinterpret_cast<uint4*>(sT + tc::kmajor_off(r, D + 8 * c, DIN)) = pack8(u);
     }
-    // 2. the network
-    tc::fence_proxy_async();
-    __syncthreads();
-    if (tid == 0) issue_layer<DIN, H>(taddr, sX, sW, &mbar);
+    // 2. the network; the activations of each layer overwrite its input tile
+    ok = weights_ready(&wbar, 0u, ok);
+    if (ok && tid == 0) issue_layer<TILES, DIN, H>(taddr, sA, sW, &mbar);
     ok = layer_done(&mbar, 0u, ok);
     if (ok) {
-      stage_weights<H, H>(sW, w2);
-      hidden_epilogue(trow, b1, sY, tid);
-      tc::fence_before_sync();
-      tc::fence_proxy_async();
-      __syncthreads();
-      if (tid == 0) issue_layer<H, H>(taddr, sY, sW, &mbar);
+      if (tid == 0) {
+        tc::mbar_expect_tx(&wbar, W2B);
+        tc::bulk_g2s(sW, w.packed + w.pk_w2, W2B, &wbar);
+      }
+      hidden_epilogue(trow, w.b1, sT, r);
+      ok = weights_ready(&wbar, 1u, ok);
+      if (ok && tid == 0) issue_layer<TILES, H, H>(taddr, sA, sW, &mbar);
       ok = layer_done(&mbar, 1u, ok);
     }
     if (ok) {
-      stage_weights<DOUT, H>(sW, w3);
-      hidden_epilogue(trow, b2, sX, tid);
-      tc::fence_before_sync();
-      tc::fence_proxy_async();
-      __syncthreads();
-      if (tid == 0) issue_layer<H, DOUT>(taddr, sX, sW, &mbar);
+      if (tid == 0) {
+        tc::mbar_expect_tx(&wbar, W3B);
+        tc::bulk_g2s(sW, w.packed + w.pk_w3, W3B, &wbar);
+      }
+      hidden_epilogue(trow, w.b2, sT, r);
+      ok = weights_ready(&wbar, 0u, ok);
+      if (ok && tid == 0) issue_layer<TILES, H, DOUT>(taddr, sA, sW, &mbar);
       ok = layer_done(&mbar, 0u, ok);
     }
-    // 3. the draw and the weight
+    // 3. the draw and the weight, eight components at a time
     if (ok) {
-      float o[DOUT];
+      const float se = (float)prm.sigma_eta, ise = 1.0f / se, lse = logf(se);
+      const float sy = (float)prm.sigma_y, isy = (float)prm.inv_sigma_y;
+      const float c2 = (float)prm.c_half_log_2pi, ls = (float)prm.log_sigma_y;
+      double l = live ? (resampled ? st->ll : lw[p]) : 0.0;
+      double corr = 0.0;  // log p(x' | x) - log q(x' | x, y), the 2 pi terms cancel
 #pragma unroll
-      for (int n0 = 0; n0 < DOUT; n0 += 16) {
-        float v[16];
-        tc::tmem_ld16(trow + (uint32_t)n0, v);
+      for (int c = 0; c < D / 8; ++c) {
+        float dl[8], sr[8];
+        tc::tmem_ld8(trow + (uint32_t)(8 * c), dl);
+        tc::tmem_ld8(trow + (uint32_t)(D + 8 * c), sr);
+        if (live) {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) o[n0 + j] = v[j] + __ldg(b3 + n0 + j);
-      }
-      if (live) {
-        const float se = (float)prm.sigma_eta, ise = 1.0f / se, lse = logf(se);
-        const float sy = (float)prm.sigma_y, isy = (float)prm.inv_sigma_y;
-        const float c2 = (float)prm.c_half_log_2pi, ls = (float)prm.log_sigma_y;
-        double l = resampled ? st->ll : lw[p];
-        double corr = 0.0;  // log p(x' | x) - log q(x' | x, y), the 2 pi terms cancel
+          for (int h = 0; h < 2; ++h) {
+            bpf_u32x4 rr = bpf_draw(seed, (uint32_t)p, (uint32_t)step, (uint32_t)(2 * c + h), BPF_RNG_NOISE);
+            float z[4];
+            bpf_normal_pair_f(rr.v[0], rr.v[1], &z[0], &z[1]);
+            bpf_normal_pair_f(rr.v[2], rr.v[3], &z[2], &z[3]);
 #pragma unroll
-        for (int b = 0; b < (D + 3) / 4; ++b) {
-          bpf_u32x4 r = bpf_draw(seed, (uint32_t)p, (uint32_t)step, (uint32_t)b, BPF_RNG_NOISE);
-          float z[4];
-          bpf_normal_pair_f(r.v[0], r.v[1], &z[0], &z[1]);
-          bpf_normal_pair_f(r.v[2], r.v[3], &z[2], &z[3]);
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            const int i = 4 * b + j;
-            if (i < D) {
-              const float delta = o[i];
-              const float s = fminf(fmaxf(o[D + i], kSMin), kSMax);
+            for (int j = 0; j < 4; ++j) {
+              const int q = 4 * h + j, i = 8 * c + q;
+              const float delta = dl[q] + __ldg(w.b3 + i);
+              const float s = fminf(fmaxf(sr[q] + __ldg(w.b3 + D + i), kSMin), kSMax);
               const float dx = delta + expf(s) * z[j];  // x' - m
               const float xi = m[i] + dx;
               x_out[(size_t)i * ld + p] = xi;
@@ -219,6 +236,8 @@ k_guided_fused(const float* __restrict__ x_in, float* __restrict__ x_out, int ld
             }
           }
         }
+      }
+      if (live) {
         l += corr;
         lw[p] = l;
         lw_push(part, l);
@@ -227,34 +246,46 @@ k_guided_fused(const float* __restrict__ x_in, float* __restrict__ x_out, int ld
   }
   tc::fence_before_sync();
   __syncthreads();
-  if (warp == 0) tc::tmem_dealloc(taddr, H);
+  if (warp == 0) tc::tmem_dealloc(taddr, 128 * TILES);
   if (ok_in && !ok && tid == 0) atomicExch(err, 1);
   transition_reduce_tail(part, partials, blockIdx.x, 0, gridDim.x, counter, n, st, ok_in && ok, resampled, true);
+}
+
+template <int TILES>
+int launch_fused(ProposalNet& net, const GuidedArgs& a, const L96Params& prm, cudaStream_t st) {
+  const int per = kGTile * TILES;
+  const int blocks = (a.n + per - 1) / per;
+  if (blocks > a.max_partials) return BPF_E_INVALID;
+  static bool configured = false;
+  if (!configured) {
+    BPF_TRY(cudaFuncSetAttribute(k_guided_fused<40, TILES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 guided_smem<TILES>()));
+    configured = true;
+  }
+  GuidedWeights w{net.packed, net.pk_w1, net.pk_w2, net.pk_w3, net.b1(), net.b2(), net.b3(), net.shift, net.scale};
+  k_guided_fused<40, TILES><<<blocks, per, guided_smem<TILES>(), st>>>(
+      (const float*)a.x_in, (float*)a.x_out, a.ld, a.n, a.as, a.lw, (const float*)a.y, a.t1, a.t2, a.seed, a.step,
+      prm, a.stats, a.partials, a.counter, w, net.err);
+  BPF_TRY(cudaGetLastError());
+  return BPF_OK;
 }
 
 }  // namespace
 
 int launch_guided(ProposalNet& net, const GuidedArgs& a, cudaStream_t st) {
   if (a.n <= 0 || !a.y) return BPF_E_INVALID;  // the proposal needs the observation
-  if (net.dim != 40 || net.hidden != kProposalHidden || net.din != 80 || net.dout != 80) return BPF_E_INVALID;
-  // the dense weights are read with 16-byte loads
-  const uintptr_t al = reinterpret_cast<uintptr_t>(net.w1h()) | reinterpret_cast<uintptr_t>(net.w2h()) |
-                       reinterpret_cast<uintptr_t>(net.w3h());
-  if (al & 15) return BPF_E_INVALID;
-  const int blocks = (a.n + kGTile - 1) / kGTile;
-  if (blocks > a.max_partials) return BPF_E_INVALID;
-  static bool configured = false;
-  if (!configured) {
-    BPF_TRY(cudaFuncSetAttribute(k_guided_fused<40>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGSmem));
-    configured = true;
-  }
+  if (net.dim != 40 || net.hidden != kProposalHidden || net.din != 80 || net.dout != 80 || !net.packed)
+    return BPF_E_INVALID;
+  // the weight images are copied in bulk: 16-byte aligned starts and sizes
+  if (((reinterpret_cast<uintptr_t>(net.packed) | (uintptr_t)net.pk_w1 | (uintptr_t)net.pk_w2 |
+        (uintptr_t)net.pk_w3) & 15) != 0)
+    return BPF_E_INVALID;
   const L96Params prm = l96_params<float>(a.theta, a.h);
-  k_guided_fused<40><<<blocks, kGTile, kGSmem, st>>>(
-      (const float*)a.x_in, (float*)a.x_out, a.ld, a.n, a.as, a.lw, (const float*)a.y, a.t1, a.t2, a.seed, a.step,
-      prm, a.stats, a.partials, a.counter, net.w1h(), net.w2h(), net.w3h(), net.b1(), net.b2(), net.b3(), net.shift,
-      net.scale, net.err);
-  BPF_TRY(cudaGetLastError());
-  return BPF_OK;
+  // two tiles per CTA once single-tile CTAs would need more than one wave
+  // at three CTAs per SM
+  const int tiles = (a.n + kGTile - 1) / kGTile;
+  if (tiles > 3 * 148) return launch_fused<2>(net, a, prm, st);
+  return launch_fused<1>(net, a, prm, st);
 }
 
 }  // namespace bpf

@@ -23,6 +23,7 @@
 #include "internal.cuh"
 #include "model_body.cuh"
 #include "mlp.cuh"
+#include "tc.cuh"
 #include "proposal.cuh"
 
 #include <cmath>
@@ -149,6 +150,30 @@ __global__ void k_adam(float* __restrict__ P, const float* __restrict__ G, float
   Ph[i] = __float2bfloat16(p);
 }
 
+// the three weight matrices into their shared-memory images
+__global__ void k_pack_weights(const __nv_bfloat16* __restrict__ Ph, int o_w1, int o_w2, int o_w3, int hidden,
+                               int din, int dout, unsigned char* __restrict__ out, int pk_w1, int pk_w2, int pk_w3) {
+  const int n1 = hidden * din, n2 = hidden * hidden, n3 = dout * hidden;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n1) {
+    *reinterpret_cast<__nv_bfloat16*>(out + pk_w1 + tc::kmajor_off(i / din, i % din, din)) = Ph[o_w1 + i];
+  } else if (i < n1 + n2) {
+    const int j = i - n1;
+    *reinterpret_cast<__nv_bfloat16*>(out + pk_w2 + tc::kmajor_off(j / hidden, j % hidden, hidden)) = Ph[o_w2 + j];
+  } else if (i < n1 + n2 + n3) {
+    const int j = i - n1 - n2;
+    *reinterpret_cast<__nv_bfloat16*>(out + pk_w3 + tc::kmajor_off(j / hidden, j % hidden, hidden)) = Ph[o_w3 + j];
+  }
+}
+
+int pack_weights(ProposalNet& p, cudaStream_t st) {
+  const int total = p.hidden * p.din + p.hidden * p.hidden + p.dout * p.hidden;
+  k_pack_weights<<<(total + 255) / 256, 256, 0, st>>>(p.params_h, p.o_w1, p.o_w2, p.o_w3, p.hidden, p.din, p.dout,
+                                                      p.packed, p.pk_w1, p.pk_w2, p.pk_w3);
+  BPF_TRY(cudaGetLastError());
+  return BPF_OK;
+}
+
 __global__ void k_to_bf16(const float* __restrict__ P, __nv_bfloat16* Ph, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) Ph[i] = __float2bfloat16(P[i]);
@@ -225,10 +250,15 @@ int ProposalNet::alloc(int d, int hid, int cap_batch) {
   o_w3 = o_b2 + hidden;
   o_b3 = o_w3 + dout * hidden;
   nparams = o_b3 + dout;
+  pk_w1 = 0;
+  pk_w2 = pk_w1 + hidden * din * 2;
+  pk_w3 = pk_w2 + hidden * hidden * 2;
+  pk_bytes = pk_w3 + dout * hidden * 2;
   cap = cap_batch;
   auto A = [](void** p, size_t b) { return cudaMalloc(p, b) == cudaSuccess ? BPF_OK : BPF_E_NOMEM; };
   int rc = A((void**)&params, (size_t)nparams * 4);
   if (!rc) rc = A((void**)&params_h, (size_t)nparams * 2);
+  if (!rc) rc = A((void**)&packed, (size_t)pk_bytes);
   if (!rc) rc = A((void**)&grads, (size_t)nparams * 4);
   if (!rc) rc = A((void**)&m1, (size_t)nparams * 4);
   if (!rc) rc = A((void**)&m2, (size_t)nparams * 4);
@@ -251,7 +281,7 @@ int ProposalNet::alloc(int d, int hid, int cap_batch) {
 }
 
 void ProposalNet::release() {
-  void* ps[] = {params, params_h, grads, m1, m2, shift, scale, err, loss, U, H1, H2, O, dO, dH, dZ, r0, mt,
+  void* ps[] = {params, params_h, packed, grads, m1, m2, shift, scale, err, loss, U, H1, H2, O, dO, dH, dZ, r0, mt,
                  colpart, loss_part};
   for (void* q : ps)
     if (q) cudaFree(q);
@@ -299,6 +329,8 @@ int upload_params(bpf_proposal* q, const float* P) {
   BPF_TRY(cudaMemcpyAsync(p.params, P, (size_t)p.nparams * 4, cudaMemcpyHostToDevice, q->stream));
   bpf::k_to_bf16<<<(p.nparams + 255) / 256, 256, 0, q->stream>>>(p.params, p.params_h, p.nparams);
   BPF_TRY(cudaGetLastError());
+  int rc = bpf::pack_weights(p, q->stream);
+  if (rc) return rc;
   BPF_TRY(cudaStreamSynchronize(q->stream));
   return BPF_OK;
 }
@@ -420,6 +452,8 @@ int bpf_proposal_train(bpf_proposal* q, int steps, int batch, double lr, float* 
       loss_trace[s] = (float)l;
     }
   }
+  int rc = bpf::pack_weights(p, q->stream);
+  if (rc) return rc;
   return check_err(q);
 }
 

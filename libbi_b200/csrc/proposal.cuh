@@ -27,6 +27,12 @@ struct ProposalNet {
   __nv_bfloat16 *U = nullptr, *H1 = nullptr, *H2 = nullptr, *dO = nullptr, *dZ = nullptr;
   float *O = nullptr, *dH = nullptr, *r0 = nullptr;
   float* mt = nullptr;  // RK4 means of the training inputs
+  // the BF16 weight matrices as shared-memory images in the canonical
+  // K-major layout (tc.cuh): W1 at byte pk_w1, W2 at pk_w2, W3 at pk_w3;
+  // rebuilt by pack_weights whenever params_h changes outside training and
+  // at the end of every training call
+  unsigned char* packed = nullptr;
+  int pk_w1 = 0, pk_w2 = 0, pk_w3 = 0, pk_bytes = 0;
   float* colpart = nullptr;  // per-chunk column sums of the bias gradients
   double* loss_part = nullptr;  // per-block loss sums
 
@@ -40,6 +46,9 @@ struct ProposalNet {
   int alloc(int d, int hid, int cap_batch);
   void release();
 };
+
+// rebuild ProposalNet::packed from params_h
+int pack_weights(ProposalNet& p, cudaStream_t st);
 
 // O [B x dout] = MLP(U [B x din]); H1, H2 [B x hidden] hold the activations
 int proposal_forward(ProposalNet& p, const __nv_bfloat16* U, int B, __nv_bfloat16* H1, __nv_bfloat16* H2, float* O,
