@@ -201,20 +201,26 @@ k_guided_fused(const float* __restrict__ x_in, float* __restrict__ x_out, int ld
       if (ok && tid == 0) issue_layer<TILES, H, DOUT>(taddr, sA, sW, &mbar);
       ok = layer_done(&mbar, 0u, ok);
     }
-    // 3. the draw and the weight, eight components at a time
+    // 3. the draw and the weight, eight components at a time.  The tile's
+    //    activations are dead once layer 3 is done: m moves there (row r,
+    //    FP32), so that the loop over components stays rolled (one copy of
+    //    the draw in the instruction stream)
     if (ok) {
+      float* mrow = reinterpret_cast<float*>(sT) + r * (D + 1);  // odd row stride: conflict-free
+#pragma unroll
+      for (int i = 0; i < D; ++i) mrow[i] = m[i];
       const float se = (float)prm.sigma_eta, ise = 1.0f / se, lse = logf(se);
       const float sy = (float)prm.sigma_y, isy = (float)prm.inv_sigma_y;
       const float c2 = (float)prm.c_half_log_2pi, ls = (float)prm.log_sigma_y;
       double l = live ? (resampled ? st->ll : lw[p]) : 0.0;
       double corr = 0.0;  // log p(x' | x) - log q(x' | x, y), the 2 pi terms cancel
-#pragma unroll
+#pragma unroll 1
       for (int c = 0; c < D / 8; ++c) {
         float dl[8], sr[8];
         tc::tmem_ld8(trow + (uint32_t)(8 * c), dl);
         tc::tmem_ld8(trow + (uint32_t)(D + 8 * c), sr);
         if (live) {
-#pragma unroll
+#pragma unroll 1
           for (int h = 0; h < 2; ++h) {
             bpf_u32x4 rr = bpf_draw(seed, (uint32_t)p, (uint32_t)step, (uint32_t)(2 * c + h), BPF_RNG_NOISE);
             float z[4];
@@ -223,10 +229,10 @@ k_guided_fused(const float* __restrict__ x_in, float* __restrict__ x_out, int ld
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
               const int q = 4 * h + j, i = 8 * c + q;
-              const float delta = dl[q] + __ldg(w.b3 + i);
-              const float s = fminf(fmaxf(sr[q] + __ldg(w.b3 + D + i), kSMin), kSMax);
+              const float delta = (h ? dl[4 + j] : dl[j]) + __ldg(w.b3 + i);
+              const float s = fminf(fmaxf((h ? sr[4 + j] : sr[j]) + __ldg(w.b3 + D + i), kSMin), kSMax);
               const float dx = delta + expf(s) * z[j];  // x' - m
-              const float xi = m[i] + dx;
+              const float xi = mrow[i] + dx;
               x_out[(size_t)i * ld + p] = xi;
               const float e = dx * ise;
               corr += (double)(-0.5f * e * e - lse) - (double)(-0.5f * z[j] * z[j] - s);

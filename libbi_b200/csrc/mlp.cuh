@@ -20,9 +20,17 @@ struct DenseArgs {
   __nv_bfloat16* Dh;     // BF16 copy, or null
   long long dh_rs;
   int* err;              // set when a bounded wait gives up
+  // split-K workspace (FP32), or null: a layer with few 128-row tiles and a
+  // long K is split over CTAs whose partial products land here and are
+  // added in a fixed order by a second kernel
+  float* ws = nullptr;
+  long long ws_floats = 0;
   // set by launch_dense: the operand is K-contiguous with 16-byte aligned
   // rows, so a chunk is staged with one 16-byte load per 8 elements
-  int a_vec = 0, b_vec = 0;
+  // (*_vec), or row-contiguous, so consecutive threads take consecutive
+  // rows (*_rfast); the K split and chunks per split
+  int a_vec = 0, b_vec = 0, a_rfast = 0, b_rfast = 0;
+  int ksplit = 1, kchunks = 0;
 };
 
 int launch_dense(const DenseArgs& g, cudaStream_t st);

@@ -196,12 +196,19 @@ static DenseArgs dense(const __nv_bfloat16* A, long long a_rs, long long a_cs, c
   return g;
 }
 
+// a training layer, with the split-K workspace
+static int run_dense(ProposalNet& p, DenseArgs g, cudaStream_t st) {
+  g.ws = p.ws;
+  g.ws_floats = p.ws_floats;
+  return launch_dense(g, st);
+}
+
 int proposal_forward(ProposalNet& p, const __nv_bfloat16* U, int B, __nv_bfloat16* H1, __nv_bfloat16* H2, float* O,
                      cudaStream_t st) {
   const int din = p.din, H = p.hidden, dout = p.dout;
-  int rc = launch_dense(dense(U, din, 1, p.w1h(), din, 1, B, H, din, p.b1(), 1, nullptr, H1, p.err), st);
-  if (!rc) rc = launch_dense(dense(H1, H, 1, p.w2h(), H, 1, B, H, H, p.b2(), 1, nullptr, H2, p.err), st);
-  if (!rc) rc = launch_dense(dense(H2, H, 1, p.w3h(), H, 1, B, dout, H, p.b3(), 0, O, nullptr, p.err), st);
+  int rc = run_dense(p, dense(U, din, 1, p.w1h(), din, 1, B, H, din, p.b1(), 1, nullptr, H1, p.err), st);
+  if (!rc) rc = run_dense(p, dense(H1, H, 1, p.w2h(), H, 1, B, H, H, p.b2(), 1, nullptr, H2, p.err), st);
+  if (!rc) rc = run_dense(p, dense(H2, H, 1, p.w3h(), H, 1, B, dout, H, p.b3(), 0, O, nullptr, p.err), st);
   return rc;
 }
 
@@ -217,21 +224,21 @@ static int loss_and_grad(ProposalNet& p, int B, cudaStream_t st) {
   float *gW1 = g + p.o_w1, *gb1 = g + p.o_b1, *gW2 = g + p.o_w2, *gb2 = g + p.o_b2, *gW3 = g + p.o_w3,
         *gb3 = g + p.o_b3;
   // layer 3: O = H2 W3^T + b3
-  rc = launch_dense(dense(p.dO, 1, dout, p.H2, 1, H, dout, H, B, nullptr, 0, gW3, nullptr, p.err), st);
+  rc = run_dense(p, dense(p.dO, 1, dout, p.H2, 1, H, dout, H, B, nullptr, 0, gW3, nullptr, p.err), st);
   if (rc) return rc;
   colsum(p.dO, B, dout, p.colpart, gb3, st);
-  rc = launch_dense(dense(p.dO, dout, 1, p.w3h(), 1, H, B, H, dout, nullptr, 0, p.dH, nullptr, p.err), st);
+  rc = run_dense(p, dense(p.dO, dout, 1, p.w3h(), 1, H, B, H, dout, nullptr, 0, p.dH, nullptr, p.err), st);
   if (rc) return rc;
   k_relu_back<<<(unsigned)(((size_t)B * H + 255) / 256), 256, 0, st>>>(p.dH, p.H2, p.dZ, (size_t)B * H);
   // layer 2: H2 = relu(H1 W2^T + b2)
-  rc = launch_dense(dense(p.dZ, 1, H, p.H1, 1, H, H, H, B, nullptr, 0, gW2, nullptr, p.err), st);
+  rc = run_dense(p, dense(p.dZ, 1, H, p.H1, 1, H, H, H, B, nullptr, 0, gW2, nullptr, p.err), st);
   if (rc) return rc;
   colsum(p.dZ, B, H, p.colpart, gb2, st);
-  rc = launch_dense(dense(p.dZ, H, 1, p.w2h(), 1, H, B, H, H, nullptr, 0, p.dH, nullptr, p.err), st);
+  rc = run_dense(p, dense(p.dZ, H, 1, p.w2h(), 1, H, B, H, H, nullptr, 0, p.dH, nullptr, p.err), st);
   if (rc) return rc;
   k_relu_back<<<(unsigned)(((size_t)B * H + 255) / 256), 256, 0, st>>>(p.dH, p.H1, p.dZ, (size_t)B * H);
   // layer 1: H1 = relu(U W1^T + b1)
-  rc = launch_dense(dense(p.dZ, 1, H, p.U, 1, din, H, din, B, nullptr, 0, gW1, nullptr, p.err), st);
+  rc = run_dense(p, dense(p.dZ, 1, H, p.U, 1, din, H, din, B, nullptr, 0, gW1, nullptr, p.err), st);
   if (rc) return rc;
   colsum(p.dZ, B, H, p.colpart, gb1, st);
   BPF_TRY(cudaGetLastError());
@@ -276,13 +283,16 @@ int ProposalNet::alloc(int d, int hid, int cap_batch) {
   if (!rc) rc = A((void**)&r0, (size_t)cap * dim * 4);
   if (!rc) rc = A((void**)&colpart, (size_t)((cap + kColChunk - 1) / kColChunk) * (hidden > dout ? hidden : dout) * 4);
   if (!rc) rc = A((void**)&loss_part, (size_t)((cap + 255) / 256) * sizeof(double));
+  // room for one partial product per SM of the widest weight gradient
+  ws_floats = 148ll * hidden * (hidden > din ? (hidden > dout ? hidden : dout) : (din > dout ? din : dout));
+  if (!rc) rc = A((void**)&ws, (size_t)ws_floats * 4);
   if (rc) cudaGetLastError();
   return rc;
 }
 
 void ProposalNet::release() {
   void* ps[] = {params, params_h, packed, grads, m1, m2, shift, scale, err, loss, U, H1, H2, O, dO, dH, dZ, r0, mt,
-                 colpart, loss_part};
+                 colpart, loss_part, ws};
   for (void* q : ps)
     if (q) cudaFree(q);
 }

@@ -34,6 +34,8 @@ struct ProposalNet {
   unsigned char* packed = nullptr;
   int pk_w1 = 0, pk_w2 = 0, pk_w3 = 0, pk_bytes = 0;
   float* colpart = nullptr;  // per-chunk column sums of the bias gradients
+  float* ws = nullptr;       // split-K workspace of the weight-gradient layers
+  long long ws_floats = 0;
   double* loss_part = nullptr;  // per-block loss sums
 
   const __nv_bfloat16* w1h() const { return params_h + o_w1; }
