@@ -508,6 +508,8 @@ def main():
     ap.add_argument("--no-large-n", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-guided", action="store_true")
+    ap.add_argument("--guided-seeds", type=int, default=64,
+                    help="filter runs per N in the guided/bootstrap comparison (64; fewer for profiling)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -643,7 +645,7 @@ def main():
         line["batched"] = batched_filters()
         line["pmmh"] = pmmh_chains()
     if rank == 0 and not args.no_guided:
-        line["guided"] = guided_vs_bootstrap(y_host)
+        line["guided"] = guided_vs_bootstrap(y_host, seeds=max(2, args.guided_seeds))
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(y_host)
     pf.close()

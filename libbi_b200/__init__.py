@@ -10,7 +10,9 @@ from .filter import (BootstrapPF, ModelL96, ModelPZ, Resampler, SystematicResamp
                      MultinomialResampler, MetropolisResampler, gather_rows, StepResult, BatchedBootstrapPF)
 from .sampler import MarginalMH, Prior, smc2  # noqa: F401
 from .proposal import LearnedProposal  # noqa: F401
+from .schedule import Observer, Schedule, ScheduleElement  # noqa: F401
 from . import configs  # noqa: F401
 
 __all__ = ["BootstrapPF", "ModelL96", "ModelPZ", "Resampler", "SystematicResampler", "MultinomialResampler",
-           "MetropolisResampler", "BatchedBootstrapPF", "MarginalMH", "Prior", "smc2", "LearnedProposal", "gather_rows", "BpfError", "ParticleFilterDegeneratedException", "configs"]
+           "MetropolisResampler", "BatchedBootstrapPF", "MarginalMH", "Prior", "smc2", "LearnedProposal", "Observer", "Schedule",
+           "ScheduleElement", "gather_rows", "BpfError", "ParticleFilterDegeneratedException", "configs"]

@@ -253,7 +253,12 @@ k_guided_fused(const float* __restrict__ x_in, float* __restrict__ x_out, int ld
   tc::fence_before_sync();
   __syncthreads();
   if (warp == 0) tc::tmem_dealloc(taddr, 128 * TILES);
-  if (ok_in && !ok && tid == 0) atomicExch(err, 1);
+  // a wait that gave up: the proposal's flag and the step's status (the
+  // filter's next read of its statistics returns it)
+  if (ok_in && !ok && tid == 0) {
+    atomicExch(err, 1);
+    st->status = BPF_E_TIMEOUT;
+  }
   transition_reduce_tail(part, partials, blockIdx.x, 0, gridDim.x, counter, n, st, ok_in && ok, resampled, true);
 }
 
