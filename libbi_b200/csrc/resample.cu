@@ -22,7 +22,6 @@
 #include "resample_common.cuh"
 #include "reduce.cuh"
 
-#include <cooperative_groups.h>
 
 namespace bpf {
 
@@ -683,182 +682,6 @@ k_systematic_coop1(const double* __restrict__ lw, int n, StepStats* st, const do
 }
 
 // ---------------------------------------------------------------------------
-// systematic resampling in one thread-block cluster (n <= kClusterMaxN)
-//
-// Eight CTAs of 1024 threads each own a contiguous chunk of at most 8192
-// log-weights.  Everything between reading the log-weights and writing the
-// ancestors stays on chip: fixed-point weights and cumulative offspring in
-// registers, the extra-copy counts E and the childless slots in shared
-// memory; CTAs exchange their totals and search each other's E through
-// distributed shared memory, and synchronise with hardware cluster
-// barriers.  Global traffic is the log-weights in and the ancestors out.
-// ---------------------------------------------------------------------------
-namespace cg = cooperative_groups;
-constexpr int kClusterCtas = 8;
-constexpr int kClusterThreads = 1024;
-constexpr int kClusterItems = 8;
-constexpr int kClusterChunk = kClusterThreads * kClusterItems;
-constexpr int kClusterMaxN = kClusterCtas * kClusterChunk;
-
-struct ClusterShared {
-  u128 wtot;        // this CTA's weight total
-  int ztot;         // this CTA's childless count
-  int efirst;       // E at this CTA's first particle
-  int begin, len;   // this CTA's chunk
-};
-
-__global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kClusterThreads)
-k_systematic_cluster(const double* __restrict__ lw, int n, StepStats* st, const double* a_in, uint64_t seed,
-                     int step, int* Os_out, int* as, const int* gate) {
-  if (gate_closed(gate, st)) return;  // uniform over the cluster
-  cg::cluster_group cluster = cg::this_cluster();
-  const int c = (int)cluster.block_rank();
-  extern __shared__ int s_dyn[];
-  int* sE = s_dyn;                       // kClusterChunk
-  int* sslot = s_dyn + kClusterChunk;    // kClusterChunk
-  __shared__ ClusterShared sh;
-  __shared__ int s_last[kClusterThreads];
-  __shared__ u128 s_wtot[kClusterCtas];
-  __shared__ int s_misc[3 * kClusterCtas];
-
-  const int begin = (int)(((long long)c * n) / kClusterCtas);
-  const int end = (int)(((long long)(c + 1) * n) / kClusterCtas);
-  const int len = end - begin;
-  const int l0 = threadIdx.x * kClusterItems;  // local index of this thread's first item
-  const double mx = st->mx;
-  double a;
-  if (a_in) {
-    a = *a_in;
-  } else {
-    bpf_u32x4 r = bpf_draw(seed, 0u, (uint32_t)step, 0u, BPF_RNG_SYSTEMATIC);
-    a = bpf_u01d(r.v[0], r.v[1]);
-  }
-
-  // phase 1: fixed-point weights, kept in registers
-  unsigned long long q[kClusterItems];
-  u128 loc = u128_zero();
-#pragma unroll
-  for (int k = 0; k < kClusterItems; ++k) {
-    const int li = l0 + k;
-    q[k] = li < len ? weight_to_fixed(nanexp(__dsub_rn(__ldg(lw + begin + li), mx))) : 0ull;
-    u128 qq; qq.lo = q[k]; qq.hi = 0;
-    loc = u128_add(loc, qq);
-  }
-  u128 ctot;
-  const u128 texcl = block_exclusive_scan_u128_nt<kClusterThreads>(loc, &ctot);
-  if (threadIdx.x == 0) { sh.wtot = ctot; sh.begin = begin; sh.len = len; }
-  cluster.sync();
-
-  // phase 2: prefix of this CTA and the total W from the other CTAs' totals
-  if (threadIdx.x < kClusterCtas) {
-    ClusterShared* rs = cluster.map_shared_rank(&sh, threadIdx.x);
-    s_wtot[threadIdx.x] = rs->wtot;
-  }
-  __syncthreads();
-  u128 prefix = u128_zero(), total = u128_zero();
-#pragma unroll
-  for (int j = 0; j < kClusterCtas; ++j) {
-    total = u128_add(total, s_wtot[j]);
-    if (j < c) prefix = u128_add(prefix, s_wtot[j]);
-  }
-  const double W = u128_to_weight(total);
-  // SystematicResampler::cumulativeOffspring throws unless W > 0
-  // (share/src/bi/resampler/SystematicResampler.hpp:118-129)
-  if (!(W > 0.0)) {
-    if (c == 0 && threadIdx.x == 0) st->status = BPF_E_DEGENERATE;
-    cluster.sync();  // no CTA leaves while another may still read its shared memory
-    return;
-  }
-  const double nd = (double)n;
-  const double yW = __ddiv_rn(1.0, W);
-  int os[kClusterItems];
-  {
-    u128 Q = u128_add(prefix, texcl);
-#pragma unroll
-    for (int k = 0; k < kClusterItems; ++k) {
-      u128 qq; qq.lo = q[k]; qq.hi = 0;
-      Q = u128_add(Q, qq);
-      os[k] = systematic_Os(u128_to_weight(Q), W, yW, nd, a, n);
-    }
-  }
-  s_last[threadIdx.x] = os[kClusterItems - 1];
-  __syncthreads();
-  const int before0 = threadIdx.x > 0 ? s_last[threadIdx.x - 1]
-                                      : (begin == 0 ? 0 : systematic_Os(u128_to_weight(prefix), W, yW, nd, a, n));
-  int zl = 0;
-  {
-    int prev = before0;
-#pragma unroll
-    for (int k = 0; k < kClusterItems; ++k) {
-      const int li = l0 + k;
-      if (li < len) {
-        zl += (os[k] == prev);
-        if (Os_out) Os_out[begin + li] = os[k];
-      }
-      prev = os[k];
-    }
-  }
-  int czt;
-  const int zexcl = block_exclusive_scan_int_nt<kClusterThreads>(zl, &czt);
-  if (threadIdx.x == 0) sh.ztot = czt;
-  cluster.sync();
-
-  // phase 3: ranks of childless slots, E, survivors in place
-  if (threadIdx.x < kClusterCtas) {
-    ClusterShared* rs = cluster.map_shared_rank(&sh, threadIdx.x);
-    s_misc[threadIdx.x] = rs->ztot;
-  }
-  __syncthreads();
-  int zprefix = 0;
-#pragma unroll
-  for (int j = 0; j < kClusterCtas; ++j) if (j < c) zprefix += s_misc[j];
-  {
-    int Z = zprefix + zexcl;
-    int prev = before0;
-#pragma unroll
-    for (int k = 0; k < kClusterItems; ++k) {
-      const int li = l0 + k;
-      if (li < len) {
-        const int i = begin + li;
-        const bool zero = os[k] == prev;
-        const int e = prev - i + Z;
-        sE[li] = e;
-        if (li == 0) sh.efirst = e;
-        if (zero) sslot[Z - zprefix] = i;
-        else as[i] = i;
-        Z += zero;
-      }
-      prev = os[k];
-    }
-  }
-  cluster.sync();
-
-  // phase 4: childless slot of rank r <- ancestor a with E_a <= r < E_{a+1},
-  // found by CTA (first E of each chunk) and then within that CTA's E
-  if (threadIdx.x < kClusterCtas) {
-    ClusterShared* rs = cluster.map_shared_rank(&sh, threadIdx.x);
-    s_misc[kClusterCtas + threadIdx.x] = rs->len > 0 ? rs->efirst : 0x7fffffff;
-    s_misc[2 * kClusterCtas + threadIdx.x] = rs->begin;
-  }
-  __syncthreads();
-  for (int j = threadIdx.x; j < czt; j += kClusterThreads) {
-    const int r = zprefix + j;
-    int cc = 0;  // last CTA whose chunk starts with E <= r (CTA 0 starts with E = 0)
-#pragma unroll
-    for (int k = 1; k < kClusterCtas; ++k) if (s_misc[kClusterCtas + k] <= r) cc = k;
-    const int* rE = cluster.map_shared_rank(sE, cc);
-    const ClusterShared* rs = cluster.map_shared_rank(&sh, cc);
-    int lo = 0, hi = rs->len;
-    while (lo < hi) {
-      int mid = (lo + hi) >> 1;
-      if (rE[mid] <= r) lo = mid + 1; else hi = mid;
-    }
-    as[sslot[j]] = s_misc[2 * kClusterCtas + cc] + lo - 1;
-  }
-  cluster.sync();  // keep this CTA's shared memory alive until every search is done
-}
-
-// ---------------------------------------------------------------------------
 // cumulative offspring from offspring counts o[] (Metropolis) or from sorted
 // ancestors (multinomial), with childless counts per tile
 // ---------------------------------------------------------------------------
@@ -1195,7 +1018,6 @@ constexpr int kMaxCoarseCoop = 8192;
 constexpr int kCoopItems = 2;
 
 static int launch_systematic_coop(const ResampleArgs& a, ResampleScratch& s, int* Os, cudaStream_t st);
-static int launch_systematic_cluster(const ResampleArgs& a, ResampleScratch& s, int* Os, cudaStream_t st);
 
 static inline int grid_stride_blocks(int n) {
   int b = (n + kBlock - 1) / kBlock;
@@ -1339,26 +1161,6 @@ static int launch_systematic_coop(const ResampleArgs& a, ResampleScratch& s, int
     BPF_TRY(cudaLaunchCooperativeKernel((const void*)k_systematic_coop<kCoopItems>, dim3(G), dim3(kBlock), args, 0,
                                         st));
   }
-  return BPF_OK;
-}
-
-// One cluster of kClusterCtas CTAs; returns BPF_E_INVALID when the device
-// cannot launch clusters, so the caller can use another path.
-static int launch_systematic_cluster(const ResampleArgs& a, ResampleScratch& s, int* Os, cudaStream_t st) {
-  static int checked = 0, ok = 0;
-  const size_t smem = 2 * (size_t)kClusterChunk * sizeof(int);
-  if (!checked) {
-    int dev = 0, cl = 0;
-    BPF_TRY(cudaGetDevice(&dev));
-    BPF_TRY(cudaDeviceGetAttribute(&cl, cudaDevAttrClusterLaunch, dev));
-    ok = cl && cudaFuncSetAttribute(k_systematic_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem) == cudaSuccess;
-    checked = 1;
-  }
-  if (!ok) return BPF_E_INVALID;
-  k_systematic_cluster<<<kClusterCtas, kClusterThreads, smem, st>>>(a.lw, a.n, s.stats, a.uniforms, a.seed, a.step,
-                                                                    Os, a.as, a.gate);
-  BPF_TRY(cudaGetLastError());
   return BPF_OK;
 }
 
