@@ -298,33 +298,52 @@ k_systematic_offspring(const double* __restrict__ lw, int n, StepStats* st,
 // ---------------------------------------------------------------------------
 constexpr long long kBarrierTimeoutCycles = 4000000000ll;  // ~2 s at 2 GHz
 
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// acquire + release: the last block to arrive acquires every earlier
+// arrival's release (their adds form one release sequence on the counter)
+// before it publishes the generation
+__device__ __forceinline__ unsigned atom_add_acq_rel_gpu(unsigned* p, unsigned v) {
+  unsigned old;
+  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+
+__device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 // Bounded grid barrier.  counter returns to zero after every barrier; gen
-// counts completed barriers.  Returns false (in every thread) on timeout.
+// counts completed barriers.  Thread 0 of each block arrives with an
+// acquire-release add (the block's writes, ordered before it by the block
+// barrier, are released with it); the last to arrive has then acquired all
+// of them, resets the counter and publishes the next generation with a
+// release store; the others poll the generation with acquire loads.
+// Returns false (in every thread) on timeout.
 __device__ __forceinline__ bool grid_barrier(unsigned* counter, unsigned* gen, StepStats* st) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned* vgen = gen;
-    const unsigned g = *vgen;
-    __threadfence();
-    const unsigned arrived = atomicAdd(counter, 1u);
+    const unsigned g = ld_acquire_gpu(gen);
+    const unsigned arrived = atom_add_acq_rel_gpu(counter, 1u);
     int ok = 1;
     if (arrived == gridDim.x - 1) {
-      *counter = 0;
-      __threadfence();
-      atomicAdd(gen, 1u);
+      *counter = 0;  // ordered before the release below; nobody arrives again before it
+      st_release_gpu(gen, g + 1u);
     } else {
       const long long t0 = clock64();
-      while (*vgen == g) {
+      while (ld_acquire_gpu(gen) == g) {
         if (clock64() - t0 > kBarrierTimeoutCycles) {
           ok = 0;
           st->status = BPF_E_TIMEOUT;
           break;
         }
-        __nanosleep(64);
       }
     }
-    __threadfence();
     s_ok = ok;
   }
   __syncthreads();
@@ -661,11 +680,23 @@ k_systematic_coop1(const double* __restrict__ lw, int n, StepStats* st, const do
   }
   if (!grid_barrier(bar_counter, bar_gen, st)) return;
 
-  // phase 4: childless slot of rank r <- ancestor a with E_a <= r < E_{a+1}
+  // phase 4: childless slot of rank r <- ancestor a with E_a <= r < E_{a+1}.
+  // The coarse index (every 2^coarse_shift-th E) comes into shared memory
+  // with 16-byte loads, all in flight at once; a 16-wide window of E is
+  // read as four 16-byte loads and counted in registers instead of four
+  // dependent probes
   const int nc = ((n - 1) >> coarse_shift) + 1;
-  for (int i = threadIdx.x; i < nc; i += blockDim.x) s_coarse[i] = __ldcg(ecoarse + i);
+  {
+    const int nc4 = nc >> 2;
+    const int4* src = reinterpret_cast<const int4*>(ecoarse);
+    int4* dst = reinterpret_cast<int4*>(s_coarse);
+#pragma unroll 4
+    for (int i = threadIdx.x; i < nc4; i += blockDim.x) dst[i] = __ldcg(src + i);
+    for (int i = 4 * nc4 + threadIdx.x; i < nc; i += blockDim.x) s_coarse[i] = __ldcg(ecoarse + i);
+  }
   __syncthreads();
   for (int r = b * blockDim.x + threadIdx.x; r < R; r += G * blockDim.x) {
+    const int sl = __ldcg(slot + r);
     int clo = 0, chi = nc;
     while (clo < chi) {
       int mid = (clo + chi) >> 1;
@@ -673,11 +704,23 @@ k_systematic_coop1(const double* __restrict__ lw, int n, StepStats* st, const do
     }
     int lo = (clo - 1) << coarse_shift;
     int hi = min(n, lo + (1 << coarse_shift));
-    while (lo < hi) {
-      int mid = (lo + hi) >> 1;
-      if (__ldcg(E + mid) <= r) lo = mid + 1; else hi = mid;
+    if (coarse_shift == 4 && hi - lo == 16) {
+      // lo is a multiple of 16: the window is 64-byte aligned
+      const int4* w = reinterpret_cast<const int4*>(E + lo);
+      int cnt = 0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int4 e = __ldcg(w + j);
+        cnt += (e.x <= r) + (e.y <= r) + (e.z <= r) + (e.w <= r);
+      }
+      lo += cnt;  // E is nondecreasing: the first index with E > r
+    } else {
+      while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (__ldcg(E + mid) <= r) lo = mid + 1; else hi = mid;
+      }
     }
-    as[__ldcg(slot + r)] = lo - 1;
+    as[sl] = lo - 1;
   }
 }
 
