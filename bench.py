@@ -357,6 +357,92 @@ def pmmh_chains(iterations=20, nchains=128, nparticles=2048, T=100):
     }
 
 
+def precision_check(y_host, seeds=16, n=N_PARTICLES, T=T_OBS):
+    """The FP32 filter against the FP64 filter on the same seeds (identical
+    Philox draws, so the two differ by rounding only), on the bench's
+    Lorenz-96 workload: per step the relative error of the log-likelihood
+    increment (relative to max(|inc64|, 1)) and of the cumulative
+    log-likelihood, the fraction of steps within 1e-4, the first step
+    beyond it, and whether the two estimators' means over the seeds agree
+    within two standard errors.  Lorenz-96 is chaotic, so rounding
+    differences grow along a run; the per-step columns show where."""
+    import numpy as np
+    from dataclasses import replace
+    from libbi_b200 import BootstrapPF, configs
+
+    m32 = configs.L96_D40_N65536["model"]
+    m64 = replace(m32, precision="f64")
+    y32 = np.asarray(y_host[:T], np.float32)
+    y64 = y32.astype(np.float64)  # the same observed values in both precisions
+    inc_e, cum_e, ll32, ll64 = [], [], [], []
+    for s in range(seeds):
+        out = []
+        for m, y in ((m32, y32), (m64, y64)):
+            pf = BootstrapPF(m, n, resampler="systematic", ess_rel=ESS_REL, seed=20_000 + s)
+            out.append(pf.filter(y, 0.0, DT))
+            pf.close()
+        (l32, i32, _), (l64, i64, _) = out
+        inc_e.append(np.abs(i32 - i64) / np.maximum(np.abs(i64), 1.0))
+        c32, c64 = np.cumsum(i32), np.cumsum(i64)
+        cum_e.append(np.abs(c32 - c64) / np.maximum(np.abs(c64), 1.0))
+        ll32.append(l32)
+        ll64.append(l64)
+    inc_e, cum_e = np.array(inc_e), np.array(cum_e)
+    ll32, ll64 = np.array(ll32), np.array(ll64)
+    one = one_step_precision(m32, m64, y32, y64, n)
+    se = float(np.sqrt(ll32.var(ddof=1) / seeds + ll64.var(ddof=1) / seeds))
+    within = cum_e.max(axis=0) <= 1e-4
+    first_bad = int(np.argmin(within)) + 1 if not within.all() else None
+    return {
+        "workload": f"l96_d40_n{n}_t{T}_fp32_vs_fp64_{seeds}seeds",
+        "increment_rel_err": {"median": float(np.median(inc_e)), "max": float(inc_e.max()),
+                              "max_first_20_steps": float(inc_e[:, :20].max())},
+        "loglik_rel_err": {"median": float(np.median(cum_e)), "max": float(cum_e.max()),
+                           "final_median": float(np.median(cum_e[:, -1]))},
+        "steps_within_1e-4": float(within.mean()),
+        "first_step_beyond_1e-4": first_bad,
+        "mean_ll_fp32": float(ll32.mean()), "mean_ll_fp64": float(ll64.mean()),
+        "mean_diff_in_standard_errors": float(abs(ll32.mean() - ll64.mean()) / se) if se > 0 else 0.0,
+        "means_within_2_se": bool(abs(ll32.mean() - ll64.mean()) <= 2 * se),
+        "one_step_same_input": one,
+    }
+
+
+def one_step_precision(m32, m64, y32, y64, n, seeds=4, at=(0, 1, 10, 50, 100, 150, 199)):
+    """Arithmetic error of one step: at sampled steps of an FP64 run, the
+    FP64 state and log-weights are written into a fresh FP32 and a fresh
+    FP64 filter (same seed, so the same draws), each takes that step, and
+    the increments are compared relative to the FP64 increment's size
+    (max(|increment|, 1)).  This separates the FP32 arithmetic from the
+    run-to-run divergence that resampling and chaos add along a run."""
+    import numpy as np
+    import torch
+    from libbi_b200 import BootstrapPF
+
+    errs = []
+    for s in range(seeds):
+        ref = BootstrapPF(m64, n, resampler="systematic", ess_rel=ESS_REL, seed=30_000 + s)
+        for k in range(max(at) + 1):
+            if k in at:
+                x, lw, _ = ref.state()
+                x, lw = x[:, :n].clone(), lw.clone()
+                lw_inj = float(torch.logsumexp(lw, 0)) - np.log(n)
+                incs = []
+                for m, y in ((m32, y32), (m64, y64)):
+                    pf = BootstrapPF(m, n, resampler="systematic", ess_rel=ESS_REL, seed=40_000 + s)
+                    xv, lwv, _ = pf.state()
+                    xv[:, :n].copy_(x.to(xv.dtype))
+                    lwv.copy_(lw)
+                    incs.append(pf.step(k * DT, (k + 1) * DT, y[k]).log_increment)
+                    pf.close()
+                errs.append(abs(incs[0] - incs[1]) / max(abs(incs[1] - lw_inj), 1.0))
+            ref.step(k * DT, (k + 1) * DT, y64[k])
+        ref.close()
+    errs = np.array(errs)
+    return {"steps_sampled": list(at), "seeds": seeds, "median_rel_err": float(np.median(errs)),
+            "max_rel_err": float(errs.max()), "within_1e-4": bool(errs.max() <= 1e-4)}
+
+
 def equal_mean_time(boot, ll_target):
     """Device time per run of a bootstrap filter whose mean log-likelihood
     equals ll_target, interpolated linearly in log N between the two
@@ -508,6 +594,7 @@ def main():
     ap.add_argument("--no-large-n", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-guided", action="store_true")
+    ap.add_argument("--no-precision", action="store_true")
     ap.add_argument("--guided-seeds", type=int, default=64,
                     help="filter runs per N in the guided/bootstrap comparison (64; fewer for profiling)")
     args = ap.parse_args()
@@ -644,6 +731,8 @@ def main():
     if rank == 0 and not args.no_batched:
         line["batched"] = batched_filters()
         line["pmmh"] = pmmh_chains()
+    if rank == 0 and not args.no_precision:
+        line["precision"] = precision_check(y_host)
     if rank == 0 and not args.no_guided:
         line["guided"] = guided_vs_bootstrap(y_host, seeds=max(2, args.guided_seeds))
     if rank == 0 and not args.no_cpu_baseline:
