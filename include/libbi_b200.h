@@ -486,6 +486,12 @@ int bpf_proposal_set_params(bpf_proposal* p, const float* params, const float* s
  * by p(y|x') p(x'|x) / q(x'|x, y); unobserved steps use the transition.  The
  * proposal must outlive its use by the handle. */
 int bpf_set_proposal(bpf_handle* h, bpf_proposal* p);
+/* The same for every filter of a batch (L96, dim 40, FP32; no counterpart in
+ * the reference): observed steps of the proposal's dt run the guided step
+ * for all filters in one launch, each filter with its own seed and theta,
+ * bit for bit a single filter's guided step with that seed and theta.  A
+ * captured filter run is recaptured after a change. */
+int bpf_batch_set_proposal(bpf_batch* b, bpf_proposal* p);
 
 /* ---- checkpoint (BootstrapPFState save/load,
  *      share/src/bi/state/BootstrapPFState.hpp:216-231) ------------------- */

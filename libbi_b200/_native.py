@@ -49,6 +49,7 @@ EXPORTS = (
     "bpf_pmmh_create", "bpf_pmmh_destroy", "bpf_pmmh_run", "bpf_pmmh_state", "bpf_dense_bf16",
     "bpf_proposal_create", "bpf_proposal_destroy", "bpf_proposal_set_data", "bpf_proposal_train",
     "bpf_proposal_loss_grad", "bpf_proposal_params", "bpf_proposal_set_params", "bpf_set_proposal",
+    "bpf_batch_set_proposal",
     "bpf_path_cache", "bpf_sample_path", "bpf_step_sparse", "bpf_smc2_run",
 )
 
@@ -167,6 +168,7 @@ def _declare(L):
         "bpf_proposal_params": (c_int, [H, c_void_p, c_void_p, c_void_p, POINTER(c_int)]),
         "bpf_proposal_set_params": (c_int, [H, c_void_p, c_void_p, c_void_p]),
         "bpf_set_proposal": (c_int, [H, H]),
+        "bpf_batch_set_proposal": (c_int, [H, H]),
         "bpf_path_cache": (c_int, [H, c_int]),
         "bpf_smc2_run": (c_int, [POINTER(ModelDesc), POINTER(Smc2Config), c_int, c_double, c_double, c_void_p,
                                  c_void_p, c_void_p, c_void_p, c_void_p, POINTER(c_int), POINTER(c_double)]),

@@ -22,6 +22,8 @@
 #include "reduce.cuh"
 #include "model_body.cuh"
 #include "resample_common.cuh"
+#include "batch.cuh"
+#include "proposal.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -29,16 +31,6 @@
 #include <vector>
 
 namespace bpf {
-
-struct BatchFilter {
-  int n;          // particles
-  int off;        // first column in the shared buffers
-  int block0;     // first transition block (and partial)
-  int nblocks;    // transition blocks
-  int resampler;  // BPF_RESAMPLER_*
-  int B;          // Metropolis steps
-  uint64_t seed;
-};
 
 constexpr int kBatchThreads = 1024;
 
@@ -91,16 +83,6 @@ __global__ void k_batch_pz_init(T* x, int ld, double* lw, const BatchFilter* fil
   x[col] = Prec<T>::exp_(Prec<T>::fma_((T)prm.p0_sigma, z0, (T)prm.p0_mu));
   x[(size_t)ld + col] = Prec<T>::exp_(Prec<T>::fma_((T)prm.z0_sigma, z1, (T)prm.z0_mu));
   lw[col] = 0.0;
-}
-
-// the finalising block of filter f appends (logIncrement, ESS, resampled)
-__device__ __forceinline__ void batch_record(const StepStats* st, double* hist, int nf, int f, int k) {
-  if (hist && threadIdx.x == 0) {
-    double* h = hist + 3 * ((size_t)k * nf + f);
-    h[0] = st->inc;
-    h[1] = st->ess;
-    h[2] = (double)st->resampled;
-  }
 }
 
 // ---------------------------------------------------------------------------
@@ -474,6 +456,9 @@ int configure_batch_resample(int max_n) {
 struct bpf_batch {
   bpf::ModelArgs model;
   int nf = 0, ld = 0, blocks = 0, max_n = 0, esz = 0, nobs = 0, bs = 0;
+  int tiles = 0;               // 128-particle tiles over all filters (guided step)
+  bpf_proposal* prop = nullptr;  // learned proposal (bpf_batch_set_proposal), owned by the caller
+  int* tile2f = nullptr;       // tile -> filter, allocated with the proposal
   double ess_rel = 0.0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
@@ -551,7 +536,7 @@ void batch_free(bpf_batch* b) {
   for (cudaEvent_t e : b->ev)
     if (e) cudaEventDestroy(e);
   void* ptrs[] = {b->x[0], b->x[1], b->lw, b->as, b->stats, b->partials, b->counters, b->filt_dev,
-                  b->prm_dev, b->blk2f, b->order, b->lu, b->os, b->y_dev, b->hist};
+                  b->prm_dev, b->blk2f, b->order, b->lu, b->os, b->y_dev, b->hist, b->tile2f};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
@@ -579,9 +564,36 @@ int batch_enqueue_step(bpf_batch* b, double t1, double t2, const void* y_dev, do
   int rc = bpf::launch_batch_resample(b->lw, b->as, b->filt_dev, b->order, b->nf, b->max_n, b->stats, b->lu,
                                       b->os, step, b->stream);
   if (rc) return rc;
-  rc = bpf::launch_batch_transition(b->model, b->x[b->cur], b->x[b->cur ^ 1], b->ld, b->as, b->lw, y_dev, t1, t2,
-                                    step, b->filt_dev, b->prm_dev, b->blk2f, b->blocks, b->stats, b->partials,
-                                    b->counters, hist, b->nf, k, b->stream);
+  if (b->prop && y_dev) {
+    // guided step: the learned proposal, trained for one interval
+    const double dt = bpf::proposal_dt(b->prop);
+    if (std::fabs((t2 - t1) - dt) > 1e-9 * dt) return BPF_E_INVALID;
+    bpf::BatchGuidedArgs g;
+    g.x_in = (const float*)b->x[b->cur];
+    g.x_out = (float*)b->x[b->cur ^ 1];
+    g.ld = b->ld;
+    g.as = b->as;
+    g.lw = b->lw;
+    g.y = (const float*)y_dev;
+    g.t1 = t1;
+    g.t2 = t2;
+    g.step = step;
+    g.filt = b->filt_dev;
+    g.prms = (const bpf::L96Params*)b->prm_dev;
+    g.tile2f = b->tile2f;
+    g.tiles = b->tiles;
+    g.stats = b->stats;
+    g.partials = b->partials;
+    g.counters = b->counters;
+    g.hist = hist;
+    g.nf = b->nf;
+    g.k = k;
+    rc = bpf::launch_batch_guided(*bpf::proposal_net(b->prop), g, b->stream);
+  } else {
+    rc = bpf::launch_batch_transition(b->model, b->x[b->cur], b->x[b->cur ^ 1], b->ld, b->as, b->lw, y_dev, t1,
+                                      t2, step, b->filt_dev, b->prm_dev, b->blk2f, b->blocks, b->stats,
+                                      b->partials, b->counters, hist, b->nf, k, b->stream);
+  }
   if (rc) return rc;
   b->cur ^= 1;
   b->step = step;
@@ -660,6 +672,9 @@ int bpf_batch_create(const bpf_model_desc* model, int nfilters, const bpf_batch_
     d.resampler = bf.resampler;
     d.B = bf.metropolis_steps;
     d.seed = bf.seed;
+    d.tile0 = b->tiles;
+    d.ntiles = (bf.nparticles + 127) / 128;
+    b->tiles += d.ntiles;
     for (int i = 0; i < BPF_MAX_THETA; ++i) b->theta[(size_t)f * BPF_MAX_THETA + i] = bf.theta[i];
     for (int k = 0; k < d.nblocks; ++k) blk2f.push_back(f);
     off += d.nblocks * b->bs;
@@ -757,6 +772,31 @@ static int batch_timing_end(bpf_batch* b, int steps) {
   BPF_TRY(cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]));
   b->timed_ms += ms;
   b->timed_steps += steps;
+  return BPF_OK;
+}
+
+int bpf_batch_set_proposal(bpf_batch* b, bpf_proposal* p) {
+  if (!b) return BPF_E_INVALID;
+  if (p) {
+    if (b->model.kind != BPF_MODEL_L96 || b->model.dim != 40 || b->model.precision != BPF_F32) return BPF_E_INVALID;
+    const bpf::ProposalNet& net = *bpf::proposal_net(p);
+    if (net.dim != b->model.dim || net.hidden != bpf::kProposalHidden) return BPF_E_INVALID;
+    if (!b->tile2f) {
+      std::vector<int> t2f((size_t)b->tiles);
+      for (int f = 0; f < b->nf; ++f)
+        for (int t = 0; t < b->filt[f].ntiles; ++t) t2f[(size_t)b->filt[f].tile0 + t] = f;
+      int rc = dalloc(&b->tile2f, t2f.size() * sizeof(int));
+      if (rc) return rc;
+      BPF_TRY(cudaMemcpyAsync(b->tile2f, t2f.data(), t2f.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+      BPF_TRY(cudaStreamSynchronize(b->stream));  // t2f is a temporary
+    }
+  }
+  if (p != b->prop && b->graph) {
+    // the captured steps launch the other step kernel
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  b->prop = p;
   return BPF_OK;
 }
 

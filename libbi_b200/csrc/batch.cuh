@@ -1,0 +1,32 @@
+// A batch of independent filters in shared structure-of-arrays buffers
+// (batch.cu): the per-filter layout the batch kernels index through, and
+// the per-step history record.  The guided step of a batch (guided.cu) uses
+// the same layout.
+#pragma once
+#include "internal.cuh"
+
+namespace bpf {
+
+struct BatchFilter {
+  int n;          // particles
+  int off;        // first column in the shared buffers
+  int block0;     // first transition block (and partial)
+  int nblocks;    // transition blocks
+  int resampler;  // BPF_RESAMPLER_*
+  int B;          // Metropolis steps
+  uint64_t seed;
+  int tile0;      // first 128-particle tile of the guided step
+  int ntiles;     // 128-particle tiles of the guided step
+};
+
+// the finalising block of filter f appends (logIncrement, ESS, resampled)
+__device__ __forceinline__ void batch_record(const StepStats* st, double* hist, int nf, int f, int k) {
+  if (hist && threadIdx.x == 0) {
+    double* h = hist + 3 * ((size_t)k * nf + f);
+    h[0] = st->inc;
+    h[1] = st->ess;
+    h[2] = (double)st->resampled;
+  }
+}
+
+}  // namespace bpf

@@ -34,6 +34,7 @@
 #include "model_body.cuh"
 #include "tc.cuh"
 #include "proposal.cuh"
+#include "batch.cuh"
 
 namespace bpf {
 
@@ -116,15 +117,42 @@ struct GuidedWeights {
   const float *b1, *b2, *b3, *shift, *scale;
 };
 
-template <int D, int TILES>
-__global__ void __launch_bounds__(kGTile * TILES, TILES == 1 ? 3 : 2)
-k_guided_fused(const float* __restrict__ x_in, float* __restrict__ x_out, int ld, int n,
-               const int* __restrict__ as, double* __restrict__ lw, const float* __restrict__ y, double t1,
-               double t2, uint64_t seed, int step, L96Params prm, StepStats* st, LwPartial* partials,
-               unsigned* counter, GuidedWeights w, int* err) {
+// Launch arguments of both forms: one filter (the per-filter fields) or a
+// batch (the per-filter fields come from the batch's tables).
+struct GuidedKernelArgs {
+  const float* x_in;
+  float* x_out;
+  int ld;
+  int* as;
+  double* lw;
+  const float* y;
+  double t1, t2;
+  int step;
+  GuidedWeights w;
+  int* err;
+  LwPartial* partials;
+  // one filter
+  int n;
+  uint64_t seed;
+  L96Params prm;
+  StepStats* st;
+  unsigned* counter;
+  // a batch: filter f owns tiles [tile0_f, tile0_f + ntiles_f)
+  const BatchFilter* filt;
+  const L96Params* prms;
+  const int* tile2f;
+  StepStats* stats;
+  unsigned* counters;
+  double* hist;
+  int nf, k;
+};
+
+template <int D, int TILES, bool BATCH>
+__global__ void __launch_bounds__(kGTile * TILES, TILES == 1 ? 3 : 2) k_guided_fused(GuidedKernelArgs a) {
   constexpr int DIN = 2 * D, DOUT = 2 * D, H = kProposalHidden;
   constexpr uint32_t W1B = H * DIN * 2, W2B = H * H * 2, W3B = DOUT * H * 2;
   static_assert(DIN % 16 == 0 && DOUT % 16 == 0 && DIN <= H && DOUT <= H && D % 8 == 0, "tile shapes");
+  static_assert(!BATCH || TILES == 1, "a batch CTA holds one tile of one filter");
   extern __shared__ unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   unsigned char* sW = smem;                // weights of the current layer
@@ -134,7 +162,48 @@ k_guided_fused(const float* __restrict__ x_in, float* __restrict__ x_out, int ld
   const int tid = threadIdx.x, warp = tid >> 5;
   const int tile = tid / kGTile, r = tid % kGTile;
   unsigned char* sT = sA + tile * kGTileBytes;  // this thread's tile
-  const int p = (blockIdx.x * TILES + tile) * kGTile + r;
+  // this CTA's filter: particles, first column, tiles before this CTA's
+  // within the filter, partial slots, draws, constants and statistics
+  int f = 0, n, off, tbase, pidx, pbase, np;
+  uint64_t seed;
+  L96Params prm;
+  StepStats* st;
+  unsigned* counter;
+  const float* y;
+  if (BATCH) {
+    f = __ldg(a.tile2f + blockIdx.x);
+    const BatchFilter fd = a.filt[f];
+    n = fd.n;
+    off = fd.off;
+    tbase = blockIdx.x - fd.tile0;
+    pidx = fd.block0 + tbase;
+    pbase = fd.block0;
+    np = fd.ntiles;
+    seed = fd.seed;
+    prm = a.prms[f];
+    st = a.stats + f;
+    counter = a.counters + f;
+    y = a.y + (size_t)f * D;
+  } else {
+    n = a.n;
+    off = 0;
+    tbase = blockIdx.x * TILES;
+    pidx = blockIdx.x;
+    pbase = 0;
+    np = gridDim.x;
+    seed = a.seed;
+    prm = a.prm;
+    st = a.st;
+    counter = a.counter;
+    y = a.y;
+  }
+  const float* __restrict__ x_in = a.x_in;
+  float* __restrict__ x_out = a.x_out;
+  double* __restrict__ lw = a.lw;
+  const int ld = a.ld, step = a.step;
+  const GuidedWeights& w = a.w;
+  const int p = (tbase + tile) * kGTile + r;  // particle within the filter
+  const int col = off + p;
   const int resampled = st->resample;
   const bool ok_in = st->status == BPF_OK;
   if (warp == 0) tc::tmem_alloc(&s_taddr, 128 * TILES);
@@ -157,17 +226,18 @@ k_guided_fused(const float* __restrict__ x_in, float* __restrict__ x_out, int ld
     }
     // 1. ancestor, RK4 mean, network input row
     const bool live = p < n;
-    const int src = live ? (resampled ? min(max(as[p], 0), n - 1) : p) : 0;
+    const int src = live ? (resampled ? min(max(a.as[col], 0), n - 1) : p) : 0;
+    if (BATCH && live && resampled) a.as[col] = src;
     float m[D], u[8];
 #pragma unroll
-    for (int i = 0; i < D; ++i) m[i] = live ? __ldg(x_in + (size_t)i * ld + src) : 0.0f;
+    for (int i = 0; i < D; ++i) m[i] = live ? __ldg(x_in + (size_t)i * ld + off + src) : 0.0f;
 #pragma unroll
     for (int c = 0; c < D / 8; ++c) {
 #pragma unroll
       for (int j = 0; j < 8; ++j) u[j] = (m[8 * c + j] - __ldg(w.shift + 8 * c + j)) * __ldg(w.scale + 8 * c + j);
       *reinterpret_cast<uint4*>(sT + tc::kmajor_off(r, 8 * c, DIN)) = pack8(u);
     }
-    l96_rk4<float, D>(m, t1, t2, (float)prm.F, (float)prm.h);
+    l96_rk4<float, D>(m, a.t1, a.t2, (float)prm.F, (float)prm.h);
 #pragma unroll
     for (int c = 0; c < D / 8; ++c) {
 #pragma unroll
@@ -212,7 +282,7 @@ k_guided_fused(const float* __restrict__ x_in, float* __restrict__ x_out, int ld
       const float se = (float)prm.sigma_eta, ise = 1.0f / se, lse = logf(se);
       const float sy = (float)prm.sigma_y, isy = (float)prm.inv_sigma_y;
       const float c2 = (float)prm.c_half_log_2pi, ls = (float)prm.log_sigma_y;
-      double l = live ? (resampled ? st->ll : lw[p]) : 0.0;
+      double l = live ? (resampled ? st->ll : lw[col]) : 0.0;
       double corr = 0.0;  // log p(x' | x) - log q(x' | x, y), the 2 pi terms cancel
 #pragma unroll 1
       for (int c = 0; c < D / 8; ++c) {
@@ -233,7 +303,7 @@ k_guided_fused(const float* __restrict__ x_in, float* __restrict__ x_out, int ld
               const float s = fminf(fmaxf((h ? sr[4 + j] : sr[j]) + __ldg(w.b3 + D + i), kSMin), kSMax);
               const float dx = delta + expf(s) * z[j];  // x' - m
               const float xi = mrow[i] + dx;
-              x_out[(size_t)i * ld + p] = xi;
+              x_out[(size_t)i * ld + col] = xi;
               const float e = dx * ise;
               corr += (double)(-0.5f * e * e - lse) - (double)(-0.5f * z[j] * z[j] - s);
               float dz = __ldg(y + i) - xi;
@@ -245,7 +315,7 @@ k_guided_fused(const float* __restrict__ x_in, float* __restrict__ x_out, int ld
       }
       if (live) {
         l += corr;
-        lw[p] = l;
+        lw[col] = l;
         lw_push(part, l);
       }
     }
@@ -256,47 +326,101 @@ k_guided_fused(const float* __restrict__ x_in, float* __restrict__ x_out, int ld
   // a wait that gave up: the proposal's flag and the step's status (the
   // filter's next read of its statistics returns it)
   if (ok_in && !ok && tid == 0) {
-    atomicExch(err, 1);
+    atomicExch(a.err, 1);
     st->status = BPF_E_TIMEOUT;
   }
-  transition_reduce_tail(part, partials, blockIdx.x, 0, gridDim.x, counter, n, st, ok_in && ok, resampled, true);
+  if (transition_reduce_tail(part, a.partials, pidx, pbase, np, counter, n, st, ok_in && ok, resampled, true) &&
+      BATCH)
+    batch_record(st, a.hist, a.nf, f, a.k);
 }
 
-template <int TILES>
-int launch_fused(ProposalNet& net, const GuidedArgs& a, const L96Params& prm, cudaStream_t st) {
-  const int per = kGTile * TILES;
-  const int blocks = (a.n + per - 1) / per;
-  if (blocks > a.max_partials) return BPF_E_INVALID;
+template <int TILES, bool BATCH>
+int launch_fused(const GuidedKernelArgs& ka, int blocks, cudaStream_t st) {
   static bool configured = false;
   if (!configured) {
-    BPF_TRY(cudaFuncSetAttribute(k_guided_fused<40, TILES>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    BPF_TRY(cudaFuncSetAttribute(k_guided_fused<40, TILES, BATCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  guided_smem<TILES>()));
     configured = true;
   }
-  GuidedWeights w{net.packed, net.pk_w1, net.pk_w2, net.pk_w3, net.b1(), net.b2(), net.b3(), net.shift, net.scale};
-  k_guided_fused<40, TILES><<<blocks, per, guided_smem<TILES>(), st>>>(
-      (const float*)a.x_in, (float*)a.x_out, a.ld, a.n, a.as, a.lw, (const float*)a.y, a.t1, a.t2, a.seed, a.step,
-      prm, a.stats, a.partials, a.counter, w, net.err);
+  k_guided_fused<40, TILES, BATCH><<<blocks, kGTile * TILES, guided_smem<TILES>(), st>>>(ka);
   BPF_TRY(cudaGetLastError());
   return BPF_OK;
 }
 
-}  // namespace
-
-int launch_guided(ProposalNet& net, const GuidedArgs& a, cudaStream_t st) {
-  if (a.n <= 0 || !a.y) return BPF_E_INVALID;  // the proposal needs the observation
+int check_net(const ProposalNet& net) {
   if (net.dim != 40 || net.hidden != kProposalHidden || net.din != 80 || net.dout != 80 || !net.packed)
     return BPF_E_INVALID;
   // the weight images are copied in bulk: 16-byte aligned starts and sizes
   if (((reinterpret_cast<uintptr_t>(net.packed) | (uintptr_t)net.pk_w1 | (uintptr_t)net.pk_w2 |
         (uintptr_t)net.pk_w3) & 15) != 0)
     return BPF_E_INVALID;
-  const L96Params prm = l96_params<float>(a.theta, a.h);
+  return BPF_OK;
+}
+
+GuidedWeights weights_of(const ProposalNet& net) {
+  return GuidedWeights{net.packed, net.pk_w1, net.pk_w2, net.pk_w3, net.b1(), net.b2(), net.b3(), net.shift,
+                       net.scale};
+}
+
+}  // namespace
+
+int launch_guided(ProposalNet& net, const GuidedArgs& a, cudaStream_t st) {
+  if (a.n <= 0 || !a.y) return BPF_E_INVALID;  // the proposal needs the observation
+  int rc = check_net(net);
+  if (rc) return rc;
+  GuidedKernelArgs ka{};
+  ka.x_in = (const float*)a.x_in;
+  ka.x_out = (float*)a.x_out;
+  ka.ld = a.ld;
+  ka.as = const_cast<int*>(a.as);
+  ka.lw = a.lw;
+  ka.y = (const float*)a.y;
+  ka.t1 = a.t1;
+  ka.t2 = a.t2;
+  ka.step = a.step;
+  ka.w = weights_of(net);
+  ka.err = net.err;
+  ka.partials = a.partials;
+  ka.n = a.n;
+  ka.seed = a.seed;
+  ka.prm = l96_params<float>(a.theta, a.h);
+  ka.st = a.stats;
+  ka.counter = a.counter;
   // two tiles per CTA once single-tile CTAs would need more than one wave
   // at three CTAs per SM
   const int tiles = (a.n + kGTile - 1) / kGTile;
-  if (tiles > 3 * 148) return launch_fused<2>(net, a, prm, st);
-  return launch_fused<1>(net, a, prm, st);
+  const int tiles_per_cta = tiles > 3 * 148 ? 2 : 1;
+  const int blocks = (tiles + tiles_per_cta - 1) / tiles_per_cta;
+  if (blocks > a.max_partials) return BPF_E_INVALID;
+  return tiles_per_cta == 2 ? launch_fused<2, false>(ka, blocks, st) : launch_fused<1, false>(ka, blocks, st);
+}
+
+int launch_batch_guided(ProposalNet& net, const BatchGuidedArgs& a, cudaStream_t st) {
+  if (a.tiles <= 0 || !a.y || !a.tile2f) return BPF_E_INVALID;
+  int rc = check_net(net);
+  if (rc) return rc;
+  GuidedKernelArgs ka{};
+  ka.x_in = a.x_in;
+  ka.x_out = a.x_out;
+  ka.ld = a.ld;
+  ka.as = a.as;
+  ka.lw = a.lw;
+  ka.y = a.y;
+  ka.t1 = a.t1;
+  ka.t2 = a.t2;
+  ka.step = a.step;
+  ka.w = weights_of(net);
+  ka.err = net.err;
+  ka.partials = a.partials;
+  ka.filt = a.filt;
+  ka.prms = a.prms;
+  ka.tile2f = a.tile2f;
+  ka.stats = a.stats;
+  ka.counters = a.counters;
+  ka.hist = a.hist;
+  ka.nf = a.nf;
+  ka.k = a.k;
+  return launch_fused<1, true>(ka, a.tiles, st);
 }
 
 }  // namespace bpf

@@ -76,6 +76,30 @@ struct GuidedArgs {
 };
 int launch_guided(ProposalNet& net, const GuidedArgs& a, cudaStream_t st);
 
+// the guided step of every filter of a batch (guided.cu, batch.cu)
+struct BatchFilter;
+struct L96Params;
+struct BatchGuidedArgs {
+  const float* x_in;
+  float* x_out;
+  int ld;
+  int* as;
+  double* lw;
+  const float* y;  // nf x dim device observations
+  double t1, t2;
+  int step;
+  const BatchFilter* filt;
+  const L96Params* prms;
+  const int* tile2f;  // 128-particle tile -> filter
+  int tiles;
+  StepStats* stats;
+  LwPartial* partials;
+  unsigned* counters;
+  double* hist;
+  int nf, k;
+};
+int launch_batch_guided(ProposalNet& net, const BatchGuidedArgs& a, cudaStream_t st);
+
 }  // namespace bpf
 
 struct bpf_proposal;

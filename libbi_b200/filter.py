@@ -480,6 +480,13 @@ class BatchedBootstrapPF:
                                 st.ctypes.data_as(ctypes.c_void_p))
         return ll, ess, st
 
+    def set_proposal(self, proposal):
+        """Attach a LearnedProposal to every filter (or None to detach):
+        observed steps then run the guided step for the whole batch."""
+        N.check(N.lib().bpf_batch_set_proposal(self._h, None if proposal is None else proposal.handle),
+                "bpf_batch_set_proposal")
+        self._proposal = proposal
+
     def filter(self, y, t0: float = 0.0, dt: float = 1.0):
         """Filter<BootstrapPF>::filter for every filter; y: (T, nfilters,
         nobs) host observations.  Returns (logLikelihood[F],
