@@ -466,7 +466,7 @@ def equal_mean_time(boot, ll_target):
 
 def guided_vs_bootstrap(y_host, seeds=64, n_guided=(4096, 16384, 65536),
                         n_boot=(16384, 65536, 262144, 1 << 20, 1 << 22), n_ref=65536, n_data=1 << 20,
-                        train_steps=3000):
+                        train_steps=3000, n_guided_batched=(1024, 4096, 16384), n_boot_batched=(16384, 32768)):
     """The learned proposal on the Lorenz-96 workload: trained on 2^20
     (x_t, x_{t+1}, y_{t+1}) triples simulated by the model (2^20 particles
     spun up for 100 intervals from the initial distribution, one more
@@ -481,10 +481,15 @@ def guided_vs_bootstrap(y_host, seeds=64, n_guided=(4096, 16384, 65536),
     the filters have lost the track (the deviation flat in N) the
     estimator's downward bias is what more particles buy; the second
     comparison is the device time at which the bootstrap sweep reaches each
-    guided filter's mean log-likelihood."""
+    guided filter's mean log-likelihood.  The batched rows run the same
+    seeds as one batch of filters (guided: the fused guided step over every
+    filter's tiles), with the device time per filter; the bootstrap filters
+    the guided ones are matched against need hundreds of thousands of
+    particles, beyond a batch's per-filter limit, and are timed singly (at
+    those sizes a single filter already fills the GPU)."""
     import numpy as np
     import torch
-    from libbi_b200 import BootstrapPF, LearnedProposal, configs
+    from libbi_b200 import BatchedBootstrapPF, BootstrapPF, LearnedProposal, configs
 
     model = configs.L96_D40_N65536["model"]
     sim = BootstrapPF(model, n_data, seed=3)
@@ -522,9 +527,39 @@ def guided_vs_bootstrap(y_host, seeds=64, n_guided=(4096, 16384, 65536),
         lls = np.array(lls)
         return {"n": n, "ll_mean": float(lls.mean()), "ll_sd": float(lls.std(ddof=1)), "ms_per_run": ms / seeds}
 
+    def run_batched(n, use_prop):
+        # the same seeds as the single filters, one filter per seed in one
+        # batch (the same numbers, bit for bit); device time of the captured
+        # run divided by the filters
+        b = BatchedBootstrapPF([model] * seeds, [n] * seeds, "systematic", [10_000 + s for s in range(seeds)],
+                               ess_rel=ESS_REL)
+        if use_prop:
+            b.set_proposal(prop)
+        yb = np.ascontiguousarray(np.repeat(np.asarray(y_host, np.float32)[:, None, :], seeds, axis=1))
+        b.filter(yb, 0.0, DT)  # capture
+        b.timing(True)
+        b.timing_read(reset=True)
+        lls, _, _, st = b.filter(yb, 0.0, DT)
+        ms, _ = b.timing_read(reset=True)
+        b.close()
+        return {"n": n, "filters": seeds, "ll_mean": float(lls.mean()), "ll_sd": float(lls.std(ddof=1)),
+                "ms_per_run": ms / seeds, "batch_ms": ms, "failed": int((st != 0).sum())}
+
     boot = [run(n, False) for n in n_boot]
     guided = [run(n, True) for n in n_guided]
+    guided_b = [run_batched(n, True) for n in n_guided_batched]
+    boot_b = [run_batched(n, False) for n in n_boot_batched]
     prop.close()
+    # the bootstrap filter's best measured cost per particle-step (single or
+    # batched): the conservative price of a bootstrap filter of any size
+    T = len(y_host)
+    best_ns = min(b["ms_per_run"] * 1e6 / (b["n"] * T) for b in boot + boot_b)
+    for gd in guided_b:
+        t_b, n_b, exact = equal_mean_time(boot, gd["ll_mean"])
+        gd["bootstrap_n_at_equal_mean_ll"] = n_b
+        gd["gpu_time_ratio_bootstrap_over_guided_at_equal_mean_ll"] = t_b / gd["ms_per_run"]
+        gd["gpu_time_ratio_at_equal_mean_ll_bootstrap_at_best_rate"] = n_b * T * best_ns * 1e-6 / gd["ms_per_run"]
+        gd["equal_mean_ll_ratio_is"] = "interpolated" if exact else "bound: outside the bootstrap sweep"
     ref = next(b for b in boot if b["n"] == n_ref)
     for gd in guided:
         t_match = gd["ms_per_run"] * (gd["ll_sd"] / ref["ll_sd"]) ** 2 if ref["ll_sd"] > 0 else float("nan")
@@ -540,6 +575,7 @@ def guided_vs_bootstrap(y_host, seeds=64, n_guided=(4096, 16384, 65536),
     slope = float(np.polyfit(ln_n, ln_sd, 1)[0]) if len(boot) > 1 else None
     best = max(guided, key=lambda gd: gd["gpu_time_ratio_bootstrap_over_guided_at_equal_sd"] or 0.0)
     best_m = max(guided, key=lambda gd: gd["gpu_time_ratio_bootstrap_over_guided_at_equal_mean_ll"])
+    best_b = max(guided_b, key=lambda gd: gd["gpu_time_ratio_bootstrap_over_guided_at_equal_mean_ll"])
     return {
         "workload": f"l96_d40_t200_guided_vs_bootstrap_n{n_ref}_{seeds}seeds",
         "train": {"triples": n_data, "steps": train_steps, "batch": 8192, "seconds": train_s,
@@ -549,12 +585,20 @@ def guided_vs_bootstrap(y_host, seeds=64, n_guided=(4096, 16384, 65536),
                                                          + 0.5))},
         "bootstrap": boot,
         "guided": guided,
+        "batched": {"guided": guided_b, "bootstrap": boot_b},
         "bootstrap_sd_exponent_in_n": slope,
         "best": {"equal_sd": {"guided_n": best["n"], "gpu_time_ratio_bootstrap_over_guided":
                               best["gpu_time_ratio_bootstrap_over_guided_at_equal_sd"]},
                  "equal_mean_ll": {"guided_n": best_m["n"], "gpu_time_ratio_bootstrap_over_guided":
                                    best_m["gpu_time_ratio_bootstrap_over_guided_at_equal_mean_ll"],
-                                   "is": best_m["equal_mean_ll_ratio_is"]}},
+                                   "is": best_m["equal_mean_ll_ratio_is"]},
+                 "equal_mean_ll_guided_batched": {
+                     "guided_n": best_b["n"], "gpu_time_ratio_bootstrap_over_guided":
+                         best_b["gpu_time_ratio_bootstrap_over_guided_at_equal_mean_ll"],
+                     "gpu_time_ratio_bootstrap_at_best_rate":
+                         best_b["gpu_time_ratio_at_equal_mean_ll_bootstrap_at_best_rate"],
+                     "is": best_b["equal_mean_ll_ratio_is"]}},
+        "bootstrap_best_ns_per_particle_step": best_ns,
         "timer": "CUDA events around each step's kernels, summed per filter run",
     }
 
