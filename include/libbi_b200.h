@@ -253,6 +253,27 @@ int bpf_resampler_ancestors(bpf_resampler* r, const double* lw, int n,
 int bpf_resampler_timing_enable(bpf_resampler* r, int enable);
 int bpf_resampler_timing_read(bpf_resampler* r, int reset, double* ms, int* calls);
 
+/* Autotuner of the one-launch systematic resampler (no counterpart in the
+ * reference): tile shapes of threads per block x particles per thread
+ * (0: 256 x 2, 1: 128 x 4, 2: 512 x 1, 3: 512 x 2, 4: 256 x 4,
+ * 5: 1024 x 1), all computing the same ancestors.  bpf_autotune_resampler
+ * times every shape that fits the GPU in one wave on seeded synthetic
+ * log-weights of n particles (on `stream`, which it synchronises; not
+ * while the stream is being captured) and keeps the fastest for n's size
+ * class (the next power of two) on the current device for the rest of the
+ * process; bpf_create runs it for its N.  out (may be NULL) receives the
+ * chosen shape and each shape's median microseconds (0: does not fit). */
+#define BPF_RESAMPLE_SHAPES 6
+typedef struct {
+  int shape;
+  double us[BPF_RESAMPLE_SHAPES];
+} bpf_tune_result;
+int bpf_autotune_resampler(int n, void* stream, bpf_tune_result* out);
+/* Pin the shape a stand-alone resampler uses (-1: the autotuned shape, else
+ * shape 0); a shape that does not fit in one wave falls back to one that
+ * does. */
+int bpf_resampler_set_shape(bpf_resampler* r, int shape);
+
 /* gather_rows (share/src/bi/primitive/matrix_primitive.hpp:630-638,
  * share/src/bi/cuda/primitive/matrix_primitive_kernel.cuh:50-57), out of
  * place on device SoA buffers: Y[j*ld + i] = X[j*ld + as[i]], j < d, i < n.

@@ -7,7 +7,8 @@ reference's filter/resampler classes.
 from ._native import (BpfError, ParticleFilterDegeneratedException, load_library,  # noqa: F401
                       LIB_PATH, EXPORTS)
 from .filter import (BootstrapPF, ModelL96, ModelPZ, Resampler, SystematicResampler,  # noqa: F401
-                     MultinomialResampler, MetropolisResampler, gather_rows, StepResult, BatchedBootstrapPF)
+                     MultinomialResampler, MetropolisResampler, gather_rows, StepResult, BatchedBootstrapPF,
+                     autotune_resampler)
 from .sampler import MarginalMH, Prior, smc2  # noqa: F401
 from .proposal import LearnedProposal  # noqa: F401
 from .schedule import Observer, Schedule, ScheduleElement  # noqa: F401
@@ -15,4 +16,4 @@ from . import configs  # noqa: F401
 
 __all__ = ["BootstrapPF", "ModelL96", "ModelPZ", "Resampler", "SystematicResampler", "MultinomialResampler",
            "MetropolisResampler", "BatchedBootstrapPF", "MarginalMH", "Prior", "smc2", "LearnedProposal", "Observer", "Schedule",
-           "ScheduleElement", "gather_rows", "BpfError", "ParticleFilterDegeneratedException", "configs"]
+           "ScheduleElement", "gather_rows", "autotune_resampler", "BpfError", "ParticleFilterDegeneratedException", "configs"]

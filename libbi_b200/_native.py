@@ -42,7 +42,7 @@ EXPORTS = (
     "bpf_logsumexp_reduce", "bpf_resampler_ancestors", "bpf_gather_rows",
     "bpf_snapshot_size", "bpf_snapshot", "bpf_restore", "bpf_version",
     "bpf_status_string", "bpf_timing_enable", "bpf_timing_read", "bpf_systematic_ancestors_static",
-    "bpf_resampler_timing_enable", "bpf_resampler_timing_read",
+    "bpf_resampler_timing_enable", "bpf_resampler_timing_read", "bpf_autotune_resampler", "bpf_resampler_set_shape",
     "bpf_batch_create", "bpf_batch_destroy", "bpf_batch_init", "bpf_batch_set_theta", "bpf_batch_step_device",
     "bpf_batch_stats", "bpf_batch_state_ptrs", "bpf_filter_batch", "bpf_batch_timing_enable",
     "bpf_batch_timing_read", "bpf_batch_set_seeds",
@@ -96,6 +96,13 @@ class Smc2Config(ctypes.Structure):
         ("ess_rel", c_double), ("theta_ess_rel", c_double), ("moves", c_int), ("seed", c_uint64),
         ("nparams", c_int), ("params", PmmhParam * BPF_MAX_THETA),
     ]
+
+
+RESAMPLE_SHAPES = 6  # BPF_RESAMPLE_SHAPES
+
+
+class TuneResult(ctypes.Structure):
+    _fields_ = [("shape", ctypes.c_int), ("us", ctypes.c_double * RESAMPLE_SHAPES)]
 
 
 class StepOut(ctypes.Structure):
@@ -182,6 +189,8 @@ def _declare(L):
         "bpf_batch_timing_read": (c_int, [H, c_int, POINTER(c_double), POINTER(c_int)]),
         "bpf_resampler_timing_enable": (c_int, [H, c_int]),
         "bpf_resampler_timing_read": (c_int, [H, c_int, POINTER(c_double), POINTER(c_int)]),
+        "bpf_autotune_resampler": (c_int, [c_int, c_void_p, POINTER(TuneResult)]),
+        "bpf_resampler_set_shape": (c_int, [H, c_int]),
         "bpf_systematic_ancestors_static": (c_int, [c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p,
                                                     c_void_p]),
         "bpf_version": (c_char_p, []),

@@ -54,6 +54,7 @@ struct bpf_handle {
 
 struct bpf_resampler {
   int kind = 0, B = 0;
+  int shape = -1;  // pinned tile shape of the one-launch systematic kernel
   cudaStream_t stream = nullptr;
   bpf::ResampleScratch rs;
   // optional device timing of the compute kernels of each call (events
@@ -304,6 +305,12 @@ int bpf_create(const bpf_model_desc* model, const bpf_config* config, bpf_handle
   }
   rc = bpf::scratch_alloc(h->rs, h->n);
   if (rc) { bpf_destroy(h); return rc; }
+  // the resampler's tile shape for this N, tuned once per size class (the
+  // shapes compute the same ancestors, so only the speed depends on it)
+  if (config->resampler == BPF_RESAMPLER_SYSTEMATIC && bpf::autotuned_shape(h->n) < 0) {
+    int best = -1;
+    if (bpf::autotune_systematic(h->n, h->stream, &best, nullptr) != BPF_OK) cudaGetLastError();
+  }
   rc = bpf_init(h);
   if (rc) { bpf_destroy(h); return rc; }
   *out = h;
@@ -792,6 +799,24 @@ int bpf_resampler_timing_read(bpf_resampler* r, int reset, double* ms, int* call
   return BPF_OK;
 }
 
+int bpf_autotune_resampler(int n, void* stream, bpf_tune_result* out) {
+  if (n <= 0) return BPF_E_INVALID;
+  int best = -1;
+  double us[BPF_RESAMPLE_SHAPES];
+  const int rc = bpf::autotune_systematic(n, (cudaStream_t)stream, &best, us);
+  if (out) {
+    out->shape = best;
+    for (int k = 0; k < BPF_RESAMPLE_SHAPES; ++k) out->us[k] = us[k];
+  }
+  return rc;
+}
+
+int bpf_resampler_set_shape(bpf_resampler* r, int shape) {
+  if (!r || shape < -1 || shape >= BPF_RESAMPLE_SHAPES) return BPF_E_INVALID;
+  r->shape = shape;
+  return BPF_OK;
+}
+
 int bpf_ess_reduce(bpf_resampler* r, const double* lw, int n, double* lW, double* ess) {
   if (!r || !lw || n <= 0 || n > r->rs.max_n) return BPF_E_INVALID;
   int rc = reset_status(r);
@@ -841,6 +866,7 @@ int bpf_resampler_ancestors(bpf_resampler* r, const double* lw, int n, const dou
   ra.Os_out = Os;
   ra.gate = nullptr;
   ra.max_known = false;
+  ra.shape = r->shape;
   if ((rc = timing_begin(r))) return rc;
   rc = bpf::launch_resample(ra, r->rs, r->stream);
   if (rc) return rc;

@@ -234,8 +234,14 @@ struct ResampleArgs {
   int* Os_out;
   const int* gate;
   bool max_known;  // s.stats->mx already holds max(lw)
+  int shape = -1;  // tile shape of the one-launch systematic kernel (-1: autotuned or default)
 };
 int launch_resample(const ResampleArgs& a, ResampleScratch& s, cudaStream_t st);
+// time every tile shape of the one-launch systematic resampler for n
+// particles and keep the fastest for n's size class on this device
+int autotune_systematic(int n, cudaStream_t st, int* best, double* us);
+// the kept shape for n's size class, -1 when none was tuned
+int autotuned_shape(int n);
 
 int launch_gather(const int* as, const void* X, void* Y, int n, int d, int ld, int esz,
                   const int* gate, cudaStream_t st);

@@ -174,6 +174,11 @@ class Resampler:
         except Exception:
             pass
 
+    def set_shape(self, shape: int = -1):
+        """Pin the tile shape of the one-launch systematic kernel (0..5; -1:
+        the autotuned shape).  Every shape computes the same ancestors."""
+        N.check(N.lib().bpf_resampler_set_shape(self._h, int(shape)), "bpf_resampler_set_shape")
+
     def timing(self, enable: bool = True):
         """Record CUDA events around the kernels of every later call."""
         N.check(N.lib().bpf_resampler_timing_enable(self._h, int(enable)), "bpf_resampler_timing_enable")
@@ -245,6 +250,18 @@ class StepResult:
     log_increment: float
     log_likelihood: float
     resampled: bool
+
+
+RESAMPLE_SHAPES = ((256, 2), (128, 4), (512, 1), (512, 2), (256, 4), (1024, 1))
+
+
+def autotune_resampler(n: int, stream=None):
+    """Time every tile shape (threads per block, particles per thread) of
+    the one-launch systematic resampler on n synthetic log-weights and keep
+    the fastest for n's size class; returns (shape index, {shape: us})."""
+    r = N.TuneResult()
+    N.check(N.lib().bpf_autotune_resampler(int(n), stream, ctypes.byref(r)), "bpf_autotune_resampler")
+    return r.shape, {RESAMPLE_SHAPES[k]: r.us[k] for k in range(N.RESAMPLE_SHAPES) if r.us[k] > 0}
 
 
 class BootstrapPF:

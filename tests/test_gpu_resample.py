@@ -189,3 +189,37 @@ def test_systematic_multi_tile_matches_oracle(cuda, oracle, n):
     ess_o, lW_o = oracle.ess_reduce(lw)
     np.testing.assert_allclose([ess, lW], [ess_o, lW_o], rtol=1e-11)
     R.close()
+
+
+@pytest.mark.parametrize("n", [700, 2049, 65536, 100003])
+def test_every_tile_shape_gives_the_oracles_ancestors(cuda, oracle, n):
+    """The one-launch systematic kernel in each of its tile shapes (threads
+    per block x particles per thread) computes the same integers: the
+    autotuner may pick any of them."""
+    import torch
+    from libbi_b200 import SystematicResampler
+    from libbi_b200._native import RESAMPLE_SHAPES
+
+    rng = np.random.default_rng(7 * n)
+    lw = rng.standard_normal(n) * 3.0
+    a = rng.random(1)
+    rc, _, Os_o, perm_o = oracle.systematic(lw, a[0], permute=True)
+    assert rc == 0
+    R = SystematicResampler(max_n=n)
+    for k in range(RESAMPLE_SHAPES):
+        R.set_shape(k)
+        perm, Os = R.ancestors(_t(lw, torch.float64), _t(a, torch.float64), permute=True, with_offspring=True)
+        assert _near_tie_ok(oracle, lw, a[0], Os.cpu().numpy(), Os_o), k
+        np.testing.assert_array_equal(perm.cpu().numpy(), perm_o, err_msg=f"shape {k}")
+    R.close()
+
+
+def test_autotune_picks_a_timed_shape(cuda):
+    from libbi_b200 import autotune_resampler
+    from libbi_b200._native import RESAMPLE_SHAPES
+    from libbi_b200.filter import RESAMPLE_SHAPES as SHAPES
+
+    best, us = autotune_resampler(65536)
+    assert 0 <= best < RESAMPLE_SHAPES
+    assert SHAPES[best] in us and us[SHAPES[best]] == min(us.values())
+    assert len(us) >= 2 and all(v > 0 for v in us.values())
