@@ -140,7 +140,8 @@ int bpf_init(bpf_handle* h);
  * with Model::observationLogDensities (model.hpp.tt:757-765) and
  * Resampler::reduce.  y: host pointer to the step's observations in the
  * model precision (L96: dim values; PZ: 1 value), or NULL for an unobserved
- * step.  out may be NULL (no sync). */
+ * step.  out may be NULL (no sync; y in pinned memory must then stay
+ * unchanged until the stream has reached the step). */
 int bpf_step(bpf_handle* h, double t1, double t2, const void* y, bpf_step_out* out);
 
 /* bpf_step with only some components observed: the observation Mask of

@@ -42,6 +42,8 @@ struct bpf_handle {
   int ev_steps = 0;
   // learned proposal (bpf_set_proposal), owned by the caller
   bpf_proposal* prop = nullptr;
+  // pinned host copy of the step statistics (read back after every step)
+  bpf::StepStats* host_stats = nullptr;
   // path cache (bpf_path_cache): pc_len states of dim x ld in the model
   // precision (slot 0 the state the recording started from, slot t the state
   // after t more steps) and the ancestors of each recorded step
@@ -101,8 +103,11 @@ int ensure_y(bpf_handle* h, size_t bytes) {
 }
 
 int read_stats(bpf_handle* h, bpf::StepStats* out) {
-  BPF_TRY(cudaMemcpyAsync(out, h->rs.stats, sizeof(*out), cudaMemcpyDeviceToHost, h->stream));
+  // through the handle's pinned copy: a direct DMA instead of a staged copy
+  bpf::StepStats* dst = h->host_stats ? h->host_stats : out;
+  BPF_TRY(cudaMemcpyAsync(dst, h->rs.stats, sizeof(*out), cudaMemcpyDeviceToHost, h->stream));
   BPF_TRY(cudaStreamSynchronize(h->stream));
+  if (dst != out) *out = *dst;
   return BPF_OK;
 }
 
@@ -145,7 +150,11 @@ int path_record(bpf_handle* h, bool after_step) {
   return BPF_OK;
 }
 
-int enqueue_step(bpf_handle* h, double t1, double t2, const void* y_dev, uint64_t mask = ~0ull) {
+// y_host, y_bytes: when given, the observation is copied from host memory
+// into y_dev after the resampling launch (which does not read it), so the
+// copy overlaps the resampling
+int enqueue_step(bpf_handle* h, double t1, double t2, const void* y_dev, uint64_t mask = ~0ull,
+                 const void* y_host = nullptr, size_t y_bytes = 0) {
   const int k = h->step + 1;
   if (h->timing) {
     int rc = timing_event(h, 0);
@@ -167,6 +176,8 @@ int enqueue_step(bpf_handle* h, double t1, double t2, const void* y_dev, uint64_
   ra.max_known = true;
   int rc = bpf::launch_resample(ra, h->rs, h->stream);
   if (rc) return rc;
+  if (y_host && y_dev) BPF_TRY(cudaMemcpyAsync(const_cast<void*>(y_dev), y_host, y_bytes, cudaMemcpyHostToDevice,
+                                               h->stream));
   if (h->timing) {
     rc = timing_event(h, 1);
     if (rc) return rc;
@@ -305,6 +316,10 @@ int bpf_create(const bpf_model_desc* model, const bpf_config* config, bpf_handle
   }
   rc = bpf::scratch_alloc(h->rs, h->n);
   if (rc) { bpf_destroy(h); return rc; }
+  if (cudaMallocHost((void**)&h->host_stats, sizeof(bpf::StepStats)) != cudaSuccess) {
+    cudaGetLastError();
+    h->host_stats = nullptr;  // read back through pageable memory instead
+  }
   // the resampler's tile shape for this N, tuned once per size class (the
   // shapes compute the same ancestors, so only the speed depends on it)
   if (config->resampler == BPF_RESAMPLER_SYSTEMATIC && bpf::autotuned_shape(h->n) < 0) {
@@ -327,6 +342,7 @@ int bpf_destroy(bpf_handle* h) {
   if (h->y_dev) cudaFree(h->y_dev);
   if (h->hist) cudaFree(h->hist);
   for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
+  if (h->host_stats) cudaFreeHost(h->host_stats);
   void* g[] = {h->pc_x, h->pc_a};
   for (void* p : g)
     if (p) cudaFree(p);
@@ -508,14 +524,14 @@ static void fill_out(const bpf::StepStats& s, bpf_step_out* out) {
 int bpf_step(bpf_handle* h, double t1, double t2, const void* y, bpf_step_out* out) {
   if (!h || !(t1 < t2)) return BPF_E_INVALID;
   const void* yd = nullptr;
+  size_t yb = 0;
   if (y) {
-    const size_t yb = (size_t)nobs(h) * h->esz;
+    yb = (size_t)nobs(h) * h->esz;
     int rc = ensure_y(h, yb);
     if (rc) return rc;
-    BPF_TRY(cudaMemcpyAsync(h->y_dev, y, yb, cudaMemcpyHostToDevice, h->stream));
     yd = h->y_dev;
   }
-  int rc = enqueue_step(h, t1, t2, yd);
+  int rc = enqueue_step(h, t1, t2, yd, ~0ull, y, yb);
   if (rc) return rc;
   if (out) {
     bpf::StepStats s;

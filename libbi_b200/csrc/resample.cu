@@ -8,16 +8,21 @@
 // variants use Thrust for the scan and search and atomics for the
 // permutation (share/src/bi/cuda/resampler/ResamplerKernel.cuh:78-165).
 //
-// Here every pass is a hand-written kernel over tiles of kTile = 2048
-// log-weights (256 threads x 8):
+// Here every pass is a hand-written kernel over tiles of kTile = 512
+// log-weights (256 threads x 2):
 //   weight tile sums   exact 128-bit fixed-point sums of the weights; the
 //                      last block to finish scans the tile sums (no waiting)
 //   offspring          per tile: exact prefix -> FP64 cumulative weight ->
 //                      cumulative offspring, childless counts
 //   permute            survivors in place; copies fill childless slots by a
 //                      search over the cumulative extra-copy counts
-// The FP64 cumulative weight of element i is the exact sum rounded once, so
-// ancestors are independent of tile order, thread count and timing.
+// Permuted systematic resampling runs all of these as phases of one
+// cooperative launch separated by bounded grid barriers (k_systematic_coop1
+// with one tile per block in one of six autotuned tile shapes, or
+// k_systematic_coop with several tiles per block); the passes above are the
+// path for multinomial and Metropolis offspring.  The FP64 cumulative weight
+// of element i is the exact sum rounded once, so ancestors are independent
+// of tile order, tile shape, thread count and timing.
 #include "internal.cuh"
 
 #include <algorithm>
