@@ -419,11 +419,17 @@ k_systematic_coop(const double* __restrict__ lw, int n, StepStats* st, const dou
   }
 
   // phase 1: exact fixed-point weight total of this block's tiles
+  // every tile loop below issues the next tile's loads before the current
+  // tile's arithmetic and block scans, so the memory latency overlaps them
   u128 wsum = u128_zero();
+  double nv[IT];
+  if (tb0 < tb1) load_blocked_n<IT>(lw, tb0 * TL + threadIdx.x * IT, n, nv);
   for (int t = tb0; t < tb1; ++t) {
     const int i0 = t * TL + threadIdx.x * IT;
     double v[IT];
-    load_blocked_n<IT>(lw, i0, n, v);
+#pragma unroll
+    for (int k = 0; k < IT; ++k) v[k] = nv[k];
+    if (t + 1 < tb1) load_blocked_n<IT>(lw, i0 + TL, n, nv);
 #pragma unroll
     for (int k = 0; k < IT; ++k) {
       if (i0 + k < n) {
@@ -455,15 +461,25 @@ k_systematic_coop(const double* __restrict__ lw, int n, StepStats* st, const dou
   u128 carry = prefix_b;
   int zeros = 0;
   if (threadIdx.x == 0) s_prev_os = tb0 == 0 ? 0 : systematic_Os(u128_to_weight(prefix_b), W, yW, nd, a, n);
+  unsigned long long nq[IT];
+  if (tb0 < tb1) {
+    const int j0 = tb0 * TL + threadIdx.x * IT;
+#pragma unroll
+    for (int k = 0; k < IT; ++k) nq[k] = (j0 + k < n) ? __ldcg(qbuf + j0 + k) : 0ull;
+  }
   for (int t = tb0; t < tb1; ++t) {
     const int i0 = t * TL + threadIdx.x * IT;
     unsigned long long q[IT];
     u128 loc = u128_zero();
 #pragma unroll
     for (int k = 0; k < IT; ++k) {
-      q[k] = (i0 + k < n) ? __ldcg(qbuf + i0 + k) : 0ull;
+      q[k] = nq[k];
       u128 qq; qq.lo = q[k]; qq.hi = 0;
       loc = u128_add(loc, qq);
+    }
+    if (t + 1 < tb1) {
+#pragma unroll
+      for (int k = 0; k < IT; ++k) nq[k] = (i0 + TL + k < n) ? __ldcg(qbuf + i0 + TL + k) : 0ull;
     }
     u128 ttot;
     u128 Q = u128_add(carry, block_exclusive_scan_u128(loc, &ttot));
@@ -499,14 +515,28 @@ k_systematic_coop(const double* __restrict__ lw, int n, StepStats* st, const dou
   // phase 3: ranks of childless slots, extra-copy counts, survivors in place
   int zcarry = block_sum_int_from_global(block_z, b);
   const int R = block_sum_int_from_global(block_z, G);
+  int nprev = 0, nos[IT];
+  if (tb0 < tb1) {
+    const int j0 = tb0 * TL + threadIdx.x * IT;
+    nprev = j0 > 0 && j0 - 1 < n ? __ldcg(Os + j0 - 1) : 0;
+#pragma unroll
+    for (int k = 0; k < IT; ++k) nos[k] = (j0 + k < n) ? __ldcg(Os + j0 + k) : nprev;
+  }
   for (int t = tb0; t < tb1; ++t) {
     const int i0 = t * TL + threadIdx.x * IT;
-    int prev = i0 > 0 && i0 - 1 < n ? __ldcg(Os + i0 - 1) : 0;
+    int prev = nprev;
     int os[IT], z[IT];
+#pragma unroll
+    for (int k = 0; k < IT; ++k) os[k] = nos[k];
+    if (t + 1 < tb1) {
+      const int j0 = i0 + TL;
+      nprev = j0 - 1 < n ? __ldcg(Os + j0 - 1) : 0;
+#pragma unroll
+      for (int k = 0; k < IT; ++k) nos[k] = (j0 + k < n) ? __ldcg(Os + j0 + k) : nprev;
+    }
     int loc = 0;
 #pragma unroll
     for (int k = 0; k < IT; ++k) {
-      os[k] = (i0 + k < n) ? __ldcg(Os + i0 + k) : prev;
       z[k] = (i0 + k < n) && (os[k] == (k == 0 ? prev : os[k - 1]));
       loc += z[k];
     }
@@ -534,10 +564,14 @@ k_systematic_coop(const double* __restrict__ lw, int n, StepStats* st, const dou
   const int TR = (R + TL - 1) / TL;
   const int rb0 = (int)(((long long)b * TR) / G), rb1 = (int)(((long long)(b + 1) * TR) / G);
   int mloc = 0;
-  for (int t = rb0; t < rb1; ++t) {
-    const int r0 = t * TL + threadIdx.x * IT;
+  for (int t = rb0; t < rb1; t += 4) {  // four tiles' loads in flight
 #pragma unroll
-    for (int k = 0; k < IT; ++k) if (r0 + k < R) mloc = max(mloc, __ldcg(marks + r0 + k));
+    for (int u = 0; u < 4; ++u) {
+      const int r0 = (t + u) * TL + threadIdx.x * IT;
+#pragma unroll
+      for (int k = 0; k < IT; ++k)
+        if (t + u < rb1 && r0 + k < R) mloc = max(mloc, __ldcg(marks + r0 + k));
+    }
   }
   const int bmax = block_max_int(mloc);
   if (threadIdx.x == 0) block_m[b] = bmax;
@@ -545,21 +579,38 @@ k_systematic_coop(const double* __restrict__ lw, int n, StepStats* st, const dou
   int mcarry = 0;
   for (int j = threadIdx.x; j < b; j += blockDim.x) mcarry = max(mcarry, __ldcg(block_m + j));
   mcarry = block_max_int(mcarry);
+  int nm[IT], nsl[IT];
+  if (rb0 < rb1) {
+    const int q0 = rb0 * TL + threadIdx.x * IT;
+#pragma unroll
+    for (int k = 0; k < IT; ++k) {
+      nm[k] = (q0 + k < R) ? __ldcg(marks + q0 + k) : 0;
+      nsl[k] = (q0 + k < R) ? __ldcg(slot + q0 + k) : 0;
+    }
+  }
   for (int t = rb0; t < rb1; ++t) {
     const int r0 = t * TL + threadIdx.x * IT;
-    int m[IT];
+    int m[IT], sl[IT];
     int run = 0;
 #pragma unroll
     for (int k = 0; k < IT; ++k) {
-      m[k] = (r0 + k < R) ? __ldcg(marks + r0 + k) : 0;
+      m[k] = nm[k];
+      sl[k] = nsl[k];
       run = max(run, m[k]);
+    }
+    if (t + 1 < rb1) {
+#pragma unroll
+      for (int k = 0; k < IT; ++k) {
+        nm[k] = (r0 + TL + k < R) ? __ldcg(marks + r0 + TL + k) : 0;
+        nsl[k] = (r0 + TL + k < R) ? __ldcg(slot + r0 + TL + k) : 0;
+      }
     }
     int tmax;
     int ex = max(mcarry, block_exclusive_scan_max_int(run, &tmax));
 #pragma unroll
     for (int k = 0; k < IT; ++k) {
       ex = max(ex, m[k]);
-      if (r0 + k < R) as[__ldcg(slot + r0 + k)] = ex - 1;
+      if (r0 + k < R) as[sl[k]] = ex - 1;
     }
     mcarry = max(mcarry, tmax);
   }
