@@ -322,7 +322,7 @@ int bpf_create(const bpf_model_desc* model, const bpf_config* config, bpf_handle
   }
   // the resampler's tile shape for this N, tuned once per size class (the
   // shapes compute the same ancestors, so only the speed depends on it)
-  if (config->resampler == BPF_RESAMPLER_SYSTEMATIC && bpf::autotuned_shape(h->n) < 0) {
+  if (config->resampler == BPF_RESAMPLER_SYSTEMATIC && bpf::autotuned_shape(h->n) == -1) {
     int best = -1;
     if (bpf::autotune_systematic(h->n, h->stream, &best, nullptr) != BPF_OK) cudaGetLastError();
   }

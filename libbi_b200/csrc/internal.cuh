@@ -240,7 +240,8 @@ int launch_resample(const ResampleArgs& a, ResampleScratch& s, cudaStream_t st);
 // time every tile shape of the one-launch systematic resampler for n
 // particles and keep the fastest for n's size class on this device
 int autotune_systematic(int n, cudaStream_t st, int* best, double* us);
-// the kept shape for n's size class, -1 when none was tuned
+// the kept shape for n's size class, -1 when none was tuned, -2 when no
+// shape holds n particles in one wave
 int autotuned_shape(int n);
 
 int launch_gather(const int* as, const void* X, void* Y, int n, int d, int ld, int esz,

@@ -1244,7 +1244,8 @@ static const CoopShape kCoopShapes[BPF_RESAMPLE_SHAPES] = {
 };
 
 // process-wide autotuned shape per device and size class (ceil log2 n);
-// -1: not tuned (the default shape 0 is used)
+// -1: not tuned, -2: no shape fits in one wave (the default shape 0, or
+// the multi-tile kernel, is used for both)
 static std::mutex g_tune_mu;
 static int g_tuned[16][32];
 static bool g_tuned_init = false;
@@ -1337,7 +1338,7 @@ static int launch_systematic_coop(const ResampleArgs& a, ResampleScratch& s, int
   // one tile per block: the pinned shape, else the autotuned one, else the
   // default; then any other shape that fits
   int first = a.shape >= 0 && a.shape < BPF_RESAMPLE_SHAPES ? a.shape : tuned_shape(dev, n);
-  if (first < 0) first = 0;
+  if (first < 0) first = 0;  // untuned, or nothing fits (the loop below then falls through)
   int rc = launch_coop1_shape(first, a, s, Os_out, sms, st);
   for (int k = 0; rc == BPF_E_INVALID && k < BPF_RESAMPLE_SHAPES; ++k)
     if (k != first) rc = launch_coop1_shape(k, a, s, Os_out, sms, st);
@@ -1380,6 +1381,17 @@ static int launch_systematic_coop(const ResampleArgs& a, ResampleScratch& s, int
   return BPF_OK;
 }
 
+// seeded synthetic log-weights N(0, 2^2), the bench's distribution
+__global__ void k_synthetic_lw(double* lw, int n) {
+  const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  if (i >= n) return;
+  const bpf_u32x4 r = bpf_draw(0x5eedull, (uint32_t)i, 0u, 0u, BPF_RNG_DATA);
+  double z0, z1;
+  bpf_normal_pair_d(r.v[0], r.v[1], &z0, &z1);
+  lw[i] = 2.0 * z0;
+  if (i + 1 < n) lw[i + 1] = 2.0 * z1;
+}
+
 int autotune_systematic(int n, cudaStream_t st, int* best, double* us) {
   if (n <= 0 || !best) return BPF_E_INVALID;
   *best = -1;
@@ -1393,14 +1405,15 @@ int autotune_systematic(int n, cudaStream_t st, int* best, double* us) {
   BPF_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   BPF_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
   if (!coop) return BPF_E_INVALID;
-  // seeded synthetic log-weights N(0, 2^2), the bench's distribution
-  std::vector<double> h((size_t)n);
-  for (int i = 0; i < n; i += 2) {
-    const bpf_u32x4 r = bpf_draw(0x5eedull, (uint32_t)i, 0u, 0u, BPF_RNG_DATA);
-    double z0, z1;
-    bpf_normal_pair_d(r.v[0], r.v[1], &z0, &z1);
-    h[i] = 2.0 * z0;
-    if (i + 1 < n) h[i + 1] = 2.0 * z1;
+  // nothing to time when no shape holds n particles in one wave
+  bool any = false;
+  for (int k = 0; k < BPF_RESAMPLE_SHAPES; ++k) {
+    const int tile = kCoopShapes[k].nt * kCoopShapes[k].it;
+    any |= (n + tile - 1) / tile <= sms * shape_per_sm(k, fill_smem(n, kMaxCoarseCoop));
+  }
+  if (!any) {
+    set_tuned_shape(dev, n, -2);
+    return BPF_E_INVALID;
   }
   ResampleScratch s;
   double* lw = nullptr;
@@ -1411,8 +1424,10 @@ int autotune_systematic(int n, cudaStream_t st, int* best, double* us) {
               cudaMalloc((void**)&as, (size_t)n * sizeof(int)) != cudaSuccess))
     rc = BPF_E_NOMEM;
   if (!rc && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)) rc = BPF_E_CUDA;
-  if (!rc && cudaMemcpyAsync(lw, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, st) != cudaSuccess)
-    rc = BPF_E_CUDA;
+  if (!rc) {
+    k_synthetic_lw<<<(n / 2 + 256) / 256, 256, 0, st>>>(lw, n);
+    if (cudaGetLastError() != cudaSuccess) rc = BPF_E_CUDA;
+  }
   if (!rc) rc = launch_lw_reduce(lw, n, s, st);  // the maximum the kernels read
   ResampleArgs a{};
   a.kind = BPF_RESAMPLER_SYSTEMATIC;
