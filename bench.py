@@ -698,12 +698,16 @@ def main():
     torch.cuda.synchronize()
     with ClockSampler(gpu_id) as clk:
         wall0 = time.perf_counter()
+        # an NVTX range around the timed steps, so that a profiler can select
+        # exactly these launches (ncu --nvtx --nvtx-include "bench_timed_steps/")
+        torch.cuda.nvtx.range_push("bench_timed_steps")
         for i in range(args.steps):
             kk = next_k()
             flush.zero_()
             starts[i].record()
             pf.step_device((kk - 1) * DT, kk * DT, y_dev[kk - 1], sync=False)
             ends[i].record()
+        torch.cuda.nvtx.range_pop()
         torch.cuda.synchronize()
         wall = time.perf_counter() - wall0
     if dist:
