@@ -442,9 +442,13 @@ int launch_batch_resample(const double* lw, int* as, const BatchFilter* filt, co
   return BPF_OK;
 }
 
+// The limit is a property of the kernel, shared by every batch: it is raised
+// to what the largest allowed filter needs (a smaller batch created later
+// must not lower it under a larger one), once per device.
 int configure_batch_resample(int max_n) {
-  BPF_TRY(cudaFuncSetAttribute(k_batch_resample, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)batch_resample_smem(max_n)));
+  if (max_n > BPF_BATCH_MAX_PARTICLES) return BPF_E_INVALID;
+  static unsigned configured = 0;
+  BPF_TRY(set_dyn_smem_once(k_batch_resample, (int)batch_resample_smem(BPF_BATCH_MAX_PARTICLES), configured));
   return BPF_OK;
 }
 

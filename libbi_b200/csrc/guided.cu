@@ -336,12 +336,8 @@ __global__ void __launch_bounds__(kGTile * TILES, TILES == 1 ? 3 : 2) k_guided_f
 
 template <int TILES, bool BATCH>
 int launch_fused(const GuidedKernelArgs& ka, int blocks, cudaStream_t st) {
-  static bool configured = false;
-  if (!configured) {
-    BPF_TRY(cudaFuncSetAttribute(k_guided_fused<40, TILES, BATCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 guided_smem<TILES>()));
-    configured = true;
-  }
+  static unsigned configured = 0;
+  BPF_TRY(set_dyn_smem_once(k_guided_fused<40, TILES, BATCH>, guided_smem<TILES>(), configured));
   k_guided_fused<40, TILES, BATCH><<<blocks, kGTile * TILES, guided_smem<TILES>(), st>>>(ka);
   BPF_TRY(cudaGetLastError());
   return BPF_OK;

@@ -247,6 +247,21 @@ int autotuned_shape(int n);
 int launch_gather(const int* as, const void* X, void* Y, int n, int d, int ld, int esz,
                   const int* gate, cudaStream_t st);
 
+// Raise a kernel's dynamic shared-memory limit once per device (the
+// attribute is per device; a process may drive several GPUs).  `done` is
+// the caller's static bitmask of configured devices.
+template <class K>
+inline cudaError_t set_dyn_smem_once(K kernel, int bytes, unsigned& done) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const unsigned bit = 1u << (dev & 31);
+  if (done & bit) return cudaSuccess;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) done |= bit;
+  return e;
+}
+
 // Models
 struct ModelArgs {
   int kind, dim, precision, integrator;

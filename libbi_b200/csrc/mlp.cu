@@ -214,11 +214,8 @@ static int launch_dense_bn(const DenseArgs& g, cudaStream_t st) {
   const size_t staging = (size_t)(128 + BN) * kTcKC * 2;
   const size_t tmem_cap = 233472 / (512 / NCOLS + 1) + 1024;
   const size_t smem = staging > tmem_cap ? staging : tmem_cap;
-  static bool configured = false;
-  if (!configured) {
-    BPF_TRY(cudaFuncSetAttribute(k_dense_tc<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    configured = true;
-  }
+  static unsigned configured = 0;
+  BPF_TRY(set_dyn_smem_once(k_dense_tc<BN>, (int)smem, configured));
   const dim3 grid((unsigned)((g.M + 127) / 128), (unsigned)g.ksplit);
   k_dense_tc<BN><<<grid, 128, smem, st>>>(g);
   BPF_TRY(cudaGetLastError());
