@@ -82,3 +82,26 @@ def test_python_api_refuses_without_gpu():
 
     with pytest.raises(RuntimeError, match="no CPU fallback"):
         BootstrapPF(ModelL96(), 1024)
+
+
+def build_cpp_client(outdir):
+    """Compile tests/cpp/filter_client.cpp against include/libbi_b200.hpp and
+    the built library; returns the executable's path."""
+    import pathlib
+    import subprocess
+
+    root = pathlib.Path(__file__).resolve().parents[1]
+    lib = root / "libbi_b200" / "_lib"
+    exe = pathlib.Path(outdir) / "filter_client"
+    subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-Wextra", "-Werror", f"-I{root / 'include'}",
+                    str(root / "tests" / "cpp" / "filter_client.cpp"), f"-L{lib}", "-lbi_b200",
+                    f"-Wl,-rpath,{lib}", "-o", str(exe)], check=True)
+    return exe
+
+
+def test_cpp_interface_compiles(tmp_path):
+    """The header-only C++ interface and a client in the shape of LibBi's
+    filter client compile and link against the library (no GPU needed)."""
+    exe = build_cpp_client(tmp_path)
+    assert exe.exists()
+
