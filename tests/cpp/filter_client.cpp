@@ -66,6 +66,10 @@ int main(int argc, char** argv) {
     c.push_back(cc);
     v.push_back(vv);
   }
+  if (!in.eof()) {
+    std::fprintf(stderr, "error: unreadable observation file %s\n", argv[5]);
+    return 1;
+  }
   const Observer obs(t, c, v);
   try {
     if (kind == "l96") {

@@ -32,7 +32,7 @@ def _sparse_obs(y, dt, rng, every=1):
 def _write(path, t, c, v):
     with open(path, "w") as f:
         for a, b, x in zip(t, c, v):
-            f.write(f"{a!r} {b} {x!r}\n")
+            f.write(f"{float(a)!r} {int(b)} {float(x)!r}\n")
 
 
 def _python(model, n, seed, ess_rel, t, c, v, dt):
