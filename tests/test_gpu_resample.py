@@ -223,3 +223,73 @@ def test_autotune_picks_a_timed_shape(cuda):
     assert 0 <= best < RESAMPLE_SHAPES
     assert SHAPES[best] in us and us[SHAPES[best]] == min(us.values())
     assert len(us) >= 2 and all(v > 0 for v in us.values())
+
+
+def _harness_lw(z, P, x):
+    """The reference harness's log-weights (test_resampler_cpu.cpp.tt:120-136):
+    log N(x; 0, 1) of standard normals x shifted by 0.5 per Z step."""
+    xs = x[:P] + 0.5 * z
+    return -0.5 * xs * xs - 0.91893853320467274178
+
+
+@pytest.mark.parametrize("kind", [0, 1, 2])
+def test_resampler_harness_metrics(cuda, oracle, kind):
+    """The metrics of the reference's resampler harness
+    (test_resampler_cpu.cpp.tt:199-245): over REPS resamplings, bias^2 =
+    sum_i (mean offspring_i - P w_i)^2 and the trace of the offspring
+    variance, per Z and P.  With the same uniforms the GPU and the oracle give
+    the same offspring, so the same metrics; and the statistics behave: bias^2
+    is Monte Carlo noise of the unbiased resamplers (about tr_var / REPS),
+    systematic has the smallest variance."""
+    import torch
+    from libbi_b200 import MetropolisResampler, MultinomialResampler, SystematicResampler
+
+    reps = 120
+    x = np.random.default_rng(11).standard_normal(4096)
+    out = {}
+    for z in (0, 2, 4):
+        for P in (16, 256, 4096):
+            lw = _harness_lw(z, P, x)
+            w = np.exp(lw - lw.max())
+            ws = P * w / w.sum()
+            if kind == 2:
+                # the harness's B for a 1% bias bound at this Z
+                Z = 0.5 * z
+                EW = np.exp(-0.25 * Z * Z) / (2.0 * np.sqrt(np.pi))
+                beta = EW / (1.0 / np.sqrt(np.pi))
+                B = int(np.ceil(np.log(1e-2) / np.log(1.0 - beta)))
+            else:
+                B = 0
+            R = (SystematicResampler, MultinomialResampler, lambda max_n: MetropolisResampler(max_n=max_n, B=B))[kind](
+                max_n=P)
+            lw_d = _t(lw, torch.float64)
+            O_gpu = np.zeros((reps, P))
+            O_orc = np.zeros((reps, P))
+            for r in range(reps):
+                u = _uniforms(oracle, kind, P, B, 1000 + r)
+                a = R.ancestors(lw_d, _t(u, torch.float64), permute=False).cpu().numpy()
+                O_gpu[r] = np.bincount(a, minlength=P)
+                if kind == 0:
+                    want = oracle.systematic(lw, u[0], permute=False)[3]
+                elif kind == 1:
+                    want = oracle.multinomial(lw, u, 0)[1]
+                else:
+                    want = oracle.metropolis(lw, B, u, 0)[1]
+                O_orc[r] = np.bincount(want, minlength=P)
+            R.close()
+            metrics = []
+            for O in (O_gpu, O_orc):
+                mu, var = O.mean(0), O.var(0, ddof=1)
+                metrics.append((float(((mu - ws) ** 2).sum()), float(var.sum())))
+            assert metrics[0] == metrics[1], (z, P, metrics)
+            bias2, tr_var = metrics[0]
+            out[(z, P)] = (bias2, tr_var)
+            if kind in (0, 1):  # unbiased: E[bias^2] = tr_var / reps
+                assert bias2 <= 3.0 * tr_var / reps + 1e-9, (z, P, bias2, tr_var)
+    if kind == 0:
+        # systematic resampling's trace variance stays below multinomial's (P (1 - sum w^2) at most)
+        for (z, P), (_, tv) in out.items():
+            lw = _harness_lw(z, P, x)
+            w = np.exp(lw - lw.max())
+            w /= w.sum()
+            assert tv <= P * (1.0 - (w * w).sum()) + 1e-9, (z, P, tv)
