@@ -103,3 +103,39 @@ def test_batch_rejects_bad_sizes(cuda):
         BatchedBootstrapPF([ModelL96(dim=40)], [32769])
     with pytest.raises(BpfError):
         BatchedBootstrapPF([ModelL96(dim=40)], [0])
+
+
+def test_c3_shape_batch_matches_sampled_single_filters(cuda, oracle):
+    """The batched configuration at its full shape: 256 Lorenz-96 filters,
+    N log-uniform in [512, 32768] rounded to 32 (about 1.9 M particles),
+    F_i ~ U(6, 10), systematic and multinomial alternating; a spread of the
+    filters (smallest, largest and others) against single filters with the
+    same settings, bit for bit over a short run."""
+    from libbi_b200 import BatchedBootstrapPF, ModelL96
+
+    rng = np.random.default_rng(3)
+    nf = 256
+    Fs = rng.uniform(6.0, 10.0, nf)
+    ns = np.floor(np.exp(rng.uniform(np.log(512), np.log(32768), nf))).astype(int)
+    ns = [int(v) for v in np.clip((ns + 31) // 32 * 32, 512, 32768)]
+    models = [ModelL96(dim=40, F=float(F)) for F in Fs]
+    res = ["systematic" if f % 2 == 0 else "multinomial" for f in range(nf)]
+    seeds = [1000 + f for f in range(nf)]
+    T, dt = 6, 0.05
+    y = np.stack([oracle.simulate(m.desc(), 300 + f, T, 0.0, dt)[0] for f, m in enumerate(models)], axis=1)
+    batch = BatchedBootstrapPF(models, ns, res, seeds, ess_rel=0.5)
+    ll, inc, ess, st = batch.filter(y, 0.0, dt)
+    assert (st == 0).all()
+    x, lw, _, offs = batch.state()
+    pick = sorted({int(np.argmin(ns)), int(np.argmax(ns)), 0, 1, 127, 255})
+    models_p = [models[f] for f in pick]
+    singles = _singles(models_p, [ns[f] for f in pick], [res[f] for f in pick], [seeds[f] for f in pick], 0.5, 0,
+                       y[:, pick], dt)
+    x, lw = x.cpu().numpy(), lw.cpu().numpy()
+    for j, f in enumerate(pick):
+        sll, sinc, sess, sx, slw = singles[j]
+        np.testing.assert_array_equal(inc[:, f], sinc)
+        np.testing.assert_array_equal(ess[:, f], sess)
+        np.testing.assert_array_equal(x[:, offs[f]:offs[f] + ns[f]], sx)
+        np.testing.assert_array_equal(lw[offs[f]:offs[f] + ns[f]], slw)
+    batch.close()

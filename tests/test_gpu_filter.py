@@ -65,6 +65,29 @@ def test_filter_matches_oracle(cuda, oracle, resampler, B, which):
     np.testing.assert_allclose(lw.cpu().numpy(), want["lw"], rtol=1e-12)
 
 
+def test_pz_config_c1_matches_oracle(cuda, oracle):
+    """The PZ configuration at its own sizes: N = 4096, FP64, RK4(3),
+    systematic resampling at every step (essRel = 1), T = 100 daily
+    observations from a seeded model run; every increment, the ESS, the
+    log-likelihood and the final state against the oracle's FP64 filter."""
+    from libbi_b200 import ModelPZ
+
+    model, n, T, dt = ModelPZ(), 4096, 100, 1.0
+    desc = model.desc()
+    y, _ = oracle.simulate(desc, 1, T, 0.0, dt)
+    pf = _mk(model, n, "systematic", 1.0, seed=2)
+    ll, inc, ess = pf.filter(y, 0.0, dt)
+    want = oracle.filter(desc, pf._cfg, y, T, 0.0, dt)
+    assert want["rc"] == 0
+    assert want["resampled"].sum() >= T - 1
+    np.testing.assert_allclose(inc, want["inc"], rtol=1e-10, atol=1e-9)
+    np.testing.assert_allclose(ess, want["ess"], rtol=1e-9)
+    np.testing.assert_allclose(ll, want["ll"], rtol=1e-10)
+    x, _, _ = pf.state()
+    np.testing.assert_array_equal(x.cpu().numpy()[:, :n], want["x"][:, :n])
+    pf.close()
+
+
 def test_step_api_and_snapshot(cuda, oracle):
     from libbi_b200 import ModelL96
 
