@@ -668,7 +668,9 @@ def main():
     model = configs.L96_D40_N65536["model"]
     y_host = synthetic_observations(model)
     y_dev = torch.as_tensor(y_host, device="cuda")
-    pf = BootstrapPF(model, N_PARTICLES, resampler="systematic", ess_rel=ESS_REL, seed=SEED + 1000 * rank)
+    from libbi_b200.replicas import max_over_ranks, replica_seed, whole_job_rate
+
+    pf = BootstrapPF(model, N_PARTICLES, resampler="systematic", ess_rel=ESS_REL, seed=replica_seed(SEED, rank))
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
     k = 0
 
@@ -716,11 +718,8 @@ def main():
     total_ms = sum(step_ms)
     res_ms, tr_ms, nst = pf.timing_read(reset=True)
     pf.timing(False)
-    if dist:
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = N_PARTICLES * args.steps * world / (total_ms / 1e3)
+    total_ms = max_over_ranks(total_ms, dist, "cuda")
+    value = whole_job_rate(N_PARTICLES * args.steps, world, total_ms / 1e3)
 
     # end to end through the public API: pinned host observation copied in,
     # step statistics read back, every step
@@ -735,11 +734,8 @@ def main():
         t0 = time.perf_counter()
         pf.step((kk - 1) * DT, kk * DT, y_np[kk - 1])
         e2e_s += time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = N_PARTICLES * args.steps * world / e2e_s
+    e2e_s = max_over_ranks(e2e_s, dist, "cuda")
+    e2e = whole_job_rate(N_PARTICLES * args.steps, world, e2e_s)
 
     hbm, how, sm_max = peaks()
     clocks = clk.summary()
