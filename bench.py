@@ -727,13 +727,15 @@ def main():
     y_pin.copy_(torch.as_tensor(y_host))
     y_np = y_pin.numpy()
     e2e_s = 0.0
+    resampled = 0
     for i in range(args.steps):
         kk = next_k()
         flush.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        pf.step((kk - 1) * DT, kk * DT, y_np[kk - 1])
+        r = pf.step((kk - 1) * DT, kk * DT, y_np[kk - 1])
         e2e_s += time.perf_counter() - t0
+        resampled += int(r.resampled)
     e2e_s = max_over_ranks(e2e_s, dist, "cuda")
     e2e = whole_job_rate(N_PARTICLES * args.steps, world, e2e_s)
 
@@ -753,7 +755,7 @@ def main():
                    "rk4_h": 0.01, "resampler": "systematic", "ess_rel": ESS_REL,
                    "parallelism": f"replicas{world}" if world > 1 else "single",
                    "l2": "flushed before every timed step (256 MiB write)",
-                   "resampled_steps_timed": None},
+                   "resampled_steps_end_to_end": f"{resampled} of {args.steps}"},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": DIM * 4,
                 "d2h_bytes_per_step": 80, "timer": "host wall clock around bpf_step"},
         "gpu_launches": LAUNCHES_PER_STEP * args.steps,
