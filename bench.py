@@ -280,6 +280,7 @@ def batched_filters(runs=5):
     models, ns, res, seeds, T = batched_workload()
     y = batched_truth(models, T)
     b = BatchedBootstrapPF(models, ns, res, seeds, ess_rel=ESS_REL)
+    rs_threads, rs_us = b.resample_threads()  # autotuned at create
     b.filter(y, 0.0, DT)  # capture the graph
     b.timing(True)
     b.timing_read(reset=True)
@@ -298,6 +299,8 @@ def batched_filters(runs=5):
     bps = TRANSITION_BYTES_PER_PARTICLE * total * T / dev_s / 1e9
     return {
         "workload": "l96_d40_256filters_n512_32768_loguniform_t100",
+        "autotuned_resample_threads": rs_threads,
+        "resample_tuning_us": {str(k): v for k, v in rs_us.items()},
         "filters": len(ns), "total_particles": total, "T": T, "runs": runs,
         "particle_steps_per_s": total * T / dev_s,
         "ms_per_filter_run": dev_s * 1e3,

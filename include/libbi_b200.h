@@ -338,6 +338,14 @@ int bpf_batch_set_theta(bpf_batch* b, const double* theta);
 /* Replace every filter's seed (host, nfilters), e.g. fresh randomness for
  * each filter run of a PMMH iteration; takes effect from the next init. */
 int bpf_batch_set_seeds(bpf_batch* b, const uint64_t* seeds);
+/* Threads per filter CTA of the batched resampler (256, 512 or 1024; no
+ * counterpart in the reference).  bpf_batch_create autotunes it: the three
+ * counts are timed on synthetic log-weights laid out as the batch's filters
+ * and the fastest is kept; every count computes the same ancestors.
+ * threads != 0 pins a count (a captured filter run is recaptured); current
+ * and tuned_us[3] (the tuning medians for 256, 512, 1024; may be NULL)
+ * report the state. */
+int bpf_batch_resample_threads(bpf_batch* b, int threads, int* current, double* tuned_us);
 /* One BootstrapPF::step of every filter (see bpf_step); y_device: device
  * observations, nfilters x (dim for L96, 1 for PZ), filter-major, in the
  * model precision, or NULL for an unobserved step.  Does not synchronise. */

@@ -45,7 +45,7 @@ EXPORTS = (
     "bpf_resampler_timing_enable", "bpf_resampler_timing_read", "bpf_autotune_resampler", "bpf_resampler_set_shape",
     "bpf_batch_create", "bpf_batch_destroy", "bpf_batch_init", "bpf_batch_set_theta", "bpf_batch_step_device",
     "bpf_batch_stats", "bpf_batch_state_ptrs", "bpf_filter_batch", "bpf_batch_timing_enable",
-    "bpf_batch_timing_read", "bpf_batch_set_seeds",
+    "bpf_batch_timing_read", "bpf_batch_set_seeds", "bpf_batch_resample_threads",
     "bpf_pmmh_create", "bpf_pmmh_destroy", "bpf_pmmh_run", "bpf_pmmh_state", "bpf_dense_bf16",
     "bpf_proposal_create", "bpf_proposal_destroy", "bpf_proposal_set_data", "bpf_proposal_train",
     "bpf_proposal_loss_grad", "bpf_proposal_params", "bpf_proposal_set_params", "bpf_set_proposal",
@@ -164,6 +164,7 @@ def _declare(L):
                                      c_void_p]),
         "bpf_batch_timing_enable": (c_int, [H, c_int]),
         "bpf_batch_set_seeds": (c_int, [H, c_void_p]),
+        "bpf_batch_resample_threads": (c_int, [H, c_int, POINTER(c_int), c_void_p]),
         "bpf_pmmh_create": (c_int, [POINTER(ModelDesc), POINTER(PmmhConfig), c_int, c_double, c_double, c_void_p,
                                     c_void_p, c_void_p, POINTER(H)]),
         "bpf_pmmh_destroy": (c_int, [H]),

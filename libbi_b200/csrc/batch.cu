@@ -23,6 +23,7 @@
 #include "model_body.cuh"
 #include "resample_common.cuh"
 #include "batch.cuh"
+#include "../../include/bpf_math.h"
 #include "proposal.cuh"
 
 #include <algorithm>
@@ -234,7 +235,8 @@ inline size_t batch_resample_smem(int max_n) {
 //   multinomial  MultinomialResamplerHost::ancestors (MultinomialResamplerHost.hpp:29-65)
 //   Metropolis   MetropolisResamplerHost::ancestors (MetropolisResamplerHost.hpp:32-62)
 // computed exactly as the single-filter kernels compute them.
-__global__ void __launch_bounds__(kBatchThreads, 1)
+template <int NT>
+__global__ void __launch_bounds__(NT, 1)
 k_batch_resample(const double* __restrict__ lw, int* __restrict__ as, const BatchFilter* __restrict__ filt,
                  const int* __restrict__ order, StepStats* stats, double* lu_buf, int* os_buf, int step) {
   extern __shared__ __align__(16) unsigned char s_raw[];
@@ -247,9 +249,9 @@ k_batch_resample(const double* __restrict__ lw, int* __restrict__ as, const Batc
   int* asf = as + fd.off;
   int* osf = os_buf + fd.off;
   double* s_coarse = reinterpret_cast<double*>(s_raw);
-  int* marks = reinterpret_cast<int*>(s_raw + kBatchThreads * sizeof(double));
+  int* marks = reinterpret_cast<int*>(s_raw + kBatchThreads * sizeof(double));  // layout for the largest NT
   unsigned char* flags = reinterpret_cast<unsigned char*>(marks + n);
-  const int IT = (n + kBatchThreads - 1) / kBatchThreads;
+  const int IT = (n + NT - 1) / NT;
   const int i0 = min(n, threadIdx.x * IT);
   const int i1 = min(n, i0 + IT);
   const double mx = st->mx;
@@ -264,7 +266,7 @@ k_batch_resample(const double* __restrict__ lw, int* __restrict__ as, const Batc
       if (mult) vacc = u128_add(vacc, spacing_to_fixed(multinomial_spacing(nullptr, i, n, fd.seed, step)));
     }
     u128 Wtot;
-    const u128 texcl = block_exclusive_scan_u128_nt<kBatchThreads>(acc, &Wtot);
+    const u128 texcl = block_exclusive_scan_u128_nt<NT>(acc, &Wtot);
     const double W = u128_to_weight(Wtot);
     // SystematicResampler::cumulativeOffspring throws
     // ParticleFilterDegeneratedException unless W > 0
@@ -284,7 +286,7 @@ k_batch_resample(const double* __restrict__ lw, int* __restrict__ as, const Batc
       }
     } else {
       u128 Vtot;
-      const u128 vexcl = block_exclusive_scan_u128_nt<kBatchThreads>(vacc, &Vtot);
+      const u128 vexcl = block_exclusive_scan_u128_nt<NT>(vacc, &Vtot);
       const double lW = log(W);
       double* luf = lu_buf + fd.off;
       // lu_s = lW + lMax_s, lMax_s = -(sum of the spacings of slots >= s)
@@ -318,7 +320,7 @@ k_batch_resample(const double* __restrict__ lw, int* __restrict__ as, const Batc
     int loc = 0;
     for (int i = i0; i < i1; ++i) loc += __ldcg(osf + i);
     int tot;
-    int run = block_exclusive_scan_int_nt<kBatchThreads>(loc, &tot);
+    int run = block_exclusive_scan_int_nt<NT>(loc, &tot);
     for (int i = i0; i < i1; ++i) { run += __ldcg(osf + i); osf[i] = run; }
   }
   __syncthreads();
@@ -335,8 +337,8 @@ k_batch_resample(const double* __restrict__ lw, int* __restrict__ as, const Batc
     }
   }
   int ztot;
-  const int zexcl = block_exclusive_scan_int_nt<kBatchThreads>(zl, &ztot);
-  for (int r = threadIdx.x; r < ztot; r += kBatchThreads) marks[r] = 0;
+  const int zexcl = block_exclusive_scan_int_nt<NT>(zl, &ztot);
+  for (int r = threadIdx.x; r < ztot; r += NT) marks[r] = 0;
   __syncthreads();
   {
     int prev = before0, Z = zexcl;
@@ -358,12 +360,12 @@ k_batch_resample(const double* __restrict__ lw, int* __restrict__ as, const Batc
   // inclusive max-scan of marks[0..ztot): rank r -> 1 + the ancestor whose
   // extra copies cover r
   {
-    const int CH = (ztot + kBatchThreads - 1) / kBatchThreads;
+    const int CH = (ztot + NT - 1) / NT;
     const int r0 = min(ztot, threadIdx.x * CH), r1 = min(ztot, r0 + CH);
     int m = 0;
     for (int r = r0; r < r1; ++r) m = max(m, marks[r]);
     int mtot;
-    const int mexcl = block_exclusive_max_int_nt<kBatchThreads>(m, &mtot);
+    const int mexcl = block_exclusive_max_int_nt<NT>(m, &mtot);
     int run = mexcl;
     for (int r = r0; r < r1; ++r) { run = max(run, marks[r]); marks[r] = run; }
   }
@@ -434,10 +436,20 @@ int launch_batch_transition(const ModelArgs& m, const void* x_in, void* x_out, i
   return BPF_OK;
 }
 
+// threads per filter CTA of the batched resampler: 256, 512 or 1024 (the
+// in-CTA arithmetic is exact, so the count changes the speed only)
 int launch_batch_resample(const double* lw, int* as, const BatchFilter* filt, const int* order, int nf,
-                          int max_n, StepStats* stats, double* lu_buf, int* os_buf, int step, cudaStream_t st) {
+                          int max_n, StepStats* stats, double* lu_buf, int* os_buf, int step, cudaStream_t st,
+                          int threads) {
   const size_t smem = batch_resample_smem(max_n);
-  k_batch_resample<<<nf, kBatchThreads, smem, st>>>(lw, as, filt, order, stats, lu_buf, os_buf, step);
+  switch (threads) {
+    case 256: k_batch_resample<256><<<nf, 256, smem, st>>>(lw, as, filt, order, stats, lu_buf, os_buf, step); break;
+    case 512: k_batch_resample<512><<<nf, 512, smem, st>>>(lw, as, filt, order, stats, lu_buf, os_buf, step); break;
+    case 1024:
+      k_batch_resample<1024><<<nf, 1024, smem, st>>>(lw, as, filt, order, stats, lu_buf, os_buf, step);
+      break;
+    default: return BPF_E_INVALID;
+  }
   BPF_TRY(cudaGetLastError());
   return BPF_OK;
 }
@@ -447,9 +459,109 @@ int launch_batch_resample(const double* lw, int* as, const BatchFilter* filt, co
 // must not lower it under a larger one), once per device.
 int configure_batch_resample(int max_n) {
   if (max_n > BPF_BATCH_MAX_PARTICLES) return BPF_E_INVALID;
-  static unsigned configured = 0;
-  BPF_TRY(set_dyn_smem_once(k_batch_resample, (int)batch_resample_smem(BPF_BATCH_MAX_PARTICLES), configured));
+  static unsigned c256 = 0, c512 = 0, c1024 = 0;
+  const int smem = (int)batch_resample_smem(BPF_BATCH_MAX_PARTICLES);
+  BPF_TRY(set_dyn_smem_once(k_batch_resample<256>, smem, c256));
+  BPF_TRY(set_dyn_smem_once(k_batch_resample<512>, smem, c512));
+  BPF_TRY(set_dyn_smem_once(k_batch_resample<1024>, smem, c1024));
   return BPF_OK;
+}
+
+// synthetic log-weights 2 N(0, 1) over the whole buffer, for the autotuner
+__global__ void k_batch_synthetic_lw(double* lw, int ld) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ld) return;
+  const bpf_u32x4 r = bpf_draw(0x7a11ull, (uint32_t)i, 0u, 0u, BPF_RNG_DATA);
+  double z0, z1;
+  bpf_normal_pair_d(r.v[0], r.v[1], &z0, &z1);
+  lw[i] = 2.0 * z0;
+}
+
+// statistics that open every filter's resampling gate, with each filter's
+// maximum log-weight
+__global__ void k_batch_tune_stats(const double* lw, const BatchFilter* filt, StepStats* st, int nf) {
+  const int f = blockIdx.x;
+  if (f >= nf) return;
+  const BatchFilter fd = filt[f];
+  double m = -INFINITY;
+  for (int i = threadIdx.x; i < fd.n; i += blockDim.x) m = fmax(m, lw[fd.off + i]);
+  m = warp_max(m);
+  __shared__ double s_m[32];
+  if ((threadIdx.x & 31) == 0) s_m[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, s_m[w]);
+    m = fmax(m, s_m[0]);
+    StepStats z{};
+    z.mx = m;
+    z.resample = 1;
+    z.status = BPF_OK;
+    z.n = fd.n;
+    st[f] = z;
+  }
+}
+
+// Time the three thread counts on synthetic log-weights laid out as the
+// batch's filters (scratch buffers: the batch's own state is untouched) and
+// return the fastest; the medians go to us[3] (256, 512, 1024).
+int tune_batch_resample(const BatchFilter* filt, const int* order, int nf, int max_n, int ld, cudaStream_t st,
+                        int* best, double* us) {
+  *best = kBatchThreads;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  BPF_TRY(cudaStreamIsCapturing(st, &cs));
+  if (cs != cudaStreamCaptureStatusNone) return BPF_OK;  // no timing inside a capture: keep the default
+  double* lw = nullptr;
+  double* lu = nullptr;
+  int *as = nullptr, *os = nullptr;
+  StepStats* stats = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = BPF_OK;
+  auto A = [&](void** p, size_t b) {
+    if (!rc && cudaMalloc(p, b) != cudaSuccess) rc = BPF_E_NOMEM;
+  };
+  A((void**)&lw, (size_t)ld * sizeof(double));
+  A((void**)&lu, (size_t)ld * sizeof(double));
+  A((void**)&as, (size_t)ld * sizeof(int));
+  A((void**)&os, (size_t)ld * sizeof(int));
+  A((void**)&stats, (size_t)nf * sizeof(StepStats));
+  if (!rc && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)) rc = BPF_E_CUDA;
+  if (!rc) {
+    k_batch_synthetic_lw<<<(ld + 255) / 256, 256, 0, st>>>(lw, ld);
+    k_batch_tune_stats<<<nf, 256, 0, st>>>(lw, filt, stats, nf);
+    if (cudaGetLastError() != cudaSuccess) rc = BPF_E_CUDA;
+  }
+  const int counts[3] = {256, 512, 1024};
+  double best_us = 0.0;
+  for (int c = 0; !rc && c < 3; ++c) {
+    constexpr int kReps = 7;
+    float t[kReps];
+    for (int r = -2; r < kReps && !rc; ++r) {  // two untimed runs first
+      if (r >= 0 && cudaEventRecord(e0, st) != cudaSuccess) rc = BPF_E_CUDA;
+      if (!rc) rc = launch_batch_resample(lw, as, filt, order, nf, max_n, stats, lu, os, 1, st, counts[c]);
+      if (r >= 0 && !rc &&
+          (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+           cudaEventElapsedTime(&t[r], e0, e1) != cudaSuccess))
+        rc = BPF_E_CUDA;
+    }
+    if (rc) break;
+    std::sort(t, t + kReps);
+    const double med = 1e3 * t[kReps / 2];
+    if (us) us[c] = med;
+    if (c == 0 || med < best_us) {
+      best_us = med;
+      *best = counts[c];
+    }
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  void* ps[] = {lw, lu, as, os, stats};
+  for (void* q : ps)
+    if (q) cudaFree(q);
+  if (rc) {
+    cudaGetLastError();
+    *best = kBatchThreads;
+  }
+  return rc;
 }
 
 }  // namespace bpf
@@ -461,6 +573,8 @@ struct bpf_batch {
   bpf::ModelArgs model;
   int nf = 0, ld = 0, blocks = 0, max_n = 0, esz = 0, nobs = 0, bs = 0;
   int tiles = 0;               // 128-particle tiles over all filters (guided step)
+  int rs_threads = 1024;       // threads per filter CTA of the resampler (autotuned at create)
+  double rs_us[3] = {0.0, 0.0, 0.0};  // its tuning medians for 256, 512, 1024 threads
   bpf_proposal* prop = nullptr;  // learned proposal (bpf_batch_set_proposal), owned by the caller
   int* tile2f = nullptr;       // tile -> filter, allocated with the proposal
   double ess_rel = 0.0;
@@ -566,7 +680,7 @@ int batch_enqueue_init(bpf_batch* b) {
 int batch_enqueue_step(bpf_batch* b, double t1, double t2, const void* y_dev, double* hist, int k) {
   const int step = b->step + 1;
   int rc = bpf::launch_batch_resample(b->lw, b->as, b->filt_dev, b->order, b->nf, b->max_n, b->stats, b->lu,
-                                      b->os, step, b->stream);
+                                      b->os, step, b->stream, b->rs_threads);
   if (rc) return rc;
   if (b->prop && y_dev) {
     // guided step: the learned proposal, trained for one interval
@@ -727,6 +841,8 @@ int bpf_batch_create(const bpf_model_desc* model, int nfilters, const bpf_batch_
               cudaStreamSynchronize(b->stream) != cudaSuccess))
     rc = BPF_E_CUDA;
   if (!rc) rc = bpf::configure_batch_resample(b->max_n);
+  if (!rc) rc = bpf::tune_batch_resample(b->filt_dev, b->order, b->nf, b->max_n, b->ld, b->stream, &b->rs_threads,
+                                         b->rs_us);
   if (!rc) rc = batch_upload_params(b);
   if (!rc) rc = batch_enqueue_init(b);
   if (rc) {
@@ -801,6 +917,22 @@ int bpf_batch_set_proposal(bpf_batch* b, bpf_proposal* p) {
     b->graph = nullptr;
   }
   b->prop = p;
+  return BPF_OK;
+}
+
+int bpf_batch_resample_threads(bpf_batch* b, int threads, int* current, double* tuned_us) {
+  if (!b) return BPF_E_INVALID;
+  if (threads != 0) {
+    if (threads != 256 && threads != 512 && threads != 1024) return BPF_E_INVALID;
+    if (threads != b->rs_threads && b->graph) {
+      cudaGraphExecDestroy(b->graph);  // the captured steps launch the other count
+      b->graph = nullptr;
+    }
+    b->rs_threads = threads;
+  }
+  if (current) *current = b->rs_threads;
+  if (tuned_us)
+    for (int c = 0; c < 3; ++c) tuned_us[c] = b->rs_us[c];
   return BPF_OK;
 }
 

@@ -497,6 +497,15 @@ class BatchedBootstrapPF:
                                 st.ctypes.data_as(ctypes.c_void_p))
         return ll, ess, st
 
+    def resample_threads(self, threads: int = 0):
+        """Threads per filter CTA of the resampler: pin 256, 512 or 1024, or
+        0 to keep the autotuned count; returns (current, {count: tuning us})."""
+        cur = ctypes.c_int()
+        us = np.zeros(3)
+        N.check(N.lib().bpf_batch_resample_threads(self._h, int(threads), ctypes.byref(cur),
+                                                   us.ctypes.data_as(ctypes.c_void_p)), "bpf_batch_resample_threads")
+        return cur.value, {256: us[0], 512: us[1], 1024: us[2]}
+
     def set_proposal(self, proposal):
         """Attach a LearnedProposal to every filter (or None to detach):
         observed steps then run the guided step for the whole batch."""

@@ -139,3 +139,26 @@ def test_c3_shape_batch_matches_sampled_single_filters(cuda, oracle):
         np.testing.assert_array_equal(x[:, offs[f]:offs[f] + ns[f]], sx)
         np.testing.assert_array_equal(lw[offs[f]:offs[f] + ns[f]], slw)
     batch.close()
+
+
+def test_every_resampler_thread_count_gives_the_single_filters(cuda, oracle):
+    """The batched resampler's CTA size is autotuned at create (256, 512 or
+    1024 threads per filter); each count must give the single filters'
+    numbers bit for bit."""
+    from libbi_b200 import BatchedBootstrapPF, ModelL96
+
+    ns = [512, 700, 4096, 32768, 1, 3000]
+    res = ["systematic", "multinomial", "metropolis", "systematic", "multinomial", "metropolis"]
+    seeds = [2000 + f for f in range(len(ns))]
+    models = [ModelL96(dim=40, F=F) for F in (6.0, 7.0, 8.0, 9.0, 10.0, 8.5)]
+    T, dt = 8, 0.05
+    y = np.stack([oracle.simulate(m.desc(), 80 + f, T, 0.0, dt)[0] for f, m in enumerate(models)], axis=1)
+    singles = _singles(models, ns, res, seeds, 0.5, 5, y, dt)
+    batch = BatchedBootstrapPF(models, ns, res, seeds, ess_rel=0.5, metropolis_steps=5)
+    tuned, us = batch.resample_threads()
+    assert tuned in (256, 512, 1024) and all(v > 0 for v in us.values())
+    for threads in (256, 512, 1024):
+        assert batch.resample_threads(threads)[0] == threads
+        _check(batch, singles, y, dt, ns)
+    batch.close()
+
