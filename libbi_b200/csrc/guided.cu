@@ -29,6 +29,13 @@
 // particles.  TILES = 2 (256 threads, 96 KB, 256 TMEM columns, at most 128
 // registers) puts 512 particles on an SM, so 65536 particles run in one wave
 // on 148 SMs; TILES = 1 spreads small filters over more SMs.
+//
+// The same kernel runs the guided step of a batch of filters (BATCH = true,
+// TILES = 1): CTA c takes tile c of the batch's 128-particle tiles, finds its
+// filter through the tile -> filter table, and uses that filter's columns,
+// seed, constants, statistics and partial slots; since a filter of a batch
+// has at most 32768 particles, its single-filter step would also use one
+// tile per CTA, so the batched step reproduces it bit for bit.
 #include "internal.cuh"
 #include "reduce.cuh"
 #include "model_body.cuh"
