@@ -530,15 +530,16 @@ def guided_vs_bootstrap(y_host, seeds=64, n_guided=(4096, 16384, 65536),
         lls = np.array(lls)
         return {"n": n, "ll_mean": float(lls.mean()), "ll_sd": float(lls.std(ddof=1)), "ms_per_run": ms / seeds}
 
-    def run_batched(n, use_prop):
+    def run_batched(n, use_prop, T=None):
         # the same seeds as the single filters, one filter per seed in one
         # batch (the same numbers, bit for bit); device time of the captured
-        # run divided by the filters
+        # run divided by the filters; T: the first T observations only
         b = BatchedBootstrapPF([model] * seeds, [n] * seeds, "systematic", [10_000 + s for s in range(seeds)],
                                ess_rel=ESS_REL)
         if use_prop:
             b.set_proposal(prop)
-        yb = np.ascontiguousarray(np.repeat(np.asarray(y_host, np.float32)[:, None, :], seeds, axis=1))
+        yy = np.asarray(y_host if T is None else y_host[:T], np.float32)
+        yb = np.ascontiguousarray(np.repeat(yy[:, None, :], seeds, axis=1))
         b.filter(yb, 0.0, DT)  # capture
         b.timing(True)
         b.timing_read(reset=True)
@@ -552,6 +553,11 @@ def guided_vs_bootstrap(y_host, seeds=64, n_guided=(4096, 16384, 65536),
     guided = [run(n, True) for n in n_guided]
     guided_b = [run_batched(n, True) for n in n_guided_batched]
     boot_b = [run_batched(n, False) for n in n_boot_batched]
+    # the first 10 observations, where the filters still track (deviation
+    # falling with N): the guided and bootstrap deviations at equal N
+    short = {"T": 10,
+             "bootstrap": [run_batched(n, False, 10) for n in (4096, 16384, 32768)],
+             "guided": [run_batched(n, True, 10) for n in (1024, 4096, 16384)]}
     prop.close()
     # the bootstrap filter's best measured cost per particle-step (single or
     # batched): the conservative price of a bootstrap filter of any size
@@ -589,6 +595,7 @@ def guided_vs_bootstrap(y_host, seeds=64, n_guided=(4096, 16384, 65536),
         "bootstrap": boot,
         "guided": guided,
         "batched": {"guided": guided_b, "bootstrap": boot_b},
+        "short_horizon_batched": short,
         "bootstrap_sd_exponent_in_n": slope,
         "best": {"equal_sd": {"guided_n": best["n"], "gpu_time_ratio_bootstrap_over_guided":
                               best["gpu_time_ratio_bootstrap_over_guided_at_equal_sd"]},
