@@ -29,4 +29,12 @@ __device__ __forceinline__ void batch_record(const StepStats* st, double* hist, 
   }
 }
 
+// the batched resampler (batch.cu): one CTA of `threads` threads per filter
+int launch_batch_resample(const double* lw, int* as, const BatchFilter* filt, const int* order, int nf,
+                          int max_n, StepStats* stats, double* lu_buf, int* os_buf, int step, cudaStream_t st,
+                          int threads);
+int configure_batch_resample(int max_n);
+int tune_batch_resample(const BatchFilter* filt, const int* order, int nf, int max_n, int ld, cudaStream_t st,
+                        int* best, double* us);
+
 }  // namespace bpf

@@ -9,9 +9,12 @@
 // kernels on the handle's stream; nothing returns to the host unless asked.
 #include "internal.cuh"
 #include "proposal.cuh"
+#include "batch.cuh"
 #include "resample_common.cuh"
 
 #include <cstdio>
+#include <map>
+#include <mutex>
 #include <cstring>
 #include <new>
 #include <cmath>
@@ -44,6 +47,12 @@ struct bpf_handle {
   bpf_proposal* prop = nullptr;
   // pinned host copy of the step statistics (read back after every step)
   bpf::StepStats* host_stats = nullptr;
+  // filters of at most kOneCtaMaxParticles resample in one CTA: the
+  // batched resampler on a one-filter table (same ancestors, no grid
+  // barriers); its CTA size is autotuned at create
+  bpf::BatchFilter* one_filt = nullptr;
+  int* one_order = nullptr;
+  int one_threads = 1024;
   // path cache (bpf_path_cache): pc_len states of dim x ld in the model
   // precision (slot 0 the state the recording started from, slot t the state
   // after t more steps) and the ancestors of each recorded step
@@ -174,7 +183,9 @@ int enqueue_step(bpf_handle* h, double t1, double t2, const void* y_dev, uint64_
   ra.Os_out = nullptr;
   ra.gate = gate;
   ra.max_known = true;
-  int rc = bpf::launch_resample(ra, h->rs, h->stream);
+  int rc = h->one_filt ? bpf::launch_batch_resample(h->lw, h->as, h->one_filt, h->one_order, 1, h->n, h->rs.stats,
+                                                    h->rs.lu, h->rs.Os, k, h->stream, h->one_threads)
+                       : bpf::launch_resample(ra, h->rs, h->stream);
   if (rc) return rc;
   if (y_host && y_dev) BPF_TRY(cudaMemcpyAsync(const_cast<void*>(y_dev), y_host, y_bytes, cudaMemcpyHostToDevice,
                                                h->stream));
@@ -261,6 +272,35 @@ __global__ void k_reset_lw(double* lw, int n, const bpf::StepStats* st) {
 
 }  // namespace
 
+// Largest filter resampled by one CTA.  On B200 (L96, d=40, a resampling
+// at every step) one CTA takes 9.6 / 12.3 / 16.4 us per systematic
+// resampling at N = 256 / 1024 / 4096 against 13.7 / 14.3 / 17.3 us for the
+// grid-wide kernels (Metropolis at 4096: 14.3 against 29.8 us), but 62 us
+// at 16384 against 17.8: past a few thousand particles the work needs more
+// than one SM.
+constexpr int kOneCtaMaxParticles = 4096;
+
+// CTA size of the one-CTA resampler, timed once per process for each
+// resampler and particle count (the sizes compute the same ancestors)
+static int one_cta_threads(bpf_handle* h, int resampler) {
+  static std::mutex mu;
+  static std::map<std::pair<int, int>, int> tuned;
+  const std::pair<int, int> key(resampler, h->n);
+  {
+    std::lock_guard<std::mutex> g(mu);
+    auto it = tuned.find(key);
+    if (it != tuned.end()) {
+      h->one_threads = it->second;
+      return BPF_OK;
+    }
+  }
+  int rc = bpf::tune_batch_resample(h->one_filt, h->one_order, 1, h->n, h->ld, h->stream, &h->one_threads, nullptr);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> g(mu);
+  tuned[key] = h->one_threads;
+  return BPF_OK;
+}
+
 extern "C" {
 
 const char* bpf_version(void) { return "libbi_b200 0.1 (sm_100a)"; }
@@ -320,9 +360,31 @@ int bpf_create(const bpf_model_desc* model, const bpf_config* config, bpf_handle
     cudaGetLastError();
     h->host_stats = nullptr;  // read back through pageable memory instead
   }
-  // the resampler's tile shape for this N, tuned once per size class (the
-  // shapes compute the same ancestors, so only the speed depends on it)
-  if (config->resampler == BPF_RESAMPLER_SYSTEMATIC && bpf::autotuned_shape(h->n) == -1) {
+  if (h->n <= kOneCtaMaxParticles) {
+    // one CTA resamples the whole filter (the resampler reads n, off,
+    // resampler, B and seed of the table entry)
+    bpf::BatchFilter f{};
+    f.n = h->n;
+    f.off = 0;
+    f.resampler = config->resampler;
+    f.B = config->metropolis_steps;
+    f.seed = config->seed;
+    const int zero = 0;
+    if (cudaMalloc((void**)&h->one_filt, sizeof(f)) != cudaSuccess ||
+        cudaMalloc((void**)&h->one_order, sizeof(int)) != cudaSuccess ||
+        cudaMemcpy(h->one_filt, &f, sizeof(f), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(h->one_order, &zero, sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess) {
+      cudaGetLastError();
+      bpf_destroy(h);
+      return BPF_E_NOMEM;
+    }
+    rc = bpf::configure_batch_resample(h->n);
+    if (!rc) rc = one_cta_threads(h, config->resampler);
+    if (rc) { bpf_destroy(h); return rc; }
+  } else if (config->resampler == BPF_RESAMPLER_SYSTEMATIC && bpf::autotuned_shape(h->n) == -1) {
+    // the one-launch cooperative resampler's tile shape for this N, tuned
+    // once per size class (the shapes compute the same ancestors, so only
+    // the speed depends on it)
     int best = -1;
     if (bpf::autotune_systematic(h->n, h->stream, &best, nullptr) != BPF_OK) cudaGetLastError();
   }
@@ -343,7 +405,7 @@ int bpf_destroy(bpf_handle* h) {
   if (h->hist) cudaFree(h->hist);
   for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
   if (h->host_stats) cudaFreeHost(h->host_stats);
-  void* g[] = {h->pc_x, h->pc_a};
+  void* g[] = {h->pc_x, h->pc_a, h->one_filt, h->one_order};
   for (void* p : g)
     if (p) cudaFree(p);
   bpf::scratch_free(h->rs);
