@@ -172,13 +172,15 @@ def cpu_baseline(y, seconds: float = 12.0):
                       f"observation steps (incl. initial draw), {threads} OpenMP threads, {el:.1f} s"}
 
 
-def large_n_kernels(sizes=(1 << 22, 1 << 24), reps=5):
+def large_n_kernels(sizes=(1 << 22, 1 << 24, 1 << 26), reps=5):
     """The memory-bound kernels at working sets beyond L2: log-weight
     reduction (ess_reduce), permuted systematic resampling and the ancestor
     gather (40 FP32 components).  Device time of the kernels from CUDA events
     (for the resampler calls, the events the resampler records around its own
-    kernels), L2 flushed before every repetition; achieved GB/s counts
-    algorithmic bytes:
+    kernels).  Before every repetition L2 is flushed: 256 MiB written, then
+    another 256 MiB read, so that L2 holds none of the kernel's inputs and
+    no dirty lines whose write-back the timed kernel would pay for.  Achieved
+    GB/s counts algorithmic bytes:
     reduce 8 B, resample 8 + 4 B (log-weight in, ancestor out), gather
     2*40*4 + 4 B per particle."""
     import torch
@@ -186,7 +188,8 @@ def large_n_kernels(sizes=(1 << 22, 1 << 24), reps=5):
 
     hbm, _, _ = peaks()
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
-    out = {}
+    flush_read = torch.ones(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    out = {"l2": "flushed before every repetition: 256 MiB written, then another 256 MiB read"}
     for n in sizes:
         g = torch.Generator(device="cuda")
         g.manual_seed(n)
@@ -205,6 +208,7 @@ def large_n_kernels(sizes=(1 << 22, 1 << 24), reps=5):
             ts = []
             for _ in range(reps):
                 flush.zero_()
+                flush_read.sum()
                 s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 R.timing_read(reset=True)
                 s0.record()
