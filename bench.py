@@ -587,6 +587,28 @@ def guided_vs_bootstrap(y_host, seeds=64, n_guided=(4096, 16384, 65536),
     ln_sd = np.log([max(b["ll_sd"], 1e-300) for b in boot])
     slope = float(np.polyfit(ln_n, ln_sd, 1)[0]) if len(boot) > 1 else None
     best = max(guided, key=lambda gd: gd["gpu_time_ratio_bootstrap_over_guided_at_equal_sd"] or 0.0)
+    # the workload's own comparison: guided N = 4096 against bootstrap
+    # N = n_ref, deviation over the same seeds (standard error of a normal
+    # sample's deviation: sd / sqrt(2 (seeds - 1)))
+    g1 = next((gd for gd in guided if gd["n"] == 4096), None)
+    gb = next((gd for gd in guided_b if gd["n"] == 4096), None)
+    named = None
+    if g1 is not None:
+        se = lambda sd: sd / np.sqrt(2.0 * (seeds - 1))
+        named = {"guided_n": 4096, "bootstrap_n": n_ref,
+                 "guided_ll_sd": g1["ll_sd"], "guided_ll_sd_se": se(g1["ll_sd"]),
+                 "bootstrap_ll_sd": ref["ll_sd"], "bootstrap_ll_sd_se": se(ref["ll_sd"]),
+                 "sd_ratio_guided_over_bootstrap": g1["ll_sd"] / ref["ll_sd"],
+                 "guided_ms_per_run_single": g1["ms_per_run"],
+                 "guided_ms_per_run_batched": gb["ms_per_run"] if gb else None,
+                 "bootstrap_ms_per_run": ref["ms_per_run"],
+                 "gpu_time_ratio_bootstrap_over_guided_single": ref["ms_per_run"] / g1["ms_per_run"],
+                 "gpu_time_ratio_bootstrap_over_guided_batched":
+                     ref["ms_per_run"] / gb["ms_per_run"] if gb else None,
+                 # near 0: the deviation does not fall with N, so matching
+                 # it says little about the estimator (the mean
+                 # log-likelihood comparisons do)
+                 "bootstrap_sd_exponent_in_n": slope}
     best_m = max(guided, key=lambda gd: gd["gpu_time_ratio_bootstrap_over_guided_at_equal_mean_ll"])
     best_b = max(guided_b, key=lambda gd: gd["gpu_time_ratio_bootstrap_over_guided_at_equal_mean_ll"])
     return {
@@ -600,6 +622,7 @@ def guided_vs_bootstrap(y_host, seeds=64, n_guided=(4096, 16384, 65536),
         "guided": guided,
         "batched": {"guided": guided_b, "bootstrap": boot_b},
         "short_horizon_batched": short,
+        "named_comparison": named,
         "bootstrap_sd_exponent_in_n": slope,
         "best": {"equal_sd": {"guided_n": best["n"], "gpu_time_ratio_bootstrap_over_guided":
                               best["gpu_time_ratio_bootstrap_over_guided_at_equal_sd"]},
