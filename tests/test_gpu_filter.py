@@ -42,12 +42,16 @@ def test_first_step_bit_identical(cuda, oracle, which):
 
 
 @pytest.mark.parametrize("resampler,B", [("systematic", 0), ("multinomial", 0), ("metropolis", 8)])
-@pytest.mark.parametrize("which", ["l96", "pz"])
+@pytest.mark.parametrize("which", ["l96", "l96_grid", "pz"])
 def test_filter_matches_oracle(cuda, oracle, resampler, B, which):
+    """Filters of up to 4096 particles resample in one CTA; l96_grid (8192
+    particles) takes the grid-wide resamplers."""
     from libbi_b200 import ModelL96, ModelPZ
 
     if which == "l96":
         model, n, T, dt, ess_rel = ModelL96(dim=40), 2048, 12, 0.05, 0.5
+    elif which == "l96_grid":
+        model, n, T, dt, ess_rel = ModelL96(dim=40), 8192, 8, 0.05, 0.5
     else:
         model, n, T, dt, ess_rel = ModelPZ(), 1024, 15, 1.0, 1.0
     desc = model.desc()
