@@ -12,6 +12,7 @@ from .filter import (BootstrapPF, ModelL96, ModelPZ, Resampler, SystematicResamp
 from .sampler import MarginalMH, Prior, smc2  # noqa: F401
 from .proposal import LearnedProposal  # noqa: F401
 from .schedule import Observer, Schedule, ScheduleElement  # noqa: F401
+from .replicas import sharded_batch_filter  # noqa: F401
 from . import configs  # noqa: F401
 
 __all__ = ["BootstrapPF", "ModelL96", "ModelPZ", "Resampler", "SystematicResampler", "MultinomialResampler",
