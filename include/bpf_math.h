@@ -203,21 +203,13 @@ BPF_HD float bpf_expf(float x) {
   return (p * bpf_bitsf((uint32_t)(ki + 64 + 127) << 23)) * bpf_bitsf((uint32_t)(-64 + 127) << 23);
 }
 
-BPF_HD float bpf_logf(float x) {
+/* log of a positive, finite, normal x times 2^e0: the body of bpf_logf
+ * without its special cases */
+BPF_HD float bpf_logf_normal(float x, int e0) {
   const float ln2_hi = 0.693145751953125f;
   const float ln2_lo = 1.428606765330187e-06f;
-  if (x != x) return x;
-  if (x < 0.0f) return NAN;
-  if (x == 0.0f) return -INFINITY;
-  if (x == INFINITY) return x;
-  int e = 0;
-  uint32_t u = bpf_fbits(x);
-  if ((u >> 23) == 0) {
-    x = x * 16777216.0f; /* 2^24 */
-    u = bpf_fbits(x);
-    e = -24;
-  }
-  e += (int)(u >> 23) - 127;
+  const uint32_t u = bpf_fbits(x);
+  int e = e0 + (int)(u >> 23) - 127;
   float m = bpf_bitsf((u & 0x007FFFFFu) | 0x3F800000u);
   if (m > 1.41421354f) { m = m * 0.5f; e += 1; }
   float s = (m - 1.0f) / (m + 1.0f);
@@ -233,17 +225,17 @@ BPF_HD float bpf_logf(float x) {
   return BPF_MATH_FMAF(ef, ln2_hi, BPF_MATH_FMAF(ef, ln2_lo, lm));
 }
 
-BPF_HD void bpf_sincospif(float x, float* sp, float* cp) {
-  float q;
-  int qi;
-  if (fabsf(x) < 1048576.0f) {  /* q = rint(2x) by the rounding constant; quadrant = low bits */
-    const float t = 2.0f * x + 12582912.0f;
-    q = t - 12582912.0f;
-    qi = (int)(bpf_fbits(t) & 3u);
-  } else {
-    q = rintf(2.0f * x);
-    qi = ((int)fmodf(q, 4.0f) + 4) & 3;
-  }
+BPF_HD float bpf_logf(float x) {
+  if (x != x) return x;
+  if (x < 0.0f) return NAN;
+  if (x == 0.0f) return -INFINITY;
+  if (x == INFINITY) return x;
+  if ((bpf_fbits(x) >> 23) == 0) return bpf_logf_normal(x * 16777216.0f, -24); /* subnormal: x 2^24 */
+  return bpf_logf_normal(x, 0);
+}
+
+/* sin(pi x), cos(pi x) from q = rint(2x) and its quadrant qi */
+BPF_HD void bpf_sincospif_q(float x, float q, int qi, float* sp, float* cp) {
   float r = BPF_MATH_FMAF(-0.5f, q, x);
   float r2 = r * r;
   float s = 0.08214588463306427f;                /* pi^9/9! */
@@ -266,15 +258,34 @@ BPF_HD void bpf_sincospif(float x, float* sp, float* cp) {
   }
 }
 
+/* bpf_sincospif for |x| < 2^20: q = rint(2x) by the rounding constant, the
+ * quadrant in its low bits */
+BPF_HD void bpf_sincospif_small(float x, float* sp, float* cp) {
+  const float t = 2.0f * x + 12582912.0f;
+  bpf_sincospif_q(x, t - 12582912.0f, (int)(bpf_fbits(t) & 3u), sp, cp);
+}
+
+BPF_HD void bpf_sincospif(float x, float* sp, float* cp) {
+  if (fabsf(x) < 1048576.0f) {
+    bpf_sincospif_small(x, sp, cp);
+    return;
+  }
+  const float q = rintf(2.0f * x);
+  bpf_sincospif_q(x, q, ((int)fmodf(q, 4.0f) + 4) & 3, sp, cp);
+}
+
 /* --------------------------------------------------- standard normals */
 
 /* Box-Muller pair from two 32-bit words: u_a, u_b are the 23-bit uniforms of
  * bpf_u01f; z0 = sqrt(-2 log u_a) cos(2 pi u_b), z1 = ... sin(2 pi u_b). */
 BPF_HD void bpf_normal_pair_f(uint32_t a, uint32_t b, float* z0, float* z1) {
+  /* u_a, u_b lie in [2^-24, 1 - 2^-24]: u_a is positive, finite and normal
+   * and |2 u_b| < 2^20, so the special cases of bpf_logf and
+   * bpf_sincospif cannot arise and their cores give the same values */
   float ua = bpf_u01f(a), ub = bpf_u01f(b);
-  float r = sqrtf(-2.0f * bpf_logf(ua));
+  float r = sqrtf(-2.0f * bpf_logf_normal(ua, 0));
   float s, c;
-  bpf_sincospif(2.0f * ub, &s, &c);
+  bpf_sincospif_small(2.0f * ub, &s, &c);
   *z0 = r * c;
   *z1 = r * s;
 }

@@ -119,11 +119,10 @@ __device__ __forceinline__ void l96_rk4(T (&x0)[D], double t1d, double t2d, T F,
 // says whether component i is observed (the observation Mask of
 // SparseStaticLogDensity, share/src/bi/state/Mask.hpp).  Returns l plus the
 // observation terms.
-template <class T, int D>
-__device__ __forceinline__ double l96_noise_obs(const T (&sx)[D][kL96Block], T* __restrict__ x_out, size_t ld,
-                                                int p_out, const T* __restrict__ y, uint64_t seed, uint32_t prng,
-                                                int step, const L96Params& prm, double l,
-                                                uint64_t mask = ~0ull) {
+template <class T, int D, bool MASKED>
+__device__ __forceinline__ double l96_noise_obs_impl(const T (&sx)[D][kL96Block], T* __restrict__ x_out, size_t ld,
+                                                     int p_out, const T* __restrict__ y, uint64_t seed, uint32_t prng,
+                                                     int step, const L96Params& prm, double l, uint64_t mask) {
   const T se = (T)prm.sigma_eta;
   const T sy = (T)prm.sigma_y, isy = (T)prm.inv_sigma_y;
   const T c2 = (T)prm.c_half_log_2pi, ls = (T)prm.log_sigma_y;
@@ -139,7 +138,7 @@ __device__ __forceinline__ double l96_noise_obs(const T (&sx)[D][kL96Block], T* 
       if (i < D) {
         const T xi = Prec<T>::add_(sx[i][threadIdx.x], Prec<T>::mul_(se, z[j]));
         x_out[(size_t)i * ld + p_out] = xi;
-        if (y && ((mask >> i) & 1ull)) {
+        if (y && (!MASKED || ((mask >> i) & 1ull))) {
           T dz = __ldg(y + i) - xi;
           dz = isy != (T)0 ? dz * isy : dz / sy;
           T term = Prec<T>::fma_((T)-0.5, dz * dz, -c2) - ls;
@@ -149,6 +148,19 @@ __device__ __forceinline__ double l96_noise_obs(const T (&sx)[D][kL96Block], T* 
     }
   }
   return l;
+}
+
+// Every component observed (the usual case): the loop without the per
+// component test of the mask.
+template <class T, int D>
+__device__ __forceinline__ double l96_noise_obs(const T (&sx)[D][kL96Block], T* __restrict__ x_out, size_t ld,
+                                                int p_out, const T* __restrict__ y, uint64_t seed, uint32_t prng,
+                                                int step, const L96Params& prm, double l,
+                                                uint64_t mask = ~0ull) {
+  constexpr uint64_t all = D >= 64 ? ~0ull : (1ull << D) - 1ull;
+  if ((mask & all) == all)
+    return l96_noise_obs_impl<T, D, false>(sx, x_out, ld, p_out, y, seed, prng, step, prm, l, mask);
+  return l96_noise_obs_impl<T, D, true>(sx, x_out, ld, p_out, y, seed, prng, step, prm, l, mask);
 }
 
 // ---------------------------------------------------------------------------
