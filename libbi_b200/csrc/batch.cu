@@ -530,22 +530,26 @@ int tune_batch_resample(const BatchFilter* filt, const int* order, int nf, int m
     k_batch_tune_stats<<<nf, 256, 0, st>>>(lw, filt, stats, nf);
     if (cudaGetLastError() != cudaSuccess) rc = BPF_E_CUDA;
   }
+  // the sizes take turns, round after round, so that a drift of clocks or
+  // caches during the tuning reaches every size alike; each size's median
+  // decides
   const int counts[3] = {256, 512, 1024};
-  double best_us = 0.0;
-  for (int c = 0; !rc && c < 3; ++c) {
-    constexpr int kReps = 7;
-    float t[kReps];
-    for (int r = -2; r < kReps && !rc; ++r) {  // two untimed runs first
-      if (r >= 0 && cudaEventRecord(e0, st) != cudaSuccess) rc = BPF_E_CUDA;
-      if (!rc) rc = launch_batch_resample(lw, as, filt, order, nf, max_n, stats, lu, os, 1, st, counts[c]);
-      if (r >= 0 && !rc &&
+  constexpr int kReps = 9;
+  float t[3][kReps];
+  for (int r = -2; !rc && r < kReps; ++r) {  // two untimed rounds first
+    for (int c = 0; !rc && c < 3; ++c) {
+      if (r >= 0 && cudaEventRecord(e0, st) != cudaSuccess) { rc = BPF_E_CUDA; break; }
+      rc = launch_batch_resample(lw, as, filt, order, nf, max_n, stats, lu, os, 1, st, counts[c]);
+      if (!rc && r >= 0 &&
           (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
-           cudaEventElapsedTime(&t[r], e0, e1) != cudaSuccess))
+           cudaEventElapsedTime(&t[c][r], e0, e1) != cudaSuccess))
         rc = BPF_E_CUDA;
     }
-    if (rc) break;
-    std::sort(t, t + kReps);
-    const double med = 1e3 * t[kReps / 2];
+  }
+  double best_us = 0.0;
+  for (int c = 0; !rc && c < 3; ++c) {
+    std::sort(t[c], t[c] + kReps);
+    const double med = 1e3 * t[c][kReps / 2];
     if (us) us[c] = med;
     if (c == 0 || med < best_us) {
       best_us = med;

@@ -1439,24 +1439,30 @@ int autotune_systematic(int n, cudaStream_t st, int* best, double* us) {
   a.as = as;
   a.max_known = true;
   a.shape = -1;
+  // the shapes take turns, round after round, so that a drift of clocks or
+  // caches during the tuning reaches every shape alike; each shape's median
+  // decides
+  constexpr int kReps = 15;
+  float t[BPF_RESAMPLE_SHAPES][kReps];
+  bool fits[BPF_RESAMPLE_SHAPES];
+  for (int k = 0; k < BPF_RESAMPLE_SHAPES; ++k) fits[k] = true;
+  for (int r = -2; !rc && r < kReps; ++r) {  // two untimed rounds first
+    for (int k = 0; !rc && k < BPF_RESAMPLE_SHAPES; ++k) {
+      if (!fits[k]) continue;
+      if (r >= 0 && cudaEventRecord(e0, st) != cudaSuccess) { rc = BPF_E_CUDA; break; }
+      const int krc = launch_coop1_shape(k, a, s, nullptr, sms, st);
+      if (krc == BPF_E_INVALID) { fits[k] = false; continue; }  // this shape does not fit in one wave
+      if (krc) { rc = krc; break; }
+      if (r >= 0 && (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                     cudaEventElapsedTime(&t[k][r], e0, e1) != cudaSuccess))
+        rc = BPF_E_CUDA;
+    }
+  }
   double best_us = 0.0;
   for (int k = 0; !rc && k < BPF_RESAMPLE_SHAPES; ++k) {
-    constexpr int kReps = 9;
-    float t[kReps];
-    int krc = BPF_OK;
-    for (int r = -2; r < kReps && !krc; ++r) {  // two untimed runs first
-      if (r >= 0 && cudaEventRecord(e0, st) != cudaSuccess) krc = BPF_E_CUDA;
-      if (!krc) krc = launch_coop1_shape(k, a, s, nullptr, sms, st);
-      if (r >= 0 && !krc) {
-        if (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
-            cudaEventElapsedTime(&t[r], e0, e1) != cudaSuccess)
-          krc = BPF_E_CUDA;
-      }
-    }
-    if (krc == BPF_E_INVALID) continue;  // this shape does not fit in one wave
-    if (krc) { rc = krc; break; }
-    std::sort(t, t + kReps);
-    const double med = 1e3 * t[kReps / 2];
+    if (!fits[k]) continue;
+    std::sort(t[k], t[k] + kReps);
+    const double med = 1e3 * t[k][kReps / 2];
     if (us) us[k] = med;
     if (*best < 0 || med < best_us) { *best = k; best_us = med; }
   }
