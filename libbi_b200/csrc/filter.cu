@@ -160,8 +160,11 @@ int path_record(bpf_handle* h, bool after_step) {
 }
 
 // y_host, y_bytes: when given, the observation is copied from host memory
-// into y_dev after the resampling launch (which does not read it), so the
-// copy overlaps the resampling
+// into y_dev on the step's stream, after the resampling launch, so that the
+// host issues the copy while the resampler runs; in stream order the copy
+// itself runs between the resampler and the transition (a second stream for
+// it, joined by events, measured slower end to end: the events cost more
+// than the 160-byte copy)
 int enqueue_step(bpf_handle* h, double t1, double t2, const void* y_dev, uint64_t mask = ~0ull,
                  const void* y_host = nullptr, size_t y_bytes = 0) {
   const int k = h->step + 1;
