@@ -398,17 +398,68 @@ __device__ __forceinline__ int block_sum_int_from_global(const int* a, int count
   return tot;
 }
 
+// Warp-wide inclusive scans (32 lanes).
+__device__ __forceinline__ u128 warp_inclusive_u128(u128 v) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const u128 o = shfl_up_u128(v, d);
+    if (lane >= d) v = u128_add(v, o);
+  }
+  return v;
+}
+
+__device__ __forceinline__ int warp_inclusive_int(int v) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const int o = __shfl_up_sync(0xffffffffu, v, d);
+    if (lane >= d) v += o;
+  }
+  return v;
+}
+
+__device__ __forceinline__ int warp_inclusive_max_int(int v) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const int o = __shfl_up_sync(0xffffffffu, v, d);
+    if (lane >= d) v = max(v, o);
+  }
+  return v;
+}
+
+// The segments [s0, s1) of warp `warp` when segments [b0, b1) are shared by
+// the block's warps in contiguous runs.
+__device__ __forceinline__ void warp_segments(int b0, int b1, int warp, int nwarps, int* s0, int* s1) {
+  const long long c = b1 - b0;
+  *s0 = b0 + (int)(c * warp / nwarps);
+  *s1 = b0 + (int)(c * (warp + 1) / nwarps);
+}
+
+// Several segments per block (n beyond one tile per resident block).  The
+// particles are cut into segments of 32 x IT; block b owns a contiguous run
+// of segments and each of its warps a contiguous run of those, so every
+// scan inside a phase is a warp scan carried from segment to segment, and
+// the block synchronises only at the phase boundaries.  Block prefixes come
+// from the G block totals published at each grid barrier, warp prefixes
+// from the block's per-warp totals in shared memory.
 template <int IT>
 __global__ void __launch_bounds__(kBlock)
 k_systematic_coop(const double* __restrict__ lw, int n, StepStats* st, const double* a_in, uint64_t seed, int step,
                   int* Os, int* as, int* marks, int* slot, unsigned long long* qbuf, u128* block_w, int* block_z, int* block_m,
                   unsigned* bar_counter, unsigned* bar_gen, const int* gate) {
   if (gate_closed(gate, st)) return;
-  __shared__ int s_prev_os;
+  constexpr int NW = kBlock / 32;
+  constexpr int S = 32 * IT;  // particles per segment
+  __shared__ u128 s_wsum[NW];
+  __shared__ int s_wint[NW];
   const int G = gridDim.x, b = blockIdx.x;
-  constexpr int TL = kBlock * IT;
-  const int T = (n + TL - 1) / TL;
-  const int tb0 = (int)(((long long)b * T) / G), tb1 = (int)(((long long)(b + 1) * T) / G);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int NS = (n + S - 1) / S;
+  const int sb0 = (int)(((long long)b * NS) / G), sb1 = (int)(((long long)(b + 1) * NS) / G);
+  int ws0, ws1;
+  warp_segments(sb0, sb1, warp, NW, &ws0, &ws1);
   const double mx = st->mx;
   double a;
   if (a_in) {
@@ -418,33 +469,35 @@ k_systematic_coop(const double* __restrict__ lw, int n, StepStats* st, const dou
     a = bpf_u01d(r.v[0], r.v[1]);
   }
 
-  // phase 1: exact fixed-point weight total of this block's tiles
-  // every tile loop below issues the next tile's loads before the current
-  // tile's arithmetic and block scans, so the memory latency overlaps them
-  u128 wsum = u128_zero();
-  double nv[IT];
-  if (tb0 < tb1) load_blocked_n<IT>(lw, tb0 * TL + threadIdx.x * IT, n, nv);
-  for (int t = tb0; t < tb1; ++t) {
-    const int i0 = t * TL + threadIdx.x * IT;
-    double v[IT];
+  // phase 1: exact fixed-point weights (kept for phase 2) and their totals
+  // per warp and per block
+  {
+    u128 wsum = u128_zero();
+    for (int sg = ws0; sg < ws1; ++sg) {
+      const int i0 = sg * S + lane * IT;
+      double v[IT];
+      load_blocked_n<IT>(lw, i0, n, v);
 #pragma unroll
-    for (int k = 0; k < IT; ++k) v[k] = nv[k];
-    if (t + 1 < tb1) load_blocked_n<IT>(lw, i0 + TL, n, nv);
-#pragma unroll
-    for (int k = 0; k < IT; ++k) {
-      if (i0 + k < n) {
-        u128 q; q.lo = weight_to_fixed(nanexp(__dsub_rn(v[k], mx))); q.hi = 0;
-        qbuf[i0 + k] = q.lo;  // phase 2 reads these instead of recomputing the exp
-        wsum = u128_add(wsum, q);
+      for (int k = 0; k < IT; ++k) {
+        if (i0 + k < n) {
+          u128 q; q.lo = weight_to_fixed(nanexp(__dsub_rn(v[k], mx))); q.hi = 0;
+          qbuf[i0 + k] = q.lo;
+          wsum = u128_add(wsum, q);
+        }
       }
     }
+    wsum = warp_inclusive_u128(wsum);  // lane 31: the warp's total
+    if (lane == 31) s_wsum[warp] = wsum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      u128 t = u128_zero();
+      for (int w = 0; w < NW; ++w) t = u128_add(t, s_wsum[w]);
+      block_w[b] = t;
+    }
   }
-  u128 btot;
-  block_exclusive_scan_u128(wsum, &btot);
-  if (threadIdx.x == 0) block_w[b] = btot;
   if (!grid_barrier(bar_counter, bar_gen, st)) return;
 
-  // phase 2: prefix of this block, total W, cumulative offspring, childless counts
+  // phase 2: cumulative offspring and childless counts
   const u128 prefix_b = block_sum_u128_from_global(block_w, b);
   const u128 total = block_sum_u128_from_global(block_w, G);
   const double W = u128_to_weight(total);
@@ -457,162 +510,153 @@ k_systematic_coop(const double* __restrict__ lw, int n, StepStats* st, const dou
   }
   const double nd = (double)n;
   const double yW = __ddiv_rn(1.0, W);
-  __shared__ int s_last[kBlock];
-  u128 carry = prefix_b;
-  int zeros = 0;
-  if (threadIdx.x == 0) s_prev_os = tb0 == 0 ? 0 : systematic_Os(u128_to_weight(prefix_b), W, yW, nd, a, n);
-  unsigned long long nq[IT];
-  if (tb0 < tb1) {
-    const int j0 = tb0 * TL + threadIdx.x * IT;
+  {
+    u128 carry = prefix_b;
+    for (int w = 0; w < warp; ++w) carry = u128_add(carry, s_wsum[w]);
+    // Os of the particle before the warp's first (0 before particle 0)
+    int prev_os = ws0 == 0 ? 0 : systematic_Os(u128_to_weight(carry), W, yW, nd, a, n);
+    int zeros = 0;
+    for (int sg = ws0; sg < ws1; ++sg) {
+      const int i0 = sg * S + lane * IT;
+      unsigned long long q[IT];
+      u128 loc = u128_zero();
 #pragma unroll
-    for (int k = 0; k < IT; ++k) nq[k] = (j0 + k < n) ? __ldcg(qbuf + j0 + k) : 0ull;
-  }
-  for (int t = tb0; t < tb1; ++t) {
-    const int i0 = t * TL + threadIdx.x * IT;
-    unsigned long long q[IT];
-    u128 loc = u128_zero();
-#pragma unroll
-    for (int k = 0; k < IT; ++k) {
-      q[k] = nq[k];
-      u128 qq; qq.lo = q[k]; qq.hi = 0;
-      loc = u128_add(loc, qq);
-    }
-    if (t + 1 < tb1) {
-#pragma unroll
-      for (int k = 0; k < IT; ++k) nq[k] = (i0 + TL + k < n) ? __ldcg(qbuf + i0 + TL + k) : 0ull;
-    }
-    u128 ttot;
-    u128 Q = u128_add(carry, block_exclusive_scan_u128(loc, &ttot));
-    int os[IT];
-#pragma unroll
-    for (int k = 0; k < IT; ++k) {
-      u128 qq; qq.lo = q[k]; qq.hi = 0;
-      Q = u128_add(Q, qq);
-      os[k] = systematic_Os(u128_to_weight(Q), W, yW, nd, a, n);
-    }
-    s_last[threadIdx.x] = os[IT - 1];
-    __syncthreads();
-    int prev = threadIdx.x > 0 ? s_last[threadIdx.x - 1] : s_prev_os;
-#pragma unroll
-    for (int k = 0; k < IT; ++k) {
-      if (i0 + k < n) {
-        Os[i0 + k] = os[k];
-        marks[i0 + k] = 0;
-        zeros += (os[k] == prev);
+      for (int k = 0; k < IT; ++k) {
+        q[k] = (i0 + k < n) ? __ldcg(qbuf + i0 + k) : 0ull;
+        u128 qq; qq.lo = q[k]; qq.hi = 0;
+        loc = u128_add(loc, qq);
       }
-      prev = os[k];
+      const u128 inc = warp_inclusive_u128(loc);
+      u128 Q = u128_add(carry, u128_sub(inc, loc));
+      int os[IT];
+#pragma unroll
+      for (int k = 0; k < IT; ++k) {
+        u128 qq; qq.lo = q[k]; qq.hi = 0;
+        Q = u128_add(Q, qq);
+        os[k] = systematic_Os(u128_to_weight(Q), W, yW, nd, a, n);
+      }
+      const int up = __shfl_up_sync(0xffffffffu, os[IT - 1], 1);
+      int prev = lane > 0 ? up : prev_os;
+#pragma unroll
+      for (int k = 0; k < IT; ++k) {
+        if (i0 + k < n) {
+          Os[i0 + k] = os[k];
+          marks[i0 + k] = 0;
+          zeros += (os[k] == prev);
+        }
+        prev = os[k];
+      }
+      carry = u128_add(carry, shfl_u128(inc, 31));
+      prev_os = __shfl_sync(0xffffffffu, os[IT - 1], 31);
     }
+    zeros = warp_inclusive_int(zeros);
+    __syncthreads();  // every warp has read s_wsum
+    if (lane == 31) s_wint[warp] = zeros;
     __syncthreads();
-    if (threadIdx.x == kBlock - 1) s_prev_os = os[IT - 1];
-    carry = u128_add(carry, ttot);
-    __syncthreads();
+    if (threadIdx.x == 0) {
+      int t = 0;
+      for (int w = 0; w < NW; ++w) t += s_wint[w];
+      block_z[b] = t;
+    }
   }
-  int ztot;
-  block_exclusive_scan_int(zeros, &ztot);
-  if (threadIdx.x == 0) block_z[b] = ztot;
   if (!grid_barrier(bar_counter, bar_gen, st)) return;
 
-  // phase 3: ranks of childless slots, extra-copy counts, survivors in place
-  int zcarry = block_sum_int_from_global(block_z, b);
+  // phase 3: ranks of childless slots, extra-copy marks, survivors in place
+  const int zcarry_b = block_sum_int_from_global(block_z, b);
   const int R = block_sum_int_from_global(block_z, G);
-  int nprev = 0, nos[IT];
-  if (tb0 < tb1) {
-    const int j0 = tb0 * TL + threadIdx.x * IT;
-    nprev = j0 > 0 && j0 - 1 < n ? __ldcg(Os + j0 - 1) : 0;
+  {
+    int zc = zcarry_b;
+    for (int w = 0; w < warp; ++w) zc += s_wint[w];
+    const int first = ws0 * S;
+    int prev_os = (ws0 < ws1 && first > 0) ? __ldcg(Os + first - 1) : 0;
+    for (int sg = ws0; sg < ws1; ++sg) {
+      const int i0 = sg * S + lane * IT;
+      int os[IT], z[IT];
 #pragma unroll
-    for (int k = 0; k < IT; ++k) nos[k] = (j0 + k < n) ? __ldcg(Os + j0 + k) : nprev;
-  }
-  for (int t = tb0; t < tb1; ++t) {
-    const int i0 = t * TL + threadIdx.x * IT;
-    int prev = nprev;
-    int os[IT], z[IT];
+      for (int k = 0; k < IT; ++k) os[k] = (i0 + k < n) ? __ldcg(Os + i0 + k) : 0;
+      const int up = __shfl_up_sync(0xffffffffu, os[IT - 1], 1);
+      const int before0 = lane > 0 ? up : prev_os;
+      int loc = 0;
+      {
+        int before = before0;
 #pragma unroll
-    for (int k = 0; k < IT; ++k) os[k] = nos[k];
-    if (t + 1 < tb1) {
-      const int j0 = i0 + TL;
-      nprev = j0 - 1 < n ? __ldcg(Os + j0 - 1) : 0;
-#pragma unroll
-      for (int k = 0; k < IT; ++k) nos[k] = (j0 + k < n) ? __ldcg(Os + j0 + k) : nprev;
-    }
-    int loc = 0;
-#pragma unroll
-    for (int k = 0; k < IT; ++k) {
-      z[k] = (i0 + k < n) && (os[k] == (k == 0 ? prev : os[k - 1]));
-      loc += z[k];
-    }
-    int ttot;
-    int Z = zcarry + block_exclusive_scan_int(loc, &ttot);
-#pragma unroll
-    for (int k = 0; k < IT; ++k) {
-      const int i = i0 + k;
-      const int before = (k == 0 ? prev : os[k - 1]);
-      if (i < n) {
-        // the first further copy of i (if any) has rank E_i = Os_{i-1} - i + Z_i
-        if (os[k] - before >= 2) marks[before - i + Z] = i + 1;
-        if (z[k]) slot[Z] = i;
-        else as[i] = i;
+        for (int k = 0; k < IT; ++k) {
+          z[k] = (i0 + k < n) && (os[k] == before);
+          loc += z[k];
+          before = os[k];
+        }
       }
-      Z += z[k];
+      const int inc = warp_inclusive_int(loc);
+      int Z = zc + inc - loc;
+      int before = before0;
+#pragma unroll
+      for (int k = 0; k < IT; ++k) {
+        const int i = i0 + k;
+        if (i < n) {
+          // the first further copy of i (if any) has rank E_i = Os_{i-1} - i + Z_i
+          if (os[k] - before >= 2) marks[before - i + Z] = i + 1;
+          if (z[k]) slot[Z] = i;
+          else as[i] = i;
+        }
+        Z += z[k];
+        before = os[k];
+      }
+      zc += __shfl_sync(0xffffffffu, inc, 31);
+      prev_os = __shfl_sync(0xffffffffu, os[IT - 1], 31);
     }
-    zcarry += ttot;
   }
   if (!grid_barrier(bar_counter, bar_gen, st)) return;
 
   // phase 4: the ancestor of rank r is the last a whose first further copy
-  // has rank <= r, i.e. the running maximum of the marks up to r (load
-  // balanced however the copies are distributed)
-  const int TR = (R + TL - 1) / TL;
-  const int rb0 = (int)(((long long)b * TR) / G), rb1 = (int)(((long long)(b + 1) * TR) / G);
-  int mloc = 0;
-  for (int t = rb0; t < rb1; t += 4) {  // four tiles' loads in flight
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int r0 = (t + u) * TL + threadIdx.x * IT;
+  // has rank <= r, i.e. the running maximum of the marks up to r
+  const int NR = (R + S - 1) / S;
+  const int rb0 = (int)(((long long)b * NR) / G), rb1 = (int)(((long long)(b + 1) * NR) / G);
+  int rs0, rs1;
+  warp_segments(rb0, rb1, warp, NW, &rs0, &rs1);
+  {
+    int mloc = 0;
+    for (int sg = rs0; sg < rs1; ++sg) {
+      const int r0 = sg * S + lane * IT;
 #pragma unroll
       for (int k = 0; k < IT; ++k)
-        if (t + u < rb1 && r0 + k < R) mloc = max(mloc, __ldcg(marks + r0 + k));
+        if (r0 + k < R) mloc = max(mloc, __ldcg(marks + r0 + k));
+    }
+    mloc = warp_inclusive_max_int(mloc);
+    __syncthreads();  // every warp has read s_wint
+    if (lane == 31) s_wint[warp] = mloc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int t = 0;
+      for (int w = 0; w < NW; ++w) t = max(t, s_wint[w]);
+      block_m[b] = t;
     }
   }
-  const int bmax = block_max_int(mloc);
-  if (threadIdx.x == 0) block_m[b] = bmax;
   if (!grid_barrier(bar_counter, bar_gen, st)) return;
-  int mcarry = 0;
-  for (int j = threadIdx.x; j < b; j += blockDim.x) mcarry = max(mcarry, __ldcg(block_m + j));
-  mcarry = block_max_int(mcarry);
-  int nm[IT], nsl[IT];
-  if (rb0 < rb1) {
-    const int q0 = rb0 * TL + threadIdx.x * IT;
-#pragma unroll
-    for (int k = 0; k < IT; ++k) {
-      nm[k] = (q0 + k < R) ? __ldcg(marks + q0 + k) : 0;
-      nsl[k] = (q0 + k < R) ? __ldcg(slot + q0 + k) : 0;
-    }
-  }
-  for (int t = rb0; t < rb1; ++t) {
-    const int r0 = t * TL + threadIdx.x * IT;
-    int m[IT], sl[IT];
-    int run = 0;
-#pragma unroll
-    for (int k = 0; k < IT; ++k) {
-      m[k] = nm[k];
-      sl[k] = nsl[k];
-      run = max(run, m[k]);
-    }
-    if (t + 1 < rb1) {
+  {
+    int mc = 0;
+    for (int j = threadIdx.x; j < b; j += blockDim.x) mc = max(mc, __ldcg(block_m + j));
+    mc = block_max_int(mc);
+    for (int w = 0; w < warp; ++w) mc = max(mc, s_wint[w]);
+    for (int sg = rs0; sg < rs1; ++sg) {
+      const int r0 = sg * S + lane * IT;
+      int m[IT], sl[IT];
+      int run = 0;
 #pragma unroll
       for (int k = 0; k < IT; ++k) {
-        nm[k] = (r0 + TL + k < R) ? __ldcg(marks + r0 + TL + k) : 0;
-        nsl[k] = (r0 + TL + k < R) ? __ldcg(slot + r0 + TL + k) : 0;
+        m[k] = (r0 + k < R) ? __ldcg(marks + r0 + k) : 0;
+        sl[k] = (r0 + k < R) ? __ldcg(slot + r0 + k) : 0;
+        run = max(run, m[k]);
       }
-    }
-    int tmax;
-    int ex = max(mcarry, block_exclusive_scan_max_int(run, &tmax));
+      const int inc = warp_inclusive_max_int(run);
+      const int up = __shfl_up_sync(0xffffffffu, inc, 1);
+      int ex = max(mc, lane > 0 ? up : 0);
 #pragma unroll
-    for (int k = 0; k < IT; ++k) {
-      ex = max(ex, m[k]);
-      if (r0 + k < R) as[sl[k]] = ex - 1;
+      for (int k = 0; k < IT; ++k) {
+        ex = max(ex, m[k]);
+        if (r0 + k < R) as[sl[k]] = ex - 1;
+      }
+      mc = max(mc, __shfl_sync(0xffffffffu, inc, 31));
     }
-    mcarry = max(mcarry, tmax);
   }
 }
 
