@@ -473,10 +473,16 @@ k_systematic_coop(const double* __restrict__ lw, int n, StepStats* st, const dou
   // per warp and per block
   {
     u128 wsum = u128_zero();
+    // every segment loop issues the next segment's loads before the current
+    // segment's arithmetic and scans, so the memory latency overlaps them
+    double nv[IT];
+    if (ws0 < ws1) load_blocked_n<IT>(lw, ws0 * S + lane * IT, n, nv);
     for (int sg = ws0; sg < ws1; ++sg) {
       const int i0 = sg * S + lane * IT;
       double v[IT];
-      load_blocked_n<IT>(lw, i0, n, v);
+#pragma unroll
+      for (int k = 0; k < IT; ++k) v[k] = nv[k];
+      if (sg + 1 < ws1) load_blocked_n<IT>(lw, i0 + S, n, nv);
 #pragma unroll
       for (int k = 0; k < IT; ++k) {
         if (i0 + k < n) {
@@ -516,15 +522,25 @@ k_systematic_coop(const double* __restrict__ lw, int n, StepStats* st, const dou
     // Os of the particle before the warp's first (0 before particle 0)
     int prev_os = ws0 == 0 ? 0 : systematic_Os(u128_to_weight(carry), W, yW, nd, a, n);
     int zeros = 0;
+    unsigned long long nq[IT];
+    if (ws0 < ws1) {
+      const int j0 = ws0 * S + lane * IT;
+#pragma unroll
+      for (int k = 0; k < IT; ++k) nq[k] = (j0 + k < n) ? __ldcg(qbuf + j0 + k) : 0ull;
+    }
     for (int sg = ws0; sg < ws1; ++sg) {
       const int i0 = sg * S + lane * IT;
       unsigned long long q[IT];
       u128 loc = u128_zero();
 #pragma unroll
       for (int k = 0; k < IT; ++k) {
-        q[k] = (i0 + k < n) ? __ldcg(qbuf + i0 + k) : 0ull;
+        q[k] = nq[k];
         u128 qq; qq.lo = q[k]; qq.hi = 0;
         loc = u128_add(loc, qq);
+      }
+      if (sg + 1 < ws1) {
+#pragma unroll
+        for (int k = 0; k < IT; ++k) nq[k] = (i0 + S + k < n) ? __ldcg(qbuf + i0 + S + k) : 0ull;
       }
       const u128 inc = warp_inclusive_u128(loc);
       u128 Q = u128_add(carry, u128_sub(inc, loc));
@@ -569,11 +585,20 @@ k_systematic_coop(const double* __restrict__ lw, int n, StepStats* st, const dou
     for (int w = 0; w < warp; ++w) zc += s_wint[w];
     const int first = ws0 * S;
     int prev_os = (ws0 < ws1 && first > 0) ? __ldcg(Os + first - 1) : 0;
+    int nos[IT];
+    if (ws0 < ws1) {
+#pragma unroll
+      for (int k = 0; k < IT; ++k) nos[k] = (first + lane * IT + k < n) ? __ldcg(Os + first + lane * IT + k) : 0;
+    }
     for (int sg = ws0; sg < ws1; ++sg) {
       const int i0 = sg * S + lane * IT;
       int os[IT], z[IT];
 #pragma unroll
-      for (int k = 0; k < IT; ++k) os[k] = (i0 + k < n) ? __ldcg(Os + i0 + k) : 0;
+      for (int k = 0; k < IT; ++k) os[k] = nos[k];
+      if (sg + 1 < ws1) {
+#pragma unroll
+        for (int k = 0; k < IT; ++k) nos[k] = (i0 + S + k < n) ? __ldcg(Os + i0 + S + k) : 0;
+      }
       const int up = __shfl_up_sync(0xffffffffu, os[IT - 1], 1);
       const int before0 = lane > 0 ? up : prev_os;
       int loc = 0;
@@ -615,11 +640,14 @@ k_systematic_coop(const double* __restrict__ lw, int n, StepStats* st, const dou
   warp_segments(rb0, rb1, warp, NW, &rs0, &rs1);
   {
     int mloc = 0;
-    for (int sg = rs0; sg < rs1; ++sg) {
-      const int r0 = sg * S + lane * IT;
+    for (int sg = rs0; sg < rs1; sg += 4) {  // four segments' loads in flight
 #pragma unroll
-      for (int k = 0; k < IT; ++k)
-        if (r0 + k < R) mloc = max(mloc, __ldcg(marks + r0 + k));
+      for (int u = 0; u < 4; ++u) {
+        const int r0 = (sg + u) * S + lane * IT;
+#pragma unroll
+        for (int k = 0; k < IT; ++k)
+          if (sg + u < rs1 && r0 + k < R) mloc = max(mloc, __ldcg(marks + r0 + k));
+      }
     }
     mloc = warp_inclusive_max_int(mloc);
     __syncthreads();  // every warp has read s_wint
@@ -637,15 +665,31 @@ k_systematic_coop(const double* __restrict__ lw, int n, StepStats* st, const dou
     for (int j = threadIdx.x; j < b; j += blockDim.x) mc = max(mc, __ldcg(block_m + j));
     mc = block_max_int(mc);
     for (int w = 0; w < warp; ++w) mc = max(mc, s_wint[w]);
+    int nm[IT], nsl[IT];
+    if (rs0 < rs1) {
+      const int q0 = rs0 * S + lane * IT;
+#pragma unroll
+      for (int k = 0; k < IT; ++k) {
+        nm[k] = (q0 + k < R) ? __ldcg(marks + q0 + k) : 0;
+        nsl[k] = (q0 + k < R) ? __ldcg(slot + q0 + k) : 0;
+      }
+    }
     for (int sg = rs0; sg < rs1; ++sg) {
       const int r0 = sg * S + lane * IT;
       int m[IT], sl[IT];
       int run = 0;
 #pragma unroll
       for (int k = 0; k < IT; ++k) {
-        m[k] = (r0 + k < R) ? __ldcg(marks + r0 + k) : 0;
-        sl[k] = (r0 + k < R) ? __ldcg(slot + r0 + k) : 0;
+        m[k] = nm[k];
+        sl[k] = nsl[k];
         run = max(run, m[k]);
+      }
+      if (sg + 1 < rs1) {
+#pragma unroll
+        for (int k = 0; k < IT; ++k) {
+          nm[k] = (r0 + S + k < R) ? __ldcg(marks + r0 + S + k) : 0;
+          nsl[k] = (r0 + S + k < R) ? __ldcg(slot + r0 + S + k) : 0;
+        }
       }
       const int inc = warp_inclusive_max_int(run);
       const int up = __shfl_up_sync(0xffffffffu, inc, 1);
