@@ -94,21 +94,13 @@ BPF_HD double bpf_exp(double x) {
   return (p * bpf_bitsd((uint64_t)(ki + 1000 + 1023) << 52)) * bpf_bitsd((uint64_t)(-1000 + 1023) << 52);
 }
 
-BPF_HD double bpf_log(double x) {
+/* log of a positive, finite, normal x times 2^e0: the body of bpf_log
+ * without its special cases */
+BPF_HD double bpf_log_normal(double x, int e0) {
   const double ln2_hi = 0.6931471803691238;
   const double ln2_lo = 1.9082149292705877e-10;
-  if (x != x) return x;
-  if (x < 0.0) return NAN;
-  if (x == 0.0) return -INFINITY;
-  if (x == INFINITY) return x;
-  int e = 0;
-  uint64_t u = bpf_dbits(x);
-  if ((u >> 52) == 0) { /* subnormal: renormalise */
-    x = x * 18014398509481984.0; /* 2^54 */
-    u = bpf_dbits(x);
-    e = -54;
-  }
-  e += (int)(u >> 52) - 1023;
+  const uint64_t u = bpf_dbits(x);
+  int e = e0 + (int)(u >> 52) - 1023;
   double m = bpf_bitsd((u & 0x000FFFFFFFFFFFFFull) | 0x3FF0000000000000ull); /* [1,2) */
   if (m > 1.4142135623730951) { m = m * 0.5; e += 1; }
   double s = (m - 1.0) / (m + 1.0);
@@ -131,18 +123,17 @@ BPF_HD double bpf_log(double x) {
   return BPF_MATH_FMA(ed, ln2_hi, BPF_MATH_FMA(ed, ln2_lo, lm));
 }
 
-/* sin(pi x) and cos(pi x) */
-BPF_HD void bpf_sincospi(double x, double* sp, double* cp) {
-  double q;
-  int qi;
-  if (fabs(x) < 1.0e15) {  /* q = rint(2x) by the rounding constant; quadrant = low bits */
-    const double t = 2.0 * x + 6755399441055744.0;
-    q = t - 6755399441055744.0;
-    qi = (int)(bpf_dbits(t) & 3u);
-  } else {
-    q = rint(2.0 * x);
-    qi = ((int)fmod(q, 4.0) + 4) & 3;
-  }
+BPF_HD double bpf_log(double x) {
+  if (x != x) return x;
+  if (x < 0.0) return NAN;
+  if (x == 0.0) return -INFINITY;
+  if (x == INFINITY) return x;
+  if ((bpf_dbits(x) >> 52) == 0) return bpf_log_normal(x * 18014398509481984.0, -54); /* subnormal: x 2^54 */
+  return bpf_log_normal(x, 0);
+}
+
+/* sin(pi x), cos(pi x) from q = rint(2x) and its quadrant qi */
+BPF_HD void bpf_sincospi_q(double x, double q, int qi, double* sp, double* cp) {
   double r = BPF_MATH_FMA(-0.5, q, x);
   double r2 = r * r;
   double s = -2.2948428997269873e-08;            /* -pi^19/19! */
@@ -172,6 +163,24 @@ BPF_HD void bpf_sincospi(double x, double* sp, double* cp) {
     case 2: *sp = -s; *cp = -c; break;
     default: *sp = -c; *cp = s; break;
   }
+}
+
+
+/* bpf_sincospi for |x| < 1e15: q = rint(2x) by the rounding constant, the
+ * quadrant in its low bits */
+BPF_HD void bpf_sincospi_small(double x, double* sp, double* cp) {
+  const double t = 2.0 * x + 6755399441055744.0;
+  bpf_sincospi_q(x, t - 6755399441055744.0, (int)(bpf_dbits(t) & 3u), sp, cp);
+}
+
+/* sin(pi x) and cos(pi x) */
+BPF_HD void bpf_sincospi(double x, double* sp, double* cp) {
+  if (fabs(x) < 1.0e15) {
+    bpf_sincospi_small(x, sp, cp);
+    return;
+  }
+  const double q = rint(2.0 * x);
+  bpf_sincospi_q(x, q, ((int)fmod(q, 4.0) + 4) & 3, sp, cp);
 }
 
 /* ----------------------------------------------------------------- float */
@@ -291,10 +300,12 @@ BPF_HD void bpf_normal_pair_f(uint32_t a, uint32_t b, float* z0, float* z1) {
 }
 
 BPF_HD void bpf_normal_pair_d(uint32_t a, uint32_t b, double* z0, double* z1) {
+  /* as in bpf_normal_pair_f: the guards of bpf_log and bpf_sincospi
+   * cannot arise for these uniforms */
   double ua = (double)bpf_u01f(a), ub = (double)bpf_u01f(b);
-  double r = sqrt(-2.0 * bpf_log(ua));
+  double r = sqrt(-2.0 * bpf_log_normal(ua, 0));
   double s, c;
-  bpf_sincospi(2.0 * ub, &s, &c);
+  bpf_sincospi_small(2.0 * ub, &s, &c);
   *z0 = r * c;
   *z1 = r * s;
 }
