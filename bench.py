@@ -809,7 +809,11 @@ def main():
         "wall_s": wall,
         "clocks": clocks,
     }
-    if rank == 0:
+    # the sections below are single-GPU measurements: under torchrun (N > 1)
+    # the line carries the replicas' headline only, so that no rank waits
+    # at the final barrier while rank 0 runs them
+    extras = rank == 0 and world == 1
+    if extras:
         # the resampler's tile shape for this N (bpf_create tuned it; timed
         # again here so the line shows each shape's median)
         from libbi_b200 import autotune_resampler
@@ -818,16 +822,16 @@ def main():
         best, us = autotune_resampler(N_PARTICLES)
         line["autotune"] = {"systematic_resampler_n": N_PARTICLES, "shape": list(RESAMPLE_SHAPES[best]),
                             "median_us": {f"{a}x{b}": v for (a, b), v in us.items()}}
-    if rank == 0 and not args.no_large_n:
+    if extras and not args.no_large_n:
         line["kernels_large_n"] = large_n_kernels()
-    if rank == 0 and not args.no_batched:
+    if extras and not args.no_batched:
         line["batched"] = batched_filters()
         line["pmmh"] = pmmh_chains()
-    if rank == 0 and not args.no_precision:
+    if extras and not args.no_precision:
         line["precision"] = precision_check(y_host)
-    if rank == 0 and not args.no_guided:
+    if extras and not args.no_guided:
         line["guided"] = guided_vs_bootstrap(y_host, seeds=max(2, args.guided_seeds))
-    if rank == 0 and not args.no_cpu_baseline:
+    if extras and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(y_host)
     pf.close()
     if dist:
