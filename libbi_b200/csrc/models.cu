@@ -28,7 +28,6 @@ k_l96_transition(const T* __restrict__ x_in, T* __restrict__ x_out, int ld, int 
   const int p = blockIdx.x * kL96Block + threadIdx.x;
   const int resampled = st->resample;
   const bool ok = st->status == BPF_OK;
-  const double ll = st->ll;
   LwPartial part = lw_empty();
   if (ok && p < n) {
     const int src = resampled ? as[p] : p;
@@ -38,8 +37,10 @@ k_l96_transition(const T* __restrict__ x_in, T* __restrict__ x_out, int ld, int 
     l96_rk4<T, D>(x0, t1d, t2d, (T)prm.F, (T)prm.h);
 #pragma unroll
     for (int i = 0; i < D; ++i) sx[i][threadIdx.x] = x0[i];
+    // st->ll is read after the ODE (not held across it); the last block
+    // rewrites it only after every block has arrived
     const double l = l96_noise_obs<T, D>(sx, x_out, (size_t)ld, p, y, seed, (uint32_t)p, step, prm,
-                                         resampled ? ll : lw[p], mask);
+                                         resampled ? st->ll : lw[p], mask);
     lw[p] = l;
     if (resampled) as[p] = src;
     lw_push(part, l);
