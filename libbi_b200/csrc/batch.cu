@@ -103,8 +103,6 @@ k_batch_l96_transition(const T* __restrict__ x_in, T* __restrict__ x_out, int ld
   const int p = (blockIdx.x - fd.block0) * kL96Block + threadIdx.x;
   const int resampled = st->resample;
   const bool ok = st->status == BPF_OK;
-  const double ll = st->ll;
-  const L96Params prm = prms[f];
   const T* yf = y ? y + (size_t)f * D : nullptr;
   LwPartial part = lw_empty();
   if (ok && p < fd.n) {
@@ -113,11 +111,15 @@ k_batch_l96_transition(const T* __restrict__ x_in, T* __restrict__ x_out, int ld
     T x0[D];
 #pragma unroll
     for (int i = 0; i < D; ++i) x0[i] = __ldg(x_in + (size_t)i * ld + fd.off + src);
-    l96_rk4<T, D>(x0, t1d, t2d, (T)prm.F, (T)prm.h);
+    l96_rk4<T, D>(x0, t1d, t2d, (T)prms[f].F, (T)prms[f].h);
 #pragma unroll
     for (int i = 0; i < D; ++i) sx[i][threadIdx.x] = x0[i];
+    // the filter's constants and log-likelihood are read after the ODE (not
+    // held across it); the last block rewrites st->ll only after every
+    // block has arrived
+    const L96Params prm = prms[f];
     const double l = l96_noise_obs<T, D>(sx, x_out, (size_t)ld, col, yf, fd.seed, (uint32_t)p, step, prm,
-                                         resampled ? ll : lw[col]);
+                                         resampled ? st->ll : lw[col]);
     lw[col] = l;
     if (resampled) as[col] = src;
     lw_push(part, l);
