@@ -126,8 +126,6 @@ __device__ __forceinline__ void load_blocked(const double* __restrict__ lw, int 
   }
 }
 
-__device__ __forceinline__ int ntiles_dev(int n) { return (n + kTile - 1) / kTile; }
-
 __device__ __forceinline__ int block_max_int(int v) {
   __shared__ int wm[kBlock / 32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -138,36 +136,6 @@ __device__ __forceinline__ int block_max_int(int v) {
   int r = lane < kBlock / 32 ? wm[lane] : 0;
 #pragma unroll
   for (int d = 16; d > 0; d >>= 1) r = max(r, __shfl_xor_sync(0xffffffffu, r, d));
-  __syncthreads();
-  return r;
-}
-
-// Block-wide exclusive max-scan of non-negative ints (identity 0).
-__device__ __forceinline__ int block_exclusive_scan_max_int(int v, int* total) {
-  __shared__ int wt[kBlock / 32];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int inc = v;
-#pragma unroll
-  for (int d = 1; d < 32; d <<= 1) {
-    int o = __shfl_up_sync(0xffffffffu, inc, d);
-    if (lane >= d) inc = max(inc, o);
-  }
-  int exc = __shfl_up_sync(0xffffffffu, inc, 1);
-  if (lane == 0) exc = 0;
-  if (lane == 31) wt[warp] = inc;
-  __syncthreads();
-  if (warp == 0) {
-    int t = lane < kBlock / 32 ? wt[lane] : 0;
-#pragma unroll
-    for (int d = 1; d < kBlock / 32; d <<= 1) {
-      int o = __shfl_up_sync(0xffffffffu, t, d);
-      if (lane >= d) t = max(t, o);
-    }
-    if (lane < kBlock / 32) wt[lane] = t;
-  }
-  __syncthreads();
-  const int r = max(warp > 0 ? wt[warp - 1] : 0, exc);
-  *total = wt[kBlock / 32 - 1];
   __syncthreads();
   return r;
 }
@@ -374,11 +342,6 @@ __device__ __forceinline__ void load_blocked_n(const double* __restrict__ lw, in
 #pragma unroll
     for (int k = 0; k < IT; ++k) v[k] = (i0 + k < n) ? __ldg(lw + i0 + k) : NAN;
   }
-}
-
-__device__ __forceinline__ void load_blocked_cg(const double* __restrict__ lw, int i0, int n, double v[kItems]) {
-#pragma unroll
-  for (int k = 0; k < kItems; ++k) v[k] = (i0 + k < n) ? lw[i0 + k] : NAN;
 }
 
 __device__ __forceinline__ u128 block_sum_u128_from_global(const u128* a, int count) {
