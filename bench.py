@@ -50,8 +50,9 @@ TRANSITION_BYTES_PER_PARTICLE = 2 * DIM * 4 + 16
 # RK4 5 sub-steps x 40 components x 31 + noise add 2 x 40 + observation 6 x 40
 TRANSITION_FLOP_PER_PARTICLE = 5 * DIM * 31 + 2 * DIM + 6 * DIM
 # DRAM bytes (read + write) of one transition launch at this workload from an
-# ncu capture (profiles/k_l96_transition_l96_d40_n65536.md): 10.8 MB read,
-# nothing written back within the launch (the new state stays in L2)
+# ncu capture of the transition (dram__bytes_read.sum + dram__bytes_write.sum):
+# 10.8 MB read, nothing written back within the launch (the new state stays
+# in L2)
 TRANSITION_DRAM_BYTES_PER_LAUNCH = 10_813_440 + 0
 
 
@@ -116,6 +117,16 @@ class ClockSampler:
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
                 "samples": len(sm)}
+
+
+L2_NOTE = "flushed before every timed step (256 MiB write)"
+
+
+def workload_config(world: int) -> dict:
+    """The workload's `config` object, the same in both arms."""
+    return {"workload": WORKLOAD, "nparticles": N_PARTICLES, "dim": DIM, "obs_interval": DT, "rk4_h": 0.01,
+            "resampler": "systematic", "ess_rel": ESS_REL,
+            "parallelism": f"replicas{world}" if world > 1 else "single", "l2": L2_NOTE}
 
 
 def observe(xs, sigma_y):
@@ -653,12 +664,15 @@ def run_reference(args):
     model = configs.L96_D40_N65536["model"]
     _, xs = Oracle().simulate(model.desc(), DATA_SEED, T_OBS, 0.0, DT)
     y = observe(xs, model.sigma_y)
+    # the host's caches are flushed the same way before the timed sample
+    import numpy as np
+
+    np.ones(L2_FLUSH_BYTES // 8)
     cb = cpu_baseline(y, seconds=max(5.0, 2.0 * (args.steps + args.warmup)))
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "nparticles": N_PARTICLES, "dim": DIM, "resampler": "systematic",
-                       "ess_rel": ESS_REL},
+            "config": workload_config(args.gpus),
             "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -788,11 +802,8 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "nparticles": N_PARTICLES, "dim": DIM, "obs_interval": DT,
-                   "rk4_h": 0.01, "resampler": "systematic", "ess_rel": ESS_REL,
-                   "parallelism": f"replicas{world}" if world > 1 else "single",
-                   "l2": "flushed before every timed step (256 MiB write)",
-                   "resampled_steps_end_to_end": f"{resampled} of {args.steps}"},
+        "config": workload_config(world),
+        "resampled_steps_end_to_end": f"{resampled} of {args.steps}",
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": DIM * 4,
                 "d2h_bytes_per_step": 80, "timer": "host wall clock around bpf_step"},
         "gpu_launches": LAUNCHES_PER_STEP * args.steps,

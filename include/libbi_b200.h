@@ -275,6 +275,18 @@ int bpf_autotune_resampler(int n, void* stream, bpf_tune_result* out);
  * does. */
 int bpf_resampler_set_shape(bpf_resampler* r, int shape);
 
+/* Diagnostic hook, no counterpart in the reference (its resamplers have no
+ * device-side waits).  Every grid-wide barrier of the cooperative systematic
+ * resampler waits at most `cycles` SM clock cycles on the current device
+ * (BPF_WAIT_LIMIT_DEFAULT, about 2 s, unless changed); a block that gives up
+ * records BPF_E_TIMEOUT and its kernel returns.  A negative value makes a
+ * block that finds a barrier still closed give up at once, so that a test
+ * can take the timeout path without a kernel that never arrives.  The next
+ * status reset (each stand-alone resampler call, bpf_init, bpf_restore)
+ * clears the barrier state the abandoned launch left. */
+#define BPF_WAIT_LIMIT_DEFAULT 4000000000LL
+int bpf_debug_set_wait_limit(long long cycles);
+
 /* gather_rows (share/src/bi/primitive/matrix_primitive.hpp:630-638,
  * share/src/bi/cuda/primitive/matrix_primitive_kernel.cuh:50-57), out of
  * place on device SoA buffers: Y[j*ld + i] = X[j*ld + as[i]], j < d, i < n.
@@ -294,8 +306,11 @@ int bpf_gather_rows(const int* as, const void* X, void* Y, int n, int d, int ld,
  * GPU that loads the library until the process exits), so n may be at most
  * BPF_STATIC_MAX_PARTICLES; larger n returns BPF_E_TOO_LARGE.  The first call
  * on each device looks up that array's address; make it before any stream
- * capture.  All calls share the array, so calls that overlap on the GPU race
- * and must be ordered by the caller.  Synchronises `stream` and returns
+ * capture.  The address is kept for the life of the process: after a
+ * cudaDeviceReset the array may move, so this entry point must not be used
+ * again in that process.  All calls share the array, so calls that overlap
+ * on the GPU race and must be ordered by the caller.  Synchronises `stream`
+ * and returns
  * BPF_E_DEGENERATE when the weights sum to zero or are not finite. */
 #define BPF_STATIC_MAX_PARTICLES 65536
 int bpf_systematic_ancestors_static(const double* lw, int n, const double* a, int permute, int* as, int* Os,

@@ -22,6 +22,7 @@ BPF_E_NOMEM = 5
 BPF_E_TOO_LARGE = 6
 BPF_STATIC_MAX_PARTICLES = 65536
 BPF_BATCH_MAX_PARTICLES = 32768
+BPF_WAIT_LIMIT_DEFAULT = 4000000000
 
 BPF_MODEL_L96 = 1
 BPF_MODEL_PZ = 2
@@ -50,7 +51,7 @@ EXPORTS = (
     "bpf_proposal_create", "bpf_proposal_destroy", "bpf_proposal_set_data", "bpf_proposal_train",
     "bpf_proposal_loss_grad", "bpf_proposal_params", "bpf_proposal_set_params", "bpf_set_proposal",
     "bpf_batch_set_proposal",
-    "bpf_path_cache", "bpf_sample_path", "bpf_step_sparse", "bpf_smc2_run",
+    "bpf_path_cache", "bpf_sample_path", "bpf_step_sparse", "bpf_smc2_run", "bpf_debug_set_wait_limit",
 )
 
 
@@ -194,6 +195,7 @@ def _declare(L):
         "bpf_resampler_set_shape": (c_int, [H, c_int]),
         "bpf_systematic_ancestors_static": (c_int, [c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p,
                                                     c_void_p]),
+        "bpf_debug_set_wait_limit": (c_int, [c_longlong]),
         "bpf_version": (c_char_p, []),
         "bpf_status_string": (c_char_p, [c_int]),
     }

@@ -18,8 +18,9 @@ OUT = os.path.join(HERE, "_lib", "libbi_b200.so")
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",
-    "-Xcompiler", "-fPIC", "-shared",
+    "-Xcompiler", "-fPIC",
 ]
+OBJ_DIR = os.path.join(HERE, "_lib", "obj")
 
 
 def nvcc() -> str:
@@ -42,13 +43,31 @@ def up_to_date() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile every source to an object in parallel (the sources share no
+    device code, so no relocatable device code is needed), then link the
+    shared library."""
     if not force and up_to_date():
         return OUT
-    os.makedirs(os.path.dirname(OUT), exist_ok=True)
-    cmd = [nvcc()] + NVCC_FLAGS + sources() + ["-o", OUT]
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    srcs = sources()
+    objs = [os.path.join(OBJ_DIR, os.path.basename(f)[:-3] + ".o") for f in srcs]
+    cmds = [[nvcc()] + NVCC_FLAGS + ["-c", f, "-o", o] for f, o in zip(srcs, objs)]
     if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
+        for c in cmds:
+            print(" ".join(c))
+    from concurrent.futures import ThreadPoolExecutor
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(lambda c: subprocess.run(c, capture_output=True, text=True), cmds))
+    for c, r in zip(cmds, results):
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise subprocess.CalledProcessError(r.returncode, c)
+    link = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-Xcompiler", "-fPIC"] + objs + [
+        "-o", OUT]
+    if verbose:
+        print(" ".join(link))
+    subprocess.run(link, check=True)
     return OUT
 
 

@@ -265,7 +265,14 @@ __global__ void k_record(const bpf::StepStats* st, double* hist, int k) {
   hist[3 * k + 2] = (double)st->resampled;
 }
 
-__global__ void k_set_status_ok(bpf::StepStats* st) { st->status = BPF_OK; }
+// the status of a stand-alone call back to BPF_OK, with the grid-barrier
+// counter and generation of the scratch (bar[0], bar[1]): a cooperative
+// launch that timed out can leave the counter above zero
+__global__ void k_set_status_ok(bpf::StepStats* st, unsigned* bar) {
+  st->status = BPF_OK;
+  bar[0] = 0u;
+  bar[1] = 0u;
+}
 
 // set_elements(s.logWeights(), s.logLikelihood), Resampler.hpp:177
 __global__ void k_reset_lw(double* lw, int n, const bpf::StepStats* st) {
@@ -569,6 +576,9 @@ int bpf_init(bpf_handle* h) {
   if (!h) return BPF_E_INVALID;
   h->cur = 0;
   h->step = 0;
+  // the last-block tickets and grid-barrier words start from zero (a
+  // cooperative resampling that timed out can leave a barrier counter set)
+  BPF_TRY(cudaMemsetAsync(h->rs.counters, 0, 16 * sizeof(unsigned), h->stream));
   int rc = bpf::launch_init(h->model, h->x[0], h->ld, h->n, h->lw, h->cfg.seed, h->rs.stats, h->cfg.ess_rel,
                             h->stream);
   if (rc) return rc;
@@ -831,7 +841,7 @@ int bpf_resampler_destroy(bpf_resampler* r) {
 }
 
 static int reset_status(bpf_resampler* r) {
-  k_set_status_ok<<<1, 1, 0, r->stream>>>(r->rs.stats);
+  k_set_status_ok<<<1, 1, 0, r->stream>>>(r->rs.stats, r->rs.counters + 8);
   BPF_TRY(cudaGetLastError());
   return BPF_OK;
 }
@@ -958,6 +968,8 @@ int bpf_resampler_ancestors(bpf_resampler* r, const double* lw, int n, const dou
   return s.status;
 }
 
+int bpf_debug_set_wait_limit(long long cycles) { return bpf::set_barrier_limit(cycles); }
+
 int bpf_gather_rows(const int* as, const void* X, void* Y, int n, int d, int ld, int elem_size, void* stream) {
   if (!as || !X || !Y || X == Y) return BPF_E_INVALID;
   return bpf::launch_gather(as, X, Y, n, d, ld, elem_size, nullptr, (cudaStream_t)stream);
@@ -1017,6 +1029,7 @@ int bpf_restore(bpf_handle* h, const void* buf, uint64_t bytes) {
   p += (size_t)h->n * sizeof(double);
   BPF_TRY(cudaMemcpyAsync(h->as, p, (size_t)h->n * sizeof(int), cudaMemcpyHostToDevice, h->stream));
   BPF_TRY(cudaMemcpyAsync(h->rs.stats, &hd.stats, sizeof(hd.stats), cudaMemcpyHostToDevice, h->stream));
+  BPF_TRY(cudaMemsetAsync(h->rs.counters, 0, 16 * sizeof(unsigned), h->stream));
   BPF_TRY(cudaStreamSynchronize(h->stream));
   h->step = hd.step;
   return BPF_OK;

@@ -244,6 +244,10 @@ int autotune_systematic(int n, cudaStream_t st, int* best, double* us);
 // shape holds n particles in one wave
 int autotuned_shape(int n);
 
+// limit of the grid-barrier waits of the cooperative resamplers on the
+// current device, in SM clock cycles (negative: give up at once)
+int set_barrier_limit(long long cycles);
+
 int launch_gather(const int* as, const void* X, void* Y, int n, int d, int ld, int esz,
                   const int* gate, cudaStream_t st);
 

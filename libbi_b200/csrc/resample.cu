@@ -276,6 +276,12 @@ k_systematic_offspring(const double* __restrict__ lw, int n, StepStats* st,
 // ---------------------------------------------------------------------------
 constexpr long long kBarrierTimeoutCycles = 4000000000ll;  // ~2 s at 2 GHz
 
+// The limit the waits use, per device (set_barrier_limit).  A negative limit
+// makes a block that finds the barrier still closed give up at once, which
+// lets a test take the BPF_E_TIMEOUT path without a kernel that never
+// arrives.
+__device__ long long g_barrier_limit = kBarrierTimeoutCycles;
+
 __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
   unsigned v;
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -301,7 +307,12 @@ __device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
 // barrier, are released with it); the last to arrive has then acquired all
 // of them, resets the counter and publishes the next generation with a
 // release store; the others poll the generation with acquire loads.
-// Returns false (in every thread) on timeout.
+// Returns false (in every thread) on timeout.  A block that gives up has
+// already arrived, so after a timeout the counter can stay above zero: the
+// host clears the counter and generation together with the status before
+// the next launch on the same scratch (the status reset of the stand-alone
+// resampler, bpf_init and bpf_restore of a filter), and until then the
+// sticky status keeps every later launch on that scratch from starting.
 __device__ __forceinline__ bool grid_barrier(unsigned* counter, unsigned* gen, StepStats* st) {
   __shared__ int s_ok;
   __syncthreads();
@@ -313,9 +324,10 @@ __device__ __forceinline__ bool grid_barrier(unsigned* counter, unsigned* gen, S
       *counter = 0;  // ordered before the release below; nobody arrives again before it
       st_release_gpu(gen, g + 1u);
     } else {
+      const long long lim = g_barrier_limit;
       const long long t0 = clock64();
       while (ld_acquire_gpu(gen) == g) {
-        if (clock64() - t0 > kBarrierTimeoutCycles) {
+        if (lim < 0 || clock64() - t0 > lim) {
           ok = 0;
           st->status = BPF_E_TIMEOUT;
           break;
@@ -1323,32 +1335,66 @@ static void set_tuned_shape(int dev, int n, int shape) {
   if (dev >= 0 && dev < 16) g_tuned[dev][size_class(n)] = shape;
 }
 
-// resident blocks per SM of each shape at a dynamic shared-memory size
-// (cached; the launch is on every filter step)
-static int shape_per_sm(int k, size_t smem) {
-  static size_t cached[BPF_RESAMPLE_SHAPES] = {(size_t)-1, (size_t)-1, (size_t)-1,
-                                               (size_t)-1, (size_t)-1, (size_t)-1};
-  static int per[BPF_RESAMPLE_SHAPES] = {0};
-  if (cached[k] != smem) {
+// Device attributes and occupancies of the cooperative launches, kept per
+// device: a process may drive several GPUs (one handle per host thread), so
+// nothing here may come from whichever device happened to be current first.
+// The launch is on every filter step, hence the cache.
+constexpr int kMaxCoopDevices = 64;
+struct CoopDevice {
+  bool init = false;
+  int coop = 0, sms = 0;
+  int per_sm_multi = 0;                      // k_systematic_coop blocks per SM
+  size_t smem[BPF_RESAMPLE_SHAPES] = {};     // shared memory the cached occupancy is for
+  int per[BPF_RESAMPLE_SHAPES] = {};         // resident blocks per SM of each shape
+  bool have[BPF_RESAMPLE_SHAPES] = {};
+};
+static std::mutex g_coop_mu;
+static CoopDevice g_coop[kMaxCoopDevices];
+
+// the current device's entry, filled on first use
+static int coop_device(int* dev_out, CoopDevice** out) {
+  int dev = 0;
+  BPF_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxCoopDevices) return BPF_E_INVALID;
+  std::lock_guard<std::mutex> lk(g_coop_mu);
+  CoopDevice& d = g_coop[dev];
+  if (!d.init) {
+    BPF_TRY(cudaDeviceGetAttribute(&d.coop, cudaDevAttrCooperativeLaunch, dev));
+    BPF_TRY(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev));
+    BPF_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&d.per_sm_multi, k_systematic_coop<kCoopItems>, kBlock, 0));
+    d.init = true;
+  }
+  *dev_out = dev;
+  *out = &d;
+  return BPF_OK;
+}
+
+// resident blocks per SM of shape k at a dynamic shared-memory size on the
+// device of entry d
+static int shape_per_sm(CoopDevice& d, int k, size_t smem) {
+  std::lock_guard<std::mutex> lk(g_coop_mu);
+  if (!d.have[k] || d.smem[k] != smem) {
     int v = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kCoopShapes[k].fn, kCoopShapes[k].nt, smem) != cudaSuccess) {
       cudaGetLastError();
       v = 0;
     }
-    per[k] = v;
-    cached[k] = smem;
+    d.per[k] = v;
+    d.smem[k] = smem;
+    d.have[k] = true;
   }
-  return per[k];
+  return d.per[k];
 }
 
 // launch shape k of the one-launch kernel if its tiles fit the GPU in one
 // wave; BPF_E_INVALID when they do not
-static int launch_coop1_shape(int k, const ResampleArgs& a, ResampleScratch& s, int* Os_out, int sms, cudaStream_t st) {
+static int launch_coop1_shape(int k, const ResampleArgs& a, ResampleScratch& s, int* Os_out, CoopDevice& d,
+                              cudaStream_t st) {
   const int n = a.n;
   const int tile = kCoopShapes[k].nt * kCoopShapes[k].it;
   const int G = (n + tile - 1) / tile;
   const size_t smem = fill_smem(n, kMaxCoarseCoop);
-  if (G < 1 || G > sms * shape_per_sm(k, smem)) return BPF_E_INVALID;
+  if (G < 1 || G > d.sms * shape_per_sm(d, k, smem)) return BPF_E_INVALID;
   int sh = coarse_shift(n, kMaxCoarseCoop);
   const double* lw = a.lw;
   StepStats* stats = s.stats;
@@ -1377,30 +1423,22 @@ static int launch_coop1_shape(int k, const ResampleArgs& a, ResampleScratch& s, 
 // grid; BPF_E_INVALID when a cooperative launch is not possible, so the
 // caller can run the passes.
 static int launch_systematic_coop(const ResampleArgs& a, ResampleScratch& s, int* Os_out, cudaStream_t st) {
-  static int coop_supported = -1, sms = 0;
   int dev = 0;
-  BPF_TRY(cudaGetDevice(&dev));
-  if (coop_supported < 0) {
-    BPF_TRY(cudaDeviceGetAttribute(&coop_supported, cudaDevAttrCooperativeLaunch, dev));
-    BPF_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  }
-  if (!coop_supported) return BPF_E_INVALID;
+  CoopDevice* d = nullptr;
+  int rc = coop_device(&dev, &d);
+  if (rc) return rc;
+  if (!d->coop) return BPF_E_INVALID;
   const int n = a.n;
   // one tile per block: the pinned shape, else the autotuned one, else the
   // default; then any other shape that fits
   int first = a.shape >= 0 && a.shape < BPF_RESAMPLE_SHAPES ? a.shape : tuned_shape(dev, n);
   if (first < 0) first = 0;  // untuned, or nothing fits (the loop below then falls through)
-  int rc = launch_coop1_shape(first, a, s, Os_out, sms, st);
+  rc = launch_coop1_shape(first, a, s, Os_out, *d, st);
   for (int k = 0; rc == BPF_E_INVALID && k < BPF_RESAMPLE_SHAPES; ++k)
-    if (k != first) rc = launch_coop1_shape(k, a, s, Os_out, sms, st);
+    if (k != first) rc = launch_coop1_shape(k, a, s, Os_out, *d, st);
   if (rc != BPF_E_INVALID) return rc;
   // several tiles per block
-  static size_t cached_smem = (size_t)-1;
-  static int per_sm = 0;
-  if (cached_smem == (size_t)-1) {
-    BPF_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_systematic_coop<kCoopItems>, kBlock, 0));
-    cached_smem = 0;
-  }
+  const int sms = d->sms, per_sm = d->per_sm_multi;
   const int T8 = (n + kBlock * kCoopItems - 1) / (kBlock * kCoopItems);  // tiles of the multi-tile variant
   int G = sms * per_sm;
   if (G > T8) G = T8;
@@ -1451,16 +1489,18 @@ int autotune_systematic(int n, cudaStream_t st, int* best, double* us) {
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   BPF_TRY(cudaStreamIsCapturing(st, &cs));
   if (cs != cudaStreamCaptureStatusNone) return BPF_E_INVALID;  // no timing inside a capture
-  int dev = 0, sms = 0, coop = 0;
-  BPF_TRY(cudaGetDevice(&dev));
-  BPF_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  BPF_TRY(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
-  if (!coop) return BPF_E_INVALID;
+  int dev = 0;
+  CoopDevice* d = nullptr;
+  {
+    const int drc = coop_device(&dev, &d);
+    if (drc) return drc;
+  }
+  if (!d->coop) return BPF_E_INVALID;
   // nothing to time when no shape holds n particles in one wave
   bool any = false;
   for (int k = 0; k < BPF_RESAMPLE_SHAPES; ++k) {
     const int tile = kCoopShapes[k].nt * kCoopShapes[k].it;
-    any |= (n + tile - 1) / tile <= sms * shape_per_sm(k, fill_smem(n, kMaxCoarseCoop));
+    any |= (n + tile - 1) / tile <= d->sms * shape_per_sm(*d, k, fill_smem(n, kMaxCoarseCoop));
   }
   if (!any) {
     set_tuned_shape(dev, n, -2);
@@ -1501,7 +1541,7 @@ int autotune_systematic(int n, cudaStream_t st, int* best, double* us) {
     for (int k = 0; !rc && k < BPF_RESAMPLE_SHAPES; ++k) {
       if (!fits[k]) continue;
       if (r >= 0 && cudaEventRecord(e0, st) != cudaSuccess) { rc = BPF_E_CUDA; break; }
-      const int krc = launch_coop1_shape(k, a, s, nullptr, sms, st);
+      const int krc = launch_coop1_shape(k, a, s, nullptr, *d, st);
       if (krc == BPF_E_INVALID) { fits[k] = false; continue; }  // this shape does not fit in one wave
       if (krc) { rc = krc; break; }
       if (r >= 0 && (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
@@ -1532,6 +1572,11 @@ int autotune_systematic(int n, cudaStream_t st, int* best, double* us) {
   scratch_free(s);
   if (rc) cudaGetLastError();
   return rc ? rc : (*best >= 0 ? BPF_OK : BPF_E_INVALID);
+}
+
+int set_barrier_limit(long long cycles) {
+  BPF_TRY(cudaMemcpyToSymbol(g_barrier_limit, &cycles, sizeof(cycles)));
+  return BPF_OK;
 }
 
 int autotuned_shape(int n) {

@@ -162,3 +162,38 @@ def test_every_resampler_thread_count_gives_the_single_filters(cuda, oracle):
         _check(batch, singles, y, dt, ns)
     batch.close()
 
+
+
+def test_c3_largest_filters_match_oracle(cuda, oracle):
+    """The batched configuration's largest filters (32768 particles, one
+    systematic and one multinomial, F = 6.5 and 9.5) over its T = 100,
+    inside a batch with small filters, each directly against the oracle's
+    filter with the same settings: increments, ESS and final states."""
+    from libbi_b200 import BatchedBootstrapPF, ModelL96
+    from libbi_b200 import _native as N
+
+    ns = [32768, 512, 32768, 1000]
+    res = ["systematic", "multinomial", "multinomial", "systematic"]
+    seeds = [1000, 1001, 1002, 1003]
+    models = [ModelL96(dim=40, F=F) for F in (6.5, 8.0, 9.5, 7.0)]
+    T, dt = 100, 0.05
+    y = np.stack([oracle.simulate(m.desc(), 500 + f, T, 0.0, dt)[0] for f, m in enumerate(models)], axis=1)
+    batch = BatchedBootstrapPF(models, ns, res, seeds, ess_rel=0.5)
+    ll, inc, ess, st = batch.filter(y, 0.0, dt)
+    assert (st == 0).all()
+    x, lw, _, offs = batch.state()
+    x, lw = x.cpu().numpy(), lw.cpu().numpy()
+    for f in (0, 2):
+        cfg = N.Config()
+        cfg.nparticles = ns[f]
+        cfg.resampler = N.BPF_RESAMPLER_SYSTEMATIC if res[f] == "systematic" else N.BPF_RESAMPLER_MULTINOMIAL
+        cfg.ess_rel = 0.5
+        cfg.seed = seeds[f]
+        want = oracle.filter(models[f].desc(), cfg, np.ascontiguousarray(y[:, f]), T, 0.0, dt)
+        assert want["rc"] == 0 and want["resampled"].sum() > 0
+        np.testing.assert_allclose(inc[:, f], want["inc"], rtol=1e-10, atol=1e-9)
+        np.testing.assert_allclose(ess[:, f], want["ess"], rtol=1e-9)
+        np.testing.assert_allclose(ll[f], want["ll"], rtol=1e-10)
+        np.testing.assert_array_equal(x[:, offs[f]:offs[f] + ns[f]], want["x"][:, :ns[f]])
+        np.testing.assert_allclose(lw[offs[f]:offs[f] + ns[f]], want["lw"], rtol=1e-12)
+    batch.close()

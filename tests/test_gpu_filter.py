@@ -92,6 +92,34 @@ def test_pz_config_c1_matches_oracle(cuda, oracle):
     pf.close()
 
 
+def test_l96_config_c2_matches_oracle(cuda, oracle):
+    """The benchmarked Lorenz-96 configuration at its own size: d = 40,
+    N = 65536 FP32 particles, RK4 h = 0.01, observations of all 40
+    components with N(0, 1) noise every 0.05, systematic resampling at
+    ESS < 0.5 N, T = 200, on the bench's synthetic observations (one model
+    run from the data seed, observed with N(0, 1) noise from a numpy
+    generator on the same seed); every increment, the ESS, the
+    log-likelihood and the final state against the oracle's filter."""
+    from libbi_b200 import ModelL96
+
+    model, n, T, dt = ModelL96(dim=40), 65536, 200, 0.05
+    desc = model.desc()
+    _, xs = oracle.simulate(desc, 102, T, 0.0, dt)
+    y = (xs + model.sigma_y * np.random.default_rng(102).standard_normal(xs.shape)).astype(np.float32)
+    pf = _mk(model, n, "systematic", 0.5, seed=2)
+    ll, inc, ess = pf.filter(y, 0.0, dt)
+    want = oracle.filter(desc, pf._cfg, y, T, 0.0, dt)
+    assert want["rc"] == 0
+    assert want["resampled"].sum() >= T // 2
+    np.testing.assert_allclose(inc, want["inc"], rtol=1e-10, atol=1e-9)
+    np.testing.assert_allclose(ess, want["ess"], rtol=1e-9)
+    np.testing.assert_allclose(ll, want["ll"], rtol=1e-10)
+    x, lw, _ = pf.state()
+    np.testing.assert_array_equal(x.cpu().numpy()[:, :n], want["x"][:, :n])
+    np.testing.assert_allclose(lw.cpu().numpy(), want["lw"], rtol=1e-12)
+    pf.close()
+
+
 def test_step_api_and_snapshot(cuda, oracle):
     from libbi_b200 import ModelL96
 

@@ -21,8 +21,9 @@ pytestmark = pytest.mark.gpu
 def _static_call(lw, a, permute, as_, Os):
     from libbi_b200 import _native as N
 
-    return N.lib().bpf_systematic_ancestors_static(lw.data_ptr(), lw.numel(), a.data_ptr(), int(permute),
-                                                    as_.data_ptr(), Os.data_ptr(), None)
+    return N.lib().bpf_systematic_ancestors_static(lw.data_ptr(), lw.numel(), None if a is None else a.data_ptr(),
+                                                    int(permute), as_.data_ptr(),
+                                                    None if Os is None else Os.data_ptr(), None)
 
 
 def test_static_matches_allocating_entry_point_twice(cuda):
@@ -64,3 +65,51 @@ def test_static_rejects_oversize_and_degenerate(cuda):
     ok = torch.zeros(100, dtype=torch.float64, device="cuda")
     assert _static_call(ok, a, 1, o1, o2) == N.BPF_OK
     np.testing.assert_array_equal(o1.cpu().numpy(), np.arange(100))
+
+
+def test_static_built_in_offset_and_no_offspring_output(cuda):
+    """Without a caller-supplied offset the library draws it from its own
+    generator (the allocating entry point draws the same one), and without
+    an Os buffer the cumulative offspring stay in the scratch array."""
+    import torch
+    from libbi_b200 import SystematicResampler
+    from libbi_b200 import _native as N
+
+    ref = SystematicResampler(max_n=N.BPF_STATIC_MAX_PARTICLES)
+    rng = np.random.default_rng(5)
+    for n in (40000, 513):
+        lw = torch.as_tensor(rng.standard_normal(n) * 2.0, device="cuda", dtype=torch.float64)
+        as_ = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+        assert _static_call(lw, None, 1, as_, None) == N.BPF_OK
+        want = ref.ancestors(lw, None, permute=True)
+        np.testing.assert_array_equal(as_.cpu().numpy(), want.cpu().numpy())
+    ref.close()
+
+
+def test_static_matches_reference_golden_vectors(cuda, oracle, golden):
+    """Tied to the reference's own output, not only to the other CUDA entry
+    point: the golden cases that the reference's resampler code produced
+    (cumulative offspring, permuted and sorted ancestors on the same
+    offsets), for every case within the static limit."""
+    import torch
+    from libbi_b200 import _native as N
+    from tests.golden.make_golden import UNIFORM_SEED
+
+    checked = 0
+    for name, c in golden.items():
+        lw = c["lw"]
+        n = lw.size
+        if n > N.BPF_STATIC_MAX_PARTICLES:
+            continue
+        a = oracle.resample_uniforms(0, n, 0, UNIFORM_SEED, int(c["step"][0]))
+        lw_d = torch.as_tensor(lw, device="cuda", dtype=torch.float64)
+        a_d = torch.as_tensor(a, device="cuda", dtype=torch.float64)
+        as_ = torch.empty(n, dtype=torch.int32, device="cuda")
+        Os = torch.empty(n, dtype=torch.int32, device="cuda")
+        assert _static_call(lw_d, a_d, 1, as_, Os) == N.BPF_OK, name
+        np.testing.assert_array_equal(Os.cpu().numpy(), c["Os"], err_msg=name)
+        np.testing.assert_array_equal(as_.cpu().numpy(), c["sys_perm"], err_msg=name)
+        assert _static_call(lw_d, a_d, 0, as_, Os) == N.BPF_OK, name
+        np.testing.assert_array_equal(as_.cpu().numpy(), c["sys_sorted"], err_msg=name)
+        checked += 1
+    assert checked >= 10
