@@ -90,7 +90,7 @@ __global__ void k_batch_pz_init(T* x, int ld, double* lw, const BatchFilter* fil
 // transitions: the single-filter bodies, indexed through the block's filter
 // ---------------------------------------------------------------------------
 template <class T, int D>
-__global__ void __launch_bounds__(kL96Block, (sizeof(T) == 4 && D <= 40 ? 8 : 4))
+__global__ void __launch_bounds__(kL96Block, l96_min_blocks(sizeof(T)))
 k_batch_l96_transition(const T* __restrict__ x_in, T* __restrict__ x_out, int ld, int* __restrict__ as,
                        double* __restrict__ lw, const T* __restrict__ y, double t1d, double t2d, int step,
                        const BatchFilter* __restrict__ filt, const L96Params* __restrict__ prms,
@@ -242,6 +242,7 @@ __global__ void __launch_bounds__(NT, 1)
 k_batch_resample(const double* __restrict__ lw, int* __restrict__ as, const BatchFilter* __restrict__ filt,
                  const int* __restrict__ order, StepStats* stats, double* lu_buf, int* os_buf, int step) {
   extern __shared__ __align__(16) unsigned char s_raw[];
+  pdl_trigger();  // a single filter's transition, a programmatic dependent, may be scheduled
   const int f = order[blockIdx.x];
   const BatchFilter fd = filt[f];
   StepStats* st = stats + f;

@@ -5,6 +5,7 @@
 #include <stdint.h>
 #include "../../include/libbi_b200.h"
 #include "../../include/bpf_philox.h"
+#include "../../include/bpf_device.cuh"
 
 #define BPF_TRY(call)                                          \
   do {                                                         \
@@ -161,29 +162,7 @@ __device__ __forceinline__ double nan_max(double a, double b) {
   return a < b ? b : a;
 }
 
-// ---------------------------------------------------------------------------
-// Log-weight reduction (max, sum e, sum e^2) with e = nanexp(lw - max).
-// ---------------------------------------------------------------------------
-struct LwPartial {
-  double mx, s1, s2;
-};
-
-// Device-side results of a reduction / filter step.
-struct StepStats {
-  double mx;        // max log-weight
-  double s1, s2;    // sum e, sum e^2 with e = nanexp(lw - mx)
-  double ess;       // s1^2 / s2
-  double lW;        // mx + log s1 - log N
-  double ll;        // logLikelihood
-  double inc;       // logIncrement of the latest correct
-  int resample;     // next step resamples (ESS < essRel*N after an observed step)
-  int resampled;    // this step resampled
-  int status;       // BPF_OK / BPF_E_DEGENERATE / BPF_E_TIMEOUT
-  int step;         // schedule index of the latest correct (0 = initial)
-  double ess_rel;
-  int n;
-  int pad;
-};
+// LwPartial and StepStats: include/bpf_device.cuh
 
 // Scratch of the resampler pipeline for up to max_n particles.
 struct ResampleScratch {
@@ -290,6 +269,8 @@ struct TransitionArgs {
   uint64_t obs_mask = ~0ull;  // bit i: component i observed (when y is given)
 };
 int launch_transition(const ModelArgs& m, const TransitionArgs& a, cudaStream_t st);
+// the step statistics of a freshly initialised filter
+int launch_stats_init(StepStats* stats, int n, double ess_rel, cudaStream_t st);
 int launch_init(const ModelArgs& m, void* x, int ld, int n, double* lw, uint64_t seed,
                 StepStats* stats, double ess_rel, cudaStream_t st);
 

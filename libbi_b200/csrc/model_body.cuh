@@ -60,10 +60,14 @@ struct L96Params {
   double x0_mean, x0_std;
 };
 
-// Blocks of 64 threads, at most 128 registers each: 8 blocks fit an SM, so
-// N = 65536 particles (1024 blocks) run as a single wave on 148 SMs with 6 or
-// 7 blocks on every SM.
-constexpr int kL96Block = 64;
+// Blocks of 128 threads, at most 128 registers each (FP32): 4 blocks fit an
+// SM, so N = 65536 particles (512 blocks) run as a single wave on 148 SMs
+// with 3 or 4 blocks on every SM.  Against 64-thread blocks this halves the
+// block partials the last block combines (measured on B200 at N = 65536:
+// 34.5 against 36.3 us per transition).
+constexpr int kL96Block = 128;
+// resident blocks per SM the L96 kernels are compiled for (launch bounds)
+constexpr int l96_min_blocks(int esz) { return esz == 4 ? 512 / kL96Block : 256 / kL96Block; }
 // PZ: one particle per thread, 128-thread blocks
 constexpr int kPZBlock = 128;
 
@@ -329,33 +333,6 @@ inline PZParams pz_params(const double* theta, double h, double atoler, double r
   p.logsafe = (double)(T)std::log((T)0.9);
   p.expo = (double)((T)0.5 * (T)std::fma(-(T)0.04, (T)0.75, (T)0.2));
   return p;
-}
-
-// ---------------------------------------------------------------------------
-// the end of every transition block: this block's (max, sum e, sum e^2) to
-// partials[pidx]; the last of the np blocks that share `counter` combines
-// partials[pbase .. pbase + np) and writes the step statistics.  Returns true
-// in the block that finalised.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ bool transition_reduce_tail(LwPartial part, LwPartial* partials, int pidx, int pbase,
-                                                       int np, unsigned* counter, int n, StepStats* st, bool ok,
-                                                       int resampled, bool observed) {
-  part = block_combine(part);
-  if (threadIdx.x == 0) partials[pidx] = part;
-  __shared__ bool am_last;
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) am_last = atomicAdd(counter, 1u) == (unsigned)np - 1;
-  __syncthreads();
-  if (am_last) {
-    __threadfence();
-    if (ok) {
-      finalize_partials(partials + pbase, np, n, st, kFinalizeStep, observed);
-      if (threadIdx.x == 0) st->resampled = resampled;
-    }
-    if (threadIdx.x == 0) *counter = 0;
-  }
-  return am_last;
 }
 
 }  // namespace bpf

@@ -424,6 +424,7 @@ __global__ void __launch_bounds__(kBlock)
 k_systematic_coop(const double* __restrict__ lw, int n, StepStats* st, const double* a_in, uint64_t seed, int step,
                   int* Os, int* as, int* marks, int* slot, unsigned long long* qbuf, u128* block_w, int* block_z, int* block_m,
                   unsigned* bar_counter, unsigned* bar_gen, const int* gate) {
+  pdl_trigger();  // as in k_systematic_coop1
   if (gate_closed(gate, st)) return;
   constexpr int NW = kBlock / 32;
   constexpr int S = 32 * IT;  // particles per segment
@@ -734,6 +735,9 @@ __global__ void __launch_bounds__(NT)
 k_systematic_coop1(const double* __restrict__ lw, int n, StepStats* st, const double* a_in, uint64_t seed,
                    int step, int* Os_out, int* as, int* E, int* ecoarse, int coarse_shift, int* slot,
                    u128* block_w, int* block_z, unsigned* bar_counter, unsigned* bar_gen, const int* gate) {
+  // the next kernel (the transition, a programmatic dependent) may be
+  // scheduled now; it waits for this kernel's completion before it reads
+  pdl_trigger();
   if (gate_closed(gate, st)) return;
   extern __shared__ int s_coarse[];
   __shared__ int s_last[NT];
