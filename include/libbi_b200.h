@@ -118,6 +118,63 @@ int bpf_create(const bpf_model_desc* model, const bpf_config* config, bpf_handle
 /* Release all device memory of the handle. */
 int bpf_destroy(bpf_handle* h);
 
+/* ---- models compiled outside the library ------------------------------- */
+/* LibBi generates a Model class per .bi file and instantiates the filter
+ * templates on it (share/tt/cpp/model.hpp.tt:95-510; the block updaters of
+ * share/tt/cpp/block/ode.hpp.tt:39-54 and pdf_.hpp.tt:46-75, which call
+ * RK4Integrator<B,S>::update, RK43Integrator<B,S>::update,
+ * StaticSampler<B,S>::samples and SparseStaticLogDensity<B,S>::logDensities).
+ * A model class of that shape, compiled by the caller with nvcc against
+ * include/bpf_model.cuh, yields this table of launchers (bpf::model_ops<B>),
+ * and the library's filter drives it exactly as it drives its built-in
+ * models: resampling, the log-weight reduction, steps, checkpoints and path
+ * output are the library's.  The launchers enqueue on `stream` and return
+ * BPF_OK, BPF_E_INVALID or BPF_E_CUDA. */
+typedef struct {
+  const void* x_in;   /* state before the step: dim columns, SoA, leading dimension ld */
+  void* x_out;        /* state after the step */
+  int ld, n;
+  int* ancestors;     /* read (gather) and rewritten when the step resamples */
+  double* lw;         /* FP64 log-weights, updated in place */
+  const void* y;      /* device observation (nobs values) or NULL (unobserved step) */
+  uint64_t obs_mask;  /* bit j: observed element j (every bit set for a full observation) */
+  double t1, t2;
+  uint64_t seed;
+  int step;           /* schedule index of the observation (random stream address) */
+  const double* params;  /* host, nparams values: the model's parameters */
+  int nparams;
+  void* stats;        /* the step statistics the kernel's last block finalises (bpf_device.cuh) */
+  void* partials;     /* one bpf::LwPartial per block */
+  int max_partials;   /* capacity of partials */
+  unsigned* counter;  /* last-block ticket, zero on entry and on exit */
+} bpf_transition_args;
+
+typedef struct {
+  void* x;            /* state to draw: dim columns, SoA, leading dimension ld */
+  int ld, n;
+  double* lw;         /* set to zero */
+  uint64_t seed;
+  const double* params;
+  int nparams;
+} bpf_init_args;
+
+typedef struct {
+  int dim;            /* state columns per particle (D_VAR then DX_VAR elements) */
+  int nobs;           /* observed elements per observation, at most 64 */
+  int nparams;        /* parameters (P_VAR elements) */
+  int precision;      /* BPF_F32 or BPF_F64: the state and observation type */
+  int (*init)(const bpf_init_args* a, void* stream);
+  int (*transition)(const bpf_transition_args* a, void* stream);
+} bpf_model_ops;
+
+/* bpf_create for a model compiled outside the library: ops from
+ * bpf::model_ops<Model>() (include/bpf_model.cuh), params the model's
+ * nparams parameter values (host; copied).  The handle supports every
+ * single-filter entry point except bpf_set_proposal.  Replaces the same
+ * construction as bpf_create (share/tt/cpp/client/filter_cpu.cpp.tt:105-184)
+ * for a model LibBi would generate. */
+int bpf_create_model(const bpf_model_ops* ops, const double* params, const bpf_config* config, bpf_handle** out);
+
 /* Device pointers of the particle store.  x: structure of arrays, component j
  * of particle p at x[j*ld + p] in the model precision (State Xdn, column-major,
  * share/src/bi/state/State.hpp:73-462); lw: N log-weights in FP64

@@ -16,7 +16,9 @@
  *   bi_b200::ParticleFilterDegeneratedException
  *       (share/src/bi/misc/exception.hpp:47)
  * The models are the two built into the library (ModelL96, ModelPZ) with
- * the constants of their .bi files.  Every call goes through the C ABI; the
+ * the constants of their .bi files, or a model class in the shape LibBi's
+ * code generator emits, compiled by the caller against bpf_model.cuh and
+ * wrapped as DeviceModel<Model>.  Every call goes through the C ABI; the
  * particles stay in device memory.  Errors throw: a degenerate filter throws
  * ParticleFilterDegeneratedException as the reference does, any other
  * status BpfError. */
@@ -109,6 +111,25 @@ struct ModelPZ {
   int nobs() const { return 1; }
   size_t esz() const { return 8; }
 };
+
+/* A model B is either one of the two built into the library (desc() gives
+ * its bpf_model_desc) or a model class compiled by the caller against
+ * bpf_model.cuh, wrapped as bi_b200::DeviceModel<Model> (ops() gives its
+ * bpf_model_ops table, params its parameter values). */
+template <class M>
+auto create_handle(const M& m, const bpf_config& c, bpf_handle** h, int) -> decltype(m.desc(), int()) {
+  bpf_model_desc d = m.desc();
+  return bpf_create(&d, &c, h);
+}
+template <class M>
+auto create_handle(const M& m, const bpf_config& c, bpf_handle** h, long) -> decltype(m.ops(), int()) {
+  bpf_model_ops o = m.ops();
+  return bpf_create_model(&o, m.params.empty() ? nullptr : m.params.data(), &c, h);
+}
+template <class M>
+auto model_dim(const M& m, int) -> decltype(m.desc(), int()) { return m.desc().dim; }
+template <class M>
+auto model_dim(const M& m, long) -> decltype(m.ops(), int()) { return m.ops().dim; }
 
 /* ---- random numbers ----------------------------------------------------- */
 /* The reference's Random holds generator state; here every draw is a
@@ -293,7 +314,6 @@ class BootstrapPFState {
     essRel_ = essRel;
     msteps_ = msteps;
     seed_ = seed;
-    bpf_model_desc d = m_.desc();
     bpf_config c{};
     c.nparticles = N_;
     c.resampler = kind;
@@ -301,7 +321,7 @@ class BootstrapPFState {
     c.ess_rel = essRel;
     c.seed = seed;
     c.stream = stream_;
-    check(bpf_create(&d, &c, &h_), "bpf_create");
+    check(create_handle(m_, c, &h_, 0), "bpf_create");
   }
 
  private:
@@ -385,10 +405,11 @@ class BootstrapPF {
    * before the run (recordPath); path: len x dim, oldest first */
   template <class S1>
   int samplePath(Random&, S1& s, std::vector<typename B::real>& path, int* particle = nullptr) {
-    path.assign((size_t)(cap_ + 1) * m_.desc().dim, (typename B::real)0);
+    const int dim = model_dim(m_, 0);
+    path.assign((size_t)(cap_ + 1) * dim, (typename B::real)0);
     int len = 0, p = 0;
     check(bpf_sample_path(s.handle(), nullptr, path.data(), &p, &len), "BootstrapPF::samplePath");
-    path.resize((size_t)len * m_.desc().dim);
+    path.resize((size_t)len * dim);
     if (particle) *particle = p;
     return len;
   }

@@ -6,7 +6,7 @@ reference's filter/resampler classes.
 """
 from ._native import (BpfError, ParticleFilterDegeneratedException, load_library,  # noqa: F401
                       LIB_PATH, EXPORTS)
-from .filter import (BootstrapPF, ModelL96, ModelPZ, Resampler, SystematicResampler,  # noqa: F401
+from .filter import (BootstrapPF, ModelL96, ModelPZ, ExternalModel, Resampler, SystematicResampler,  # noqa: F401
                      MultinomialResampler, MetropolisResampler, gather_rows, StepResult, BatchedBootstrapPF,
                      autotune_resampler)
 from .sampler import MarginalMH, Prior, smc2  # noqa: F401
@@ -15,6 +15,6 @@ from .schedule import Observer, Schedule, ScheduleElement  # noqa: F401
 from .replicas import sharded_batch_filter  # noqa: F401
 from . import configs  # noqa: F401
 
-__all__ = ["BootstrapPF", "ModelL96", "ModelPZ", "Resampler", "SystematicResampler", "MultinomialResampler",
+__all__ = ["BootstrapPF", "ModelL96", "ModelPZ", "ExternalModel", "Resampler", "SystematicResampler", "MultinomialResampler",
            "MetropolisResampler", "BatchedBootstrapPF", "MarginalMH", "Prior", "smc2", "LearnedProposal", "Observer", "Schedule",
            "ScheduleElement", "gather_rows", "autotune_resampler", "BpfError", "ParticleFilterDegeneratedException", "configs"]

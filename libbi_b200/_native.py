@@ -51,7 +51,7 @@ EXPORTS = (
     "bpf_proposal_create", "bpf_proposal_destroy", "bpf_proposal_set_data", "bpf_proposal_train",
     "bpf_proposal_loss_grad", "bpf_proposal_params", "bpf_proposal_set_params", "bpf_set_proposal",
     "bpf_batch_set_proposal",
-    "bpf_path_cache", "bpf_sample_path", "bpf_step_sparse", "bpf_smc2_run", "bpf_debug_set_wait_limit",
+    "bpf_path_cache", "bpf_sample_path", "bpf_step_sparse", "bpf_smc2_run", "bpf_debug_set_wait_limit", "bpf_create_model",
 )
 
 
@@ -104,6 +104,14 @@ RESAMPLE_SHAPES = 6  # BPF_RESAMPLE_SHAPES
 
 class TuneResult(ctypes.Structure):
     _fields_ = [("shape", ctypes.c_int), ("us", ctypes.c_double * RESAMPLE_SHAPES)]
+
+
+class ModelOps(ctypes.Structure):
+    """bpf_model_ops: the launchers of a model compiled outside the library."""
+    _fields_ = [
+        ("dim", c_int), ("nobs", c_int), ("nparams", c_int), ("precision", c_int),
+        ("init", c_void_p), ("transition", c_void_p),
+    ]
 
 
 class StepOut(ctypes.Structure):
@@ -196,6 +204,7 @@ def _declare(L):
         "bpf_systematic_ancestors_static": (c_int, [c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p,
                                                     c_void_p]),
         "bpf_debug_set_wait_limit": (c_int, [c_longlong]),
+        "bpf_create_model": (c_int, [POINTER(ModelOps), c_void_p, POINTER(Config), POINTER(H)]),
         "bpf_version": (c_char_p, []),
         "bpf_status_string": (c_char_p, [c_int]),
     }

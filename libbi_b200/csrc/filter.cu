@@ -25,6 +25,11 @@ void bpf_set_last_cuda_error(cudaError_t e) { g_last_cuda_error = e; }
 
 struct bpf_handle {
   bpf::ModelArgs model;
+  // a model compiled outside the library (bpf_create_model): its launchers
+  // and parameters; model.kind is 0 then
+  bool custom = false;
+  bpf_model_ops ops{};
+  std::vector<double> params;
   bpf_config cfg;
   int n = 0, ld = 0, dim = 0, esz = 0;
   void* x[2] = {nullptr, nullptr};
@@ -99,7 +104,36 @@ int check_model(const bpf_model_desc* m) {
 }
 
 // observed values per observation: every component for L96, log P for PZ
-int nobs(const bpf_handle* h) { return h->model.kind == BPF_MODEL_L96 ? h->dim : 1; }
+int nobs(const bpf_handle* h) {
+  if (h->custom) return h->ops.nobs;
+  return h->model.kind == BPF_MODEL_L96 ? h->dim : 1;
+}
+
+// the step's transition: the built-in model's fused kernel, or the
+// launcher of a model compiled outside the library
+int launch_model_transition(bpf_handle* h, const bpf::TransitionArgs& ta) {
+  if (!h->custom) return bpf::launch_transition(h->model, ta, h->stream);
+  bpf_transition_args a{};
+  a.x_in = ta.x_in;
+  a.x_out = ta.x_out;
+  a.ld = ta.ld;
+  a.n = ta.n;
+  a.ancestors = const_cast<int*>(ta.as);
+  a.lw = ta.lw;
+  a.y = ta.y;
+  a.obs_mask = ta.obs_mask;
+  a.t1 = ta.t1;
+  a.t2 = ta.t2;
+  a.seed = ta.seed;
+  a.step = ta.step;
+  a.params = h->params.empty() ? nullptr : h->params.data();
+  a.nparams = (int)h->params.size();
+  a.stats = ta.stats;
+  a.partials = ta.partials;
+  a.max_partials = ta.max_partials;
+  a.counter = ta.counter;
+  return h->ops.transition(&a, h->stream);
+}
 
 int ensure_y(bpf_handle* h, size_t bytes) {
   if (bytes <= h->y_cap) return BPF_OK;
@@ -247,7 +281,7 @@ int enqueue_step(bpf_handle* h, double t1, double t2, const void* y_dev, uint64_
   ta.max_partials = h->rs.max_partials;
   ta.counter = h->rs.counters + 4;
   ta.obs_mask = mask;
-  rc = bpf::launch_transition(h->model, ta, h->stream);
+  rc = launch_model_transition(h, ta);
   if (rc) return rc;
   if (h->timing) {
     rc = timing_event(h, 2);
@@ -328,35 +362,26 @@ const char* bpf_status_string(int s) {
   }
 }
 
-int bpf_create(const bpf_model_desc* model, const bpf_config* config, bpf_handle** out) {
-  if (!out || !config) return BPF_E_INVALID;
-  *out = nullptr;
-  int rc = check_model(model);
-  if (rc) return rc;
-  if (config->nparticles <= 0) return BPF_E_INVALID;
+static int check_config(const bpf_config* config) {
+  if (!config || config->nparticles <= 0) return BPF_E_INVALID;
   if (config->resampler < BPF_RESAMPLER_SYSTEMATIC || config->resampler > BPF_RESAMPLER_METROPOLIS)
     return BPF_E_INVALID;
   if (config->resampler == BPF_RESAMPLER_METROPOLIS && config->metropolis_steps < 0) return BPF_E_INVALID;
   // Resampler constructor pre-condition, share/src/bi/resampler/Resampler.hpp:129
   if (!(config->ess_rel >= 0.0 && config->ess_rel <= 1.0)) return BPF_E_INVALID;
-  bpf_handle* h = new (std::nothrow) bpf_handle();
-  if (!h) return BPF_E_NOMEM;
-  h->model.kind = model->kind;
-  h->model.dim = model->dim;
-  h->model.precision = model->precision;
-  h->model.integrator = model->integrator;
-  h->model.h = model->h;
-  h->model.atoler = model->atoler;
-  h->model.rtoler = model->rtoler;
-  for (int i = 0; i < BPF_MAX_THETA; ++i) h->model.theta[i] = model->theta[i];
+  return BPF_OK;
+}
+
+// buffers, resampler and initial draw of a handle whose model fields are set
+static int create_common(bpf_handle* h, const bpf_config* config, int dim, int precision, bpf_handle** out) {
   h->cfg = *config;
   h->stream = (cudaStream_t)config->stream;
   h->n = config->nparticles;
   // leading dimension rounded up to 32 particles (State::roundup for CUDA,
   // share/src/bi/state/State.hpp:40-57), so every component row is 128-byte aligned
   h->ld = ((h->n + 31) / 32) * 32;
-  h->dim = model->dim;
-  h->esz = model->precision == BPF_F64 ? 8 : 4;
+  h->dim = dim;
+  h->esz = precision == BPF_F64 ? 8 : 4;
   const size_t xb = (size_t)h->ld * h->dim * h->esz;
   if (cudaMalloc(&h->x[0], xb) != cudaSuccess || cudaMalloc(&h->x[1], xb) != cudaSuccess ||
       cudaMalloc((void**)&h->lw, (size_t)h->ld * sizeof(double)) != cudaSuccess ||
@@ -364,7 +389,7 @@ int bpf_create(const bpf_model_desc* model, const bpf_config* config, bpf_handle
     bpf_destroy(h);
     return BPF_E_NOMEM;
   }
-  rc = bpf::scratch_alloc(h->rs, h->n);
+  int rc = bpf::scratch_alloc(h->rs, h->n);
   if (rc) { bpf_destroy(h); return rc; }
   if (cudaMallocHost((void**)&h->host_stats, sizeof(bpf::StepStats)) != cudaSuccess) {
     cudaGetLastError();
@@ -402,6 +427,45 @@ int bpf_create(const bpf_model_desc* model, const bpf_config* config, bpf_handle
   if (rc) { bpf_destroy(h); return rc; }
   *out = h;
   return BPF_OK;
+}
+
+int bpf_create(const bpf_model_desc* model, const bpf_config* config, bpf_handle** out) {
+  if (!out || !config) return BPF_E_INVALID;
+  *out = nullptr;
+  int rc = check_model(model);
+  if (rc) return rc;
+  if ((rc = check_config(config))) return rc;
+  bpf_handle* h = new (std::nothrow) bpf_handle();
+  if (!h) return BPF_E_NOMEM;
+  h->model.kind = model->kind;
+  h->model.dim = model->dim;
+  h->model.precision = model->precision;
+  h->model.integrator = model->integrator;
+  h->model.h = model->h;
+  h->model.atoler = model->atoler;
+  h->model.rtoler = model->rtoler;
+  for (int i = 0; i < BPF_MAX_THETA; ++i) h->model.theta[i] = model->theta[i];
+  return create_common(h, config, model->dim, model->precision, out);
+}
+
+int bpf_create_model(const bpf_model_ops* ops, const double* params, const bpf_config* config, bpf_handle** out) {
+  if (!out || !config || !ops) return BPF_E_INVALID;
+  *out = nullptr;
+  if (ops->dim <= 0 || ops->nobs < 0 || ops->nobs > 64 || ops->nparams < 0 || ops->nparams > 4096 ||
+      (ops->nparams > 0 && !params) || !ops->init || !ops->transition ||
+      (ops->precision != BPF_F32 && ops->precision != BPF_F64))
+    return BPF_E_INVALID;
+  int rc = check_config(config);
+  if (rc) return rc;
+  bpf_handle* h = new (std::nothrow) bpf_handle();
+  if (!h) return BPF_E_NOMEM;
+  h->custom = true;
+  h->ops = *ops;
+  if (ops->nparams > 0) h->params.assign(params, params + ops->nparams);
+  h->model.kind = 0;
+  h->model.dim = ops->dim;
+  h->model.precision = ops->precision;
+  return create_common(h, config, ops->dim, ops->precision, out);
 }
 
 int bpf_destroy(bpf_handle* h) {
@@ -579,8 +643,22 @@ int bpf_init(bpf_handle* h) {
   // the last-block tickets and grid-barrier words start from zero (a
   // cooperative resampling that timed out can leave a barrier counter set)
   BPF_TRY(cudaMemsetAsync(h->rs.counters, 0, 16 * sizeof(unsigned), h->stream));
-  int rc = bpf::launch_init(h->model, h->x[0], h->ld, h->n, h->lw, h->cfg.seed, h->rs.stats, h->cfg.ess_rel,
-                            h->stream);
+  int rc;
+  if (h->custom) {
+    bpf_init_args a{};
+    a.x = h->x[0];
+    a.ld = h->ld;
+    a.n = h->n;
+    a.lw = h->lw;
+    a.seed = h->cfg.seed;
+    a.params = h->params.empty() ? nullptr : h->params.data();
+    a.nparams = (int)h->params.size();
+    rc = h->ops.init(&a, h->stream);
+    if (!rc) rc = bpf::launch_stats_init(h->rs.stats, h->n, h->cfg.ess_rel, h->stream);
+  } else {
+    rc = bpf::launch_init(h->model, h->x[0], h->ld, h->n, h->lw, h->cfg.seed, h->rs.stats, h->cfg.ess_rel,
+                          h->stream);
+  }
   if (rc) return rc;
   h->pc_len = 0;
   h->pc_full = false;

@@ -144,6 +144,36 @@ class ModelPZ:
         return d
 
 
+class ExternalModel:
+    """A model compiled outside the library: a model class in the shape of
+    LibBi's generated Model (share/tt/cpp/model.hpp.tt) built with nvcc
+    against include/bpf_model.cuh into a shared library that returns its
+    bpf_model_ops table from `symbol` (bpf::model_ops<Model>()).  params:
+    the model's parameter (P_VAR) values.  BootstrapPF drives it through
+    bpf_create_model exactly as it drives the built-in models."""
+
+    def __init__(self, library: str, symbol: str, params: Sequence[float] = (), name: str = ""):
+        self._lib = ctypes.CDLL(library)
+        f = getattr(self._lib, symbol)
+        f.restype = N.ModelOps
+        f.argtypes = []
+        self.ops = f()
+        self.params = np.ascontiguousarray(np.asarray(params, dtype=np.float64).reshape(-1))
+        if self.params.size != self.ops.nparams:
+            raise ValueError(f"the model takes {self.ops.nparams} parameters, got {self.params.size}")
+        self.name = name or symbol
+        self.dim = int(self.ops.dim)
+        self.precision = "f32" if self.ops.precision == N.BPF_F32 else "f64"
+
+    @property
+    def nobs(self) -> int:
+        return int(self.ops.nobs)
+
+    @property
+    def np_dtype(self):
+        return np.float32 if self.precision == "f32" else np.float64
+
+
 # ---------------------------------------------------------------------------
 # resamplers
 # ---------------------------------------------------------------------------
@@ -278,10 +308,17 @@ class BootstrapPF:
         cfg.ess_rel = ess_rel
         cfg.seed = seed
         cfg.stream = stream
-        self._desc = model.desc()
         self._cfg = cfg
         self._h = ctypes.c_void_p()
-        N.check(N.lib().bpf_create(ctypes.byref(self._desc), ctypes.byref(cfg), ctypes.byref(self._h)), "bpf_create")
+        if isinstance(model, ExternalModel):
+            self._desc = None
+            N.check(N.lib().bpf_create_model(ctypes.byref(model.ops), _ptr_np(model.params) if model.params.size
+                                             else None, ctypes.byref(cfg), ctypes.byref(self._h)),
+                    "bpf_create_model")
+        else:
+            self._desc = model.desc()
+            N.check(N.lib().bpf_create(ctypes.byref(self._desc), ctypes.byref(cfg), ctypes.byref(self._h)),
+                    "bpf_create")
 
     def close(self):
         if self._h:
