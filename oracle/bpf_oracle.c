@@ -463,9 +463,179 @@ static double pz_particle_d(const bpf_model_desc* m, double* x, const double* y,
   return l;
 }
 
+/* ------------------------------------------- models in the generated form
+ *
+ * Two models written as LibBi's code generator renders them and compiled by
+ * nvcc against include/bpf_model.cuh with -fmad=false (tests/cpp/): every
+ * expression of the model source in its source order, no contraction, the
+ * integrators' own arithmetic as in the built-in kernels.  The oracle kinds
+ * below restate them for the oracle's filter loop:
+ *   ORC_MODEL_TEST_AR1  the reference's Test.bi (AR(1)) plus an observation,
+ *                       tests/cpp/model_test_ar1.cuh: theta = {theta, sigma2}
+ *   ORC_MODEL_L96_GEN   Lorenz '96 in the generated form,
+ *                       tests/cpp/model_l96_generated.cuh:
+ *                       theta = {F, sigma_eta, sigma_y, x0 mean, x0 std}
+ * Normal i of a particle's step is the i-th of the stream the built-in models
+ * use (block i/4, Box-Muller pairs), rng.gaussian(mu, sigma) = mu + sigma*z
+ * with the product rounded first. */
+#define ORC_MODEL_TEST_AR1 101
+#define ORC_MODEL_L96_GEN 102
+
+static void gen_normals_f(uint64_t seed, uint32_t p, int step, uint32_t tag, int n, float* z) {
+  for (int b = 0; b < (n + 3) / 4; ++b) {
+    bpf_u32x4 r = bpf_draw(seed, p, (uint32_t)step, (uint32_t)b, tag);
+    float f[4];
+    bpf_normal_pair_f(r.v[0], r.v[1], &f[0], &f[1]);
+    bpf_normal_pair_f(r.v[2], r.v[3], &f[2], &f[3]);
+    for (int j = 0; j < 4 && 4 * b + j < n; ++j) z[4 * b + j] = f[j];
+  }
+}
+
+static void gen_normals_d(uint64_t seed, uint32_t p, int step, uint32_t tag, int n, double* z) {
+  for (int b = 0; b < (n + 3) / 4; ++b) {
+    bpf_u32x4 r = bpf_draw(seed, p, (uint32_t)step, (uint32_t)b, tag);
+    double f[4];
+    bpf_normal_pair_d(r.v[0], r.v[1], &f[0], &f[1]);
+    bpf_normal_pair_d(r.v[2], r.v[3], &f[2], &f[3]);
+    for (int j = 0; j < 4 && 4 * b + j < n; ++j) z[4 * b + j] = f[j];
+  }
+}
+
+/* y ~ gaussian(mu, sigma): -0.5*pow((y - mu)/sigma, 2) - BI_HALF_LOG_TWO_PI - log(sigma)
+ * (share/tt/cpp/action/gaussian.hpp.tt:58-69) in source order */
+static float gen_gauss_term_f(float y, float mu, float sigma) {
+  float a = (y - mu) / sigma;
+  float c = a * a;
+  float d = -0.5f * c;
+  float e = d - (float)HALF_LOG_TWO_PI;
+  return e - bpf_logf(sigma);
+}
+
+static double gen_gauss_term_d(double y, double mu, double sigma) {
+  double a = (y - mu) / sigma;
+  double c = a * a;
+  double d = -0.5 * c;
+  double e = d - HALF_LOG_TWO_PI;
+  return e - bpf_log(sigma);
+}
+
+/* AR(1): w ~ gaussian(0, sqrt(sigma2)); x <- theta*x + w; y ~ gaussian(x, 0.5) */
+static double ar1_particle(const bpf_model_desc* m, void* xv, const void* y, uint64_t seed, int step, uint32_t p,
+                           double base, uint64_t mask) {
+  double l = base;
+  if (m->precision == BPF_F32) {
+    float* x = (float*)xv;
+    float z;
+    gen_normals_f(seed, p, step, BPF_RNG_NOISE, 1, &z);
+    const float theta = (float)m->theta[0], sigma2 = (float)m->theta[1];
+    const float sigma = sqrtf(sigma2);
+    const float w = 0.0f + sigma * z;
+    x[0] = theta * x[0] + w;
+    if (y && (mask & 1u)) l += (double)gen_gauss_term_f(((const float*)y)[0], x[0], 0.5f);
+  } else {
+    double* x = (double*)xv;
+    double z;
+    gen_normals_d(seed, p, step, BPF_RNG_NOISE, 1, &z);
+    const double theta = m->theta[0], sigma2 = m->theta[1];
+    const double sigma = sqrt(sigma2);
+    const double w = 0.0 + sigma * z;
+    x[0] = theta * x[0] + w;
+    if (y && (mask & 1u)) l += gen_gauss_term_d(((const double*)y)[0], x[0], 0.5);
+  }
+  return l;
+}
+
+/* Lorenz '96 in the generated form: noise block, RK4 over the dfdt action
+ * (x[n+1] - x[n-2])*x[n-1] - x[n] + F in source order, x <- x + eta,
+ * observation terms gaussian(x, sigma_y) */
+#define L96GEN_DFDT(REAL, X, K)                                                               \
+  for (int i = 0; i < D; ++i) {                                                               \
+    REAL a = X[(i + 1) % D] - X[(i + D - 2) % D];                                             \
+    REAL b = a * X[(i + D - 1) % D];                                                          \
+    REAL c = b - X[i];                                                                        \
+    K[i] = c + F;                                                                             \
+  }
+#define L96GEN_RK4(REAL, FMA, X)                                                              \
+  {                                                                                           \
+    const REAL b1 = (REAL)(1.0 / 6.0), b2 = (REAL)(1.0 / 3.0), b3 = (REAL)(1.0 / 3.0),        \
+               b4 = (REAL)(1.0 / 6.0);                                                        \
+    REAL xs[64], k[64], acc[64];                                                              \
+    const REAL t2 = (REAL)t2d;                                                                \
+    REAL t = (REAL)t1d, h = (REAL)m->h;                                                       \
+    while (t < t2) {                                                                          \
+      if (FMA((REAL)1.01, h, t) - t2 > (REAL)0) {                                             \
+        h = t2 - t;                                                                           \
+        if (h <= (REAL)0) { t = t2; break; }                                                  \
+      }                                                                                       \
+      const REAL hh = (REAL)0.5 * h;                                                          \
+      L96GEN_DFDT(REAL, X, k)                                                                 \
+      for (int i = 0; i < D; ++i) { acc[i] = b1 * k[i]; xs[i] = FMA(hh, k[i], X[i]); }        \
+      L96GEN_DFDT(REAL, xs, k)                                                                \
+      for (int i = 0; i < D; ++i) { acc[i] = FMA(b2, k[i], acc[i]); xs[i] = FMA(hh, k[i], X[i]); } \
+      L96GEN_DFDT(REAL, xs, k)                                                                \
+      for (int i = 0; i < D; ++i) { acc[i] = FMA(b3, k[i], acc[i]); xs[i] = FMA(h, k[i], X[i]); } \
+      L96GEN_DFDT(REAL, xs, k)                                                                \
+      for (int i = 0; i < D; ++i) { acc[i] = FMA(b4, k[i], acc[i]); X[i] = FMA(h, acc[i], X[i]); } \
+      t += h;                                                                                 \
+    }                                                                                         \
+  }
+
+static double l96gen_particle(const bpf_model_desc* m, void* xv, const void* y, double t1d, double t2d,
+                              uint64_t seed, int step, uint32_t p, double base, uint64_t mask) {
+  const int D = m->dim;
+  double l = base;
+  if (m->precision == BPF_F32) {
+    float* x = (float*)xv;
+    const float F = (float)m->theta[0], se = (float)m->theta[1], sy = (float)m->theta[2];
+    float eta[64];
+    gen_normals_f(seed, p, step, BPF_RNG_NOISE, D, eta);
+    for (int i = 0; i < D; ++i) eta[i] = 0.0f + se * eta[i];
+    L96GEN_RK4(float, fmaf, x)
+    for (int i = 0; i < D; ++i) x[i] = x[i] + eta[i];
+    if (y)
+      for (int i = 0; i < D; ++i)
+        if ((mask >> i) & 1u) l += (double)gen_gauss_term_f(((const float*)y)[i], x[i], sy);
+  } else {
+    double* x = (double*)xv;
+    const double F = m->theta[0], se = m->theta[1], sy = m->theta[2];
+    double eta[64];
+    gen_normals_d(seed, p, step, BPF_RNG_NOISE, D, eta);
+    for (int i = 0; i < D; ++i) eta[i] = 0.0 + se * eta[i];
+    L96GEN_RK4(double, fma, x)
+    for (int i = 0; i < D; ++i) x[i] = x[i] + eta[i];
+    if (y)
+      for (int i = 0; i < D; ++i)
+        if ((mask >> i) & 1u) l += gen_gauss_term_d(((const double*)y)[i], x[i], sy);
+  }
+  return l;
+}
+#undef L96GEN_RK4
+#undef L96GEN_DFDT
+
+static int is_gen_kind(int kind) { return kind == ORC_MODEL_TEST_AR1 || kind == ORC_MODEL_L96_GEN; }
+
+/* initial draw of a generated-form model: AR(1) x ~ gaussian();
+ * Lorenz '96 x[i] ~ gaussian(x0 mean, x0 std) */
+static void gen_init_particle(const bpf_model_desc* m, void* x, int ld, uint32_t p, uint64_t seed) {
+  const int D = m->dim;
+  const double mu = m->kind == ORC_MODEL_TEST_AR1 ? 0.0 : m->theta[3];
+  const double sd = m->kind == ORC_MODEL_TEST_AR1 ? 1.0 : m->theta[4];
+  if (m->precision == BPF_F32) {
+    float z[64];
+    gen_normals_f(seed, p, 0, BPF_RNG_INIT, D, z);
+    for (int i = 0; i < D; ++i) ((float*)x)[(size_t)i * ld + p] = (float)mu + (float)sd * z[i];
+  } else {
+    double z[64];
+    gen_normals_d(seed, p, 0, BPF_RNG_INIT, D, z);
+    for (int i = 0; i < D; ++i) ((double*)x)[(size_t)i * ld + p] = mu + sd * z[i];
+  }
+}
+
 /* initial draw of particle p (Model::initialSamples) */
 static void init_particle(const bpf_model_desc* m, void* x, int ld, uint32_t p, uint64_t seed) {
-  if (m->kind == BPF_MODEL_L96) {
+  if (is_gen_kind(m->kind)) {
+    gen_init_particle(m, x, ld, p, seed);
+  } else if (m->kind == BPF_MODEL_L96) {
     for (int b = 0; b < (m->dim + 3) / 4; ++b) {
       bpf_u32x4 r = bpf_draw(seed, p, 0u, (uint32_t)b, BPF_RNG_INIT);
       if (m->precision == BPF_F32) {
@@ -511,7 +681,15 @@ void orc_transition_mask(const bpf_model_desc* m, const void* x_in, void* x_out,
   for (int p = 0; p < n; ++p) {
     const int src = resampled ? as[p] : p;
     const double base = resampled ? ll : lw[p];
-    if (m->precision == BPF_F32) {
+    if (is_gen_kind(m->kind)) {
+      double xp[64];
+      const size_t esz = m->precision == BPF_F32 ? 4 : 8;
+      for (int i = 0; i < D; ++i) memcpy((char*)xp + i * esz, (const char*)x_in + ((size_t)i * ld + src) * esz, esz);
+      lw[p] = m->kind == ORC_MODEL_TEST_AR1
+                  ? ar1_particle(m, xp, y, seed, step, (uint32_t)p, base, mask)
+                  : l96gen_particle(m, xp, y, t1, t2, seed, step, (uint32_t)p, base, mask);
+      for (int i = 0; i < D; ++i) memcpy((char*)x_out + ((size_t)i * ld + p) * esz, (char*)xp + i * esz, esz);
+    } else if (m->precision == BPF_F32) {
       float xp[64];
       for (int i = 0; i < D; ++i) xp[i] = ((const float*)x_in)[(size_t)i * ld + src];
       lw[p] = l96_particle_f(m, xp, (const float*)y, t1, t2, seed, step, (uint32_t)p, base, mask);
@@ -544,7 +722,7 @@ void orc_transition(const bpf_model_desc* m, const void* x_in, void* x_out, int 
 int orc_filter(const bpf_model_desc* m, const bpf_config* cfg, int T, double t0, double dt, const void* y,
                double* inc, double* ess_out, int* resampled_out, double* ll_out, void* x_final, double* lw_final) {
   const int n = cfg->nparticles, D = m->dim;
-  const int nobs = m->kind == BPF_MODEL_L96 ? D : 1;
+  const int nobs = m->kind == BPF_MODEL_L96 || m->kind == ORC_MODEL_L96_GEN ? D : 1;
   const int ld = ((n + 31) / 32) * 32;
   const size_t esz = m->precision == BPF_F64 ? 8 : 4;
   void* xa = calloc((size_t)ld * D, esz);
