@@ -68,6 +68,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <type_traits>
+#include <stdexcept>
 #include <vector>
 
 #include "libbi_b200.h"
@@ -127,8 +128,9 @@ template <int REPS, class L, class R> struct tree_node {};
  * structure-of-arrays buffers in device memory.  x: D_VAR then DX_VAR
  * columns, element j of particle p at x[j * ld + p]; r: R_VAR columns
  * likewise; prm: the P_VAR values (shared by all particles); y: the O_VAR
- * values of the current observation.  seed and step address the random
- * draws.  Inside the fused kernel the action functions receive a State
+ * values of the current observation.  step addresses the random draws (the
+ * seed comes with the sampler's Random); stream: where the updaters below
+ * enqueue their kernels.  Inside the fused kernel the action functions receive a State
  * whose fields they do not use: every variable is fetched through pax and
  * x. */
 template <class B, Location L> class State;
@@ -140,8 +142,8 @@ template <class B> class State<B, ON_DEVICE> {
   const real* y = nullptr;
   int ld = 0;
   int n = 0;
-  uint64_t seed = 0;
   int step = 0;
+  cudaStream_t stream = 0;
   CUDA_FUNC_BOTH int size() const { return n; }
 };
 
@@ -820,6 +822,174 @@ inline bpf_model_ops model_ops() {
 }
 
 }  // namespace bpf
+
+/* ---- the block updaters, one kernel each ------------------------------------------ */
+namespace bpf {
+
+/* one particle's variables from / to a device State<B, ON_DEVICE> */
+template <class B, class T>
+__device__ __forceinline__ void load_state(ParticleVars<B, T>& v, const bi::State<B, bi::ON_DEVICE>& s, int p) {
+  v.r = nullptr;
+#pragma unroll
+  for (int j = 0; j < B::ND; ++j) v.d[j] = s.x[(size_t)j * s.ld + p];
+#pragma unroll
+  for (int j = 0; j < B::NDX; ++j) v.dx[j] = s.x[(size_t)(B::ND + j) * s.ld + p];
+#pragma unroll
+  for (int j = 0; j < B::NP; ++j) v.p[j] = s.prm[j];
+}
+
+template <class B, class T>
+__device__ __forceinline__ void load_noise(ParticleVars<B, T>& v, const bi::State<B, bi::ON_DEVICE>& s, int p,
+                                           T* smem) {
+  v.r = smem + threadIdx.x;
+  v.rstride = blockDim.x;
+  if (s.r) {
+#pragma unroll
+    for (int j = 0; j < B::NR; ++j) v.r[j * v.rstride] = s.r[(size_t)j * s.ld + p];
+  }
+}
+
+template <class B, class T>
+__device__ __forceinline__ void store_state(const ParticleVars<B, T>& v, const bi::State<B, bi::ON_DEVICE>& s, int p) {
+#pragma unroll
+  for (int j = 0; j < B::ND; ++j) s.x[(size_t)j * s.ld + p] = v.d[j];
+#pragma unroll
+  for (int j = 0; j < B::NDX; ++j) s.x[(size_t)(B::ND + j) * s.ld + p] = v.dx[j];
+  if (s.r) {
+#pragma unroll
+    for (int j = 0; j < B::NR; ++j) s.r[(size_t)j * s.ld + p] = v.r[j * v.rstride];
+  }
+}
+
+/* kind: 0 noise draws (StaticSampler), 1 deterministic update
+ * (StaticUpdater), 2 RK4, 3 RK4(3) */
+template <class B, class T, class S, int KIND>
+__global__ void __launch_bounds__(kModelBlock) k_block_update(bi::State<B, bi::ON_DEVICE> s, uint64_t seed,
+                                                              double t1, double t2, double h, double atoler,
+                                                              double rtoler) {
+  extern __shared__ unsigned char bpf_model_smem[];
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= s.n) return;
+  ParticleVars<B, T> v;
+  load_state<B, T>(v, s, p);
+  load_noise<B, T>(v, s, p, reinterpret_cast<T*>(bpf_model_smem));
+  VarAccess<B, T> acc{v};
+  if constexpr (KIND == 0) {
+    ParticleRng<T> rng(seed, (uint32_t)p, (uint32_t)s.step, s.step == 0 ? BPF_RNG_INIT : BPF_RNG_NOISE);
+    SampleVisit<B, T> f{s, acc, rng, p};
+    tree<S>::each(f);
+  } else if constexpr (KIND == 1) {
+    SimulateVisit<B, T> f{s, acc, p};
+    tree<S>::each(f);
+  } else if constexpr (KIND == 2) {
+    ode_rk4<B, T, S>(v, acc, s, p, t1, t2, h);
+  } else {
+    ode_rk43<B, T, S>(v, acc, s, p, t1, t2, h, atoler, rtoler);
+  }
+  store_state<B, T>(v, s, p);
+}
+
+template <class B, class T, class S>
+__global__ void __launch_bounds__(kModelBlock) k_block_log_density(bi::State<B, bi::ON_DEVICE> s, uint64_t mask,
+                                                                   double* lp) {
+  extern __shared__ unsigned char bpf_model_smem[];
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= s.n) return;
+  ParticleVars<B, T> v;
+  load_state<B, T>(v, s, p);
+  load_noise<B, T>(v, s, p, reinterpret_cast<T*>(bpf_model_smem));
+#pragma unroll
+  for (int j = 0; j < B::NO; ++j) v.o[j] = s.y[j];
+  VarAccess<B, T> acc{v};
+  double l = lp[p];
+  LogDensityVisit<B, T> f{s, acc, p, mask, l};
+  tree<S>::each(f);
+  lp[p] = l;
+}
+
+template <class B, class S, int KIND>
+inline void block_update(bi::State<B, bi::ON_DEVICE>& s, uint64_t seed, double t1, double t2, double h,
+                         double atoler, double rtoler) {
+  if (s.n <= 0) return;
+  const int blocks = (s.n + kModelBlock - 1) / kModelBlock;
+  k_block_update<B, real, S, KIND><<<blocks, kModelBlock, noise_smem_bytes<B>(), s.stream>>>(s, seed, t1, t2, h,
+                                                                                             atoler, rtoler);
+  if (cudaGetLastError() != cudaSuccess) throw std::runtime_error("block updater launch failed");
+}
+
+}  // namespace bpf
+
+namespace bi {
+
+/* The integrator constants the generated ode block sets before it integrates
+ * (bi_ode_set, share/src/bi/ode/IntegratorConstants.hpp:38-57, called from
+ * share/tt/cpp/block/ode.hpp.tt): the step h (initial step for RK4(3)) and
+ * the tolerances. */
+struct OdeConstants {
+  double h = 1.0e-2, atoler = 1.0e-3, rtoler = 1.0e-3;
+};
+inline OdeConstants& ode_constants() {
+  static OdeConstants c;
+  return c;
+}
+inline void bi_ode_set(double h, double atoler, double rtoler) {
+  ode_constants() = OdeConstants{h, atoler, rtoler};
+}
+
+/* StaticSampler<B,S>::samples (share/src/bi/updater/StaticSampler.hpp; block/pdf_.hpp.tt:46-75):
+ * draws the actions of S for every particle of s into their targets (R_VAR
+ * columns in s.r, D_VAR / DX_VAR columns in s.x), with the draws of the
+ * particle's step s.step (0: the initial block's stream) under rng.seed,
+ * the same numbers as the fused kernel's first noise block. */
+template <class B, class S>
+struct StaticSampler {
+  template <class R1>
+  static void samples(R1& rng, State<B, ON_DEVICE>& s) {
+    bpf::block_update<B, S, 0>(s, rng.seed, 0.0, 0.0, 0.0, 0.0, 0.0);
+  }
+};
+
+/* StaticUpdater<B,S>::update (block/eval_.hpp.tt): the deterministic actions of S */
+template <class B, class S>
+struct StaticUpdater {
+  static void update(State<B, ON_DEVICE>& s) { bpf::block_update<B, S, 1>(s, 0, 0.0, 0.0, 0.0, 0.0, 0.0); }
+};
+
+/* RK4Integrator<B,S>::update (share/src/bi/ode/RK4Integrator.hpp;
+ * block/ode.hpp.tt:39-54) from t1 to t2 with the step of bi_ode_set */
+template <class B, class S, class T1 = real>
+struct RK4Integrator {
+  static void update(const T1 t1, const T1 t2, State<B, ON_DEVICE>& s) {
+    const OdeConstants& c = ode_constants();
+    bpf::block_update<B, S, 2>(s, 0, (double)t1, (double)t2, c.h, c.atoler, c.rtoler);
+  }
+};
+
+/* RK43Integrator<B,S>::update (share/src/bi/ode/RK43Integrator.hpp) */
+template <class B, class S, class T1 = real>
+struct RK43Integrator {
+  static void update(const T1 t1, const T1 t2, State<B, ON_DEVICE>& s) {
+    const OdeConstants& c = ode_constants();
+    bpf::block_update<B, S, 3>(s, 0, (double)t1, (double)t2, c.h, c.atoler, c.rtoler);
+  }
+};
+
+/* SparseStaticLogDensity<B,S>::logDensities
+ * (share/src/bi/updater/SparseStaticLogDensity.hpp; block/pdf_.hpp.tt:46-75):
+ * adds each particle's observation terms to lp[p] (device, FP64), for the
+ * O_VAR elements whose bit is set in mask, the observed values in s.y */
+template <class B, class S>
+struct SparseStaticLogDensity {
+  static void logDensities(State<B, ON_DEVICE>& s, uint64_t mask, double* lp) {
+    if (s.n <= 0) return;
+    const int blocks = (s.n + bpf::kModelBlock - 1) / bpf::kModelBlock;
+    bpf::k_block_log_density<B, real, S><<<blocks, bpf::kModelBlock, bpf::noise_smem_bytes<B>(), s.stream>>>(
+        s, mask, lp);
+    if (cudaGetLastError() != cudaSuccess) throw std::runtime_error("log-density launch failed");
+  }
+};
+
+}  // namespace bi
 
 namespace bi_b200 {
 

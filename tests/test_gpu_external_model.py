@@ -190,3 +190,47 @@ def test_cpp_client_with_generated_model(cuda, model_libs, tmp_path):
     got = np.array([float(s) for s in out])
     assert got[0] == want["loglik"]
     np.testing.assert_array_equal(got[1:], want["log_increments"])
+
+
+@pytest.mark.parametrize("which,precision", [("l96", "float"), ("l96", "double"), ("ar1", "double")])
+def test_unfused_block_updaters_equal_the_fused_step(cuda, model_libs, which, precision):
+    """The bi:: block updaters of include/bpf_model.cuh (StaticSampler,
+    RK4Integrator, StaticUpdater, SparseStaticLogDensity on a device
+    State<B, ON_DEVICE>, one kernel each, called in the order of the
+    generated transition and observation blocks) give the fused step's
+    states and log-weights bit for bit, from the same initial particles."""
+    import ctypes
+
+    import torch
+    from libbi_b200 import BootstrapPF, ExternalModel
+
+    lib = ctypes.CDLL(model_libs[precision])
+    f = getattr(lib, f"test_{which}_unfused_step")
+    P = ctypes.c_void_p
+    f.argtypes = [P, P, ctypes.c_int, ctypes.c_int, P, P, ctypes.c_double, ctypes.c_double, ctypes.c_uint64,
+                  ctypes.c_int, P]
+    f.restype = ctypes.c_int
+    tdt = torch.float32 if precision == "float" else torch.float64
+    if which == "l96":
+        model = ExternalModel(model_libs[precision], "test_l96_ops", [8.0])
+        n, t1, t2, nr = 3000, 0.0, 0.05, 40
+        y = 8.0 + torch.randn(40, generator=torch.Generator().manual_seed(2), dtype=torch.float64)
+    else:
+        model = ExternalModel(model_libs[precision], "test_ar1_ops", [0.9, 0.25])
+        n, t1, t2, nr = 3000, 0.0, 1.0, 1
+        y = torch.tensor([0.3], dtype=torch.float64)
+    seed = 5
+    pf = BootstrapPF(model, n, ess_rel=0.0, seed=seed)
+    x0, _, _ = pf.state()
+    xs = x0.clone()
+    pf.step(t1, t2, y.numpy())
+    x1, lw1, _ = pf.state()
+    ld = xs.shape[1]
+    r = torch.zeros((nr, ld), dtype=tdt, device="cuda")
+    prm = torch.as_tensor(model.params, dtype=tdt, device="cuda")
+    yd = y.to(device="cuda", dtype=tdt)
+    lp = torch.zeros(n, dtype=torch.float64, device="cuda")
+    assert f(xs.data_ptr(), r.data_ptr(), ld, n, prm.data_ptr(), yd.data_ptr(), t1, t2, seed, 1, lp.data_ptr()) == 0
+    assert torch.equal(xs[:, :n], x1[:, :n])
+    assert torch.equal(lp, lw1)
+    pf.close()
