@@ -375,16 +375,29 @@ def pmmh_chains(iterations=20, nchains=128, nparticles=2048, T=100):
     }
 
 
-def precision_check(y_host, seeds=16, n=N_PARTICLES, T=T_OBS):
+def precision_check(y_host, seeds=16, n=N_PARTICLES, T=T_OBS, same_input_seeds=4):
     """The FP32 filter against the FP64 filter on the same seeds (identical
     Philox draws, so the two differ by rounding only), on the bench's
-    Lorenz-96 workload: per step the relative error of the log-likelihood
-    increment (relative to max(|inc64|, 1)) and of the cumulative
-    log-likelihood, the fraction of steps within 1e-4, the first step
-    beyond it, and whether the two estimators' means over the seeds agree
-    within two standard errors.  Lorenz-96 is chaotic, so rounding
-    differences grow along a run; the per-step columns show where."""
+    Lorenz-96 workload.
+
+    Along a run: per step the relative error of the FP32 filter's
+    log-likelihood increment against the FP64 filter's (relative to
+    max(|inc64|, 1)) and of the cumulative log-likelihood; the fraction of
+    steps within 1e-4; whether the two estimators' means over the seeds agree
+    within two standard errors.
+
+    From the same input, at EVERY step of the first `same_input_seeds` FP64
+    runs: the FP64 run's state and log-weights before the step are written
+    into an FP32 and an FP64 probe filter (same seed, so the same draws),
+    each takes that one step, and the increments are compared (relative to
+    the step's own increment, max(|inc64 - lW_in|, 1)).  This is the
+    arithmetic error of one step.  Every step whose along-run error exceeds
+    1e-4 in those runs is then classified: "inputs diverged" when the
+    same-input error at that step is within 1e-4 (the FP32 run's particles
+    had already parted from the FP64 run's: a resampling integer decided by
+    a rounding tie, then Lorenz-96's chaos), "arithmetic" otherwise."""
     import numpy as np
+    import torch
     from dataclasses import replace
     from libbi_b200 import BootstrapPF, configs
 
@@ -392,25 +405,49 @@ def precision_check(y_host, seeds=16, n=N_PARTICLES, T=T_OBS):
     m64 = replace(m32, precision="f64")
     y32 = np.asarray(y_host[:T], np.float32)
     y64 = y32.astype(np.float64)  # the same observed values in both precisions
-    inc_e, cum_e, ll32, ll64 = [], [], [], []
+    inc_e, cum_e, ll32, ll64, same_e = [], [], [], [], []
     for s in range(seeds):
-        out = []
-        for m, y in ((m32, y32), (m64, y64)):
-            pf = BootstrapPF(m, n, resampler="systematic", ess_rel=ESS_REL, seed=20_000 + s)
-            out.append(pf.filter(y, 0.0, DT))
-            pf.close()
-        (l32, i32, _), (l64, i64, _) = out
+        seed = 20_000 + s
+        pf32 = BootstrapPF(m32, n, resampler="systematic", ess_rel=ESS_REL, seed=seed)
+        l32, i32, _ = pf32.filter(y32, 0.0, DT)
+        pf32.close()
+        ref = BootstrapPF(m64, n, resampler="systematic", ess_rel=ESS_REL, seed=seed)
+        if s < same_input_seeds:
+            probes = [BootstrapPF(m, n, resampler="systematic", ess_rel=ESS_REL, seed=40_000 + s)
+                      for m in (m32, m64)]
+            i64, errs = np.zeros(T), np.zeros(T)
+            for k in range(T):
+                x, lw, _ = ref.state()
+                lw_in = float(torch.logsumexp(lw, 0)) - np.log(n)
+                incs = []
+                for pr, y in zip(probes, (y32, y64)):
+                    pr.init()
+                    xv, lwv, _ = pr.state()
+                    xv[:, :n].copy_(x[:, :n].to(xv.dtype))
+                    lwv.copy_(lw)
+                    incs.append(pr.step(k * DT, (k + 1) * DT, y[k]).log_increment)
+                errs[k] = abs(incs[0] - incs[1]) / max(abs(incs[1] - lw_in), 1.0)
+                i64[k] = ref.step(k * DT, (k + 1) * DT, y64[k]).log_increment
+            l64 = float(torch.logsumexp(ref.state()[1], 0)) - np.log(n)
+            for pr in probes:
+                pr.close()
+            same_e.append(errs)
+        else:
+            l64, i64, _ = ref.filter(y64, 0.0, DT)
+        ref.close()
         inc_e.append(np.abs(i32 - i64) / np.maximum(np.abs(i64), 1.0))
         c32, c64 = np.cumsum(i32), np.cumsum(i64)
         cum_e.append(np.abs(c32 - c64) / np.maximum(np.abs(c64), 1.0))
         ll32.append(l32)
         ll64.append(l64)
-    inc_e, cum_e = np.array(inc_e), np.array(cum_e)
+    inc_e, cum_e, same_e = np.array(inc_e), np.array(cum_e), np.array(same_e)
     ll32, ll64 = np.array(ll32), np.array(ll64)
-    one = one_step_precision(m32, m64, y32, y64, n)
     se = float(np.sqrt(ll32.var(ddof=1) / seeds + ll64.var(ddof=1) / seeds))
     within = cum_e.max(axis=0) <= 1e-4
     first_bad = int(np.argmin(within)) + 1 if not within.all() else None
+    beyond = inc_e[:same_input_seeds] > 1e-4
+    diverged = int(np.sum(beyond & (same_e <= 1e-4)))
+    arithmetic = int(np.sum(beyond & (same_e > 1e-4)))
     return {
         "workload": f"l96_d40_n{n}_t{T}_fp32_vs_fp64_{seeds}seeds",
         "increment_rel_err": {"median": float(np.median(inc_e)), "max": float(inc_e.max()),
@@ -422,43 +459,51 @@ def precision_check(y_host, seeds=16, n=N_PARTICLES, T=T_OBS):
         "mean_ll_fp32": float(ll32.mean()), "mean_ll_fp64": float(ll64.mean()),
         "mean_diff_in_standard_errors": float(abs(ll32.mean() - ll64.mean()) / se) if se > 0 else 0.0,
         "means_within_2_se": bool(abs(ll32.mean() - ll64.mean()) <= 2 * se),
-        "one_step_same_input": one,
+        "same_input_every_step": {
+            "seeds": same_input_seeds, "steps": T, "median_rel_err": float(np.median(same_e)),
+            "max_rel_err": float(same_e.max()), "within_1e-4": bool(same_e.max() <= 1e-4)},
+        "steps_beyond_1e-4_along_run": {
+            "seeds": same_input_seeds, "count": int(beyond.sum()), "inputs_diverged": diverged,
+            "arithmetic": arithmetic},
     }
 
 
-def one_step_precision(m32, m64, y32, y64, n, seeds=4, at=(0, 1, 10, 50, 100, 150, 199)):
-    """Arithmetic error of one step: at sampled steps of an FP64 run, the
-    FP64 state and log-weights are written into a fresh FP32 and a fresh
-    FP64 filter (same seed, so the same draws), each takes that step, and
-    the increments are compared relative to the FP64 increment's size
-    (max(|increment|, 1)).  This separates the FP32 arithmetic from the
-    run-to-run divergence that resampling and chaos add along a run."""
+def batched_precision(T=100):
+    """The batched workload (256 Lorenz-96 filters) in FP32 against the same
+    256 filters in FP64 on the same seeds and observations: per-filter
+    log-likelihood relative error, per-step increment errors, and the paired
+    difference of the estimates (FP32 minus FP64) in standard errors of its
+    mean over the filters."""
     import numpy as np
-    import torch
-    from libbi_b200 import BootstrapPF
+    from dataclasses import replace
+    from libbi_b200 import BatchedBootstrapPF
 
-    errs = []
-    for s in range(seeds):
-        ref = BootstrapPF(m64, n, resampler="systematic", ess_rel=ESS_REL, seed=30_000 + s)
-        for k in range(max(at) + 1):
-            if k in at:
-                x, lw, _ = ref.state()
-                x, lw = x[:, :n].clone(), lw.clone()
-                lw_inj = float(torch.logsumexp(lw, 0)) - np.log(n)
-                incs = []
-                for m, y in ((m32, y32), (m64, y64)):
-                    pf = BootstrapPF(m, n, resampler="systematic", ess_rel=ESS_REL, seed=40_000 + s)
-                    xv, lwv, _ = pf.state()
-                    xv[:, :n].copy_(x.to(xv.dtype))
-                    lwv.copy_(lw)
-                    incs.append(pf.step(k * DT, (k + 1) * DT, y[k]).log_increment)
-                    pf.close()
-                errs.append(abs(incs[0] - incs[1]) / max(abs(incs[1] - lw_inj), 1.0))
-            ref.step(k * DT, (k + 1) * DT, y64[k])
-        ref.close()
-    errs = np.array(errs)
-    return {"steps_sampled": list(at), "seeds": seeds, "median_rel_err": float(np.median(errs)),
-            "max_rel_err": float(errs.max()), "within_1e-4": bool(errs.max() <= 1e-4)}
+    models, ns, res, seeds, T = batched_workload(T=T)
+    y = batched_truth(models, T)
+    out = {}
+    for prec in ("f32", "f64"):
+        ms = [replace(m, precision=prec) for m in models]
+        b = BatchedBootstrapPF(ms, ns, res, seeds, ess_rel=ESS_REL)
+        yy = y if prec == "f32" else y.astype(np.float64)
+        ll, inc, _, st = b.filter(yy, 0.0, DT)
+        b.close()
+        out[prec] = (ll, inc, st)
+    (l32, i32, s32), (l64, i64, s64) = out["f32"], out["f64"]
+    ok = (s32 == 0) & (s64 == 0)
+    rel = np.abs(l32 - l64) / np.maximum(np.abs(l64), 1.0)
+    inc_e = np.abs(i32 - i64) / np.maximum(np.abs(i64), 1.0)
+    d = (l32 - l64)[ok]
+    se = float(d.std(ddof=1) / np.sqrt(d.size)) if d.size > 1 else 0.0
+    return {
+        "workload": "l96_d40_256filters_fp32_vs_fp64_t100",
+        "filters": int(ok.sum()),
+        "loglik_rel_err": {"median": float(np.median(rel[ok])), "max": float(rel[ok].max())},
+        "increment_rel_err": {"median": float(np.median(inc_e[:, ok])), "max": float(inc_e[:, ok].max()),
+                              "steps_within_1e-4": float(np.mean(inc_e[:, ok] <= 1e-4))},
+        "mean_paired_diff": float(d.mean()), "paired_diff_se": se,
+        "mean_diff_in_standard_errors": float(abs(d.mean()) / se) if se > 0 else 0.0,
+        "means_within_2_se": bool(abs(d.mean()) <= 2 * se),
+    }
 
 
 def equal_mean_time(boot, ll_target):
@@ -799,7 +844,23 @@ def main():
         e2e_s += time.perf_counter() - t0
         resampled += int(r.resampled)
     e2e_s = max_over_ranks(e2e_s, dist, "cuda")
-    e2e = whole_job_rate(N_PARTICLES * args.steps, world, e2e_s)
+    e2e_step_api = whole_job_rate(N_PARTICLES * args.steps, world, e2e_s)
+
+    # end to end through the call a LibBi filter client makes,
+    # Filter<BootstrapPF>::filter -> bpf_filter: the T observations copied
+    # from pinned host memory, the initial draw, T steps, the final term, and
+    # the increments, ESS and log-likelihood read back, host wall clock
+    # around each whole call (L2 flushed before each)
+    e2e_runs = max(3, args.steps // 10)
+    e2e_filter_s = 0.0
+    for _ in range(e2e_runs):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        pf.filter(y_np, 0.0, DT)
+        e2e_filter_s += time.perf_counter() - t0
+    e2e_filter_s = max_over_ranks(e2e_filter_s, dist, "cuda")
+    e2e = whole_job_rate(N_PARTICLES * T_OBS * e2e_runs, world, e2e_filter_s)
 
     hbm, how, sm_max = peaks()
     clocks = clk.summary()
@@ -816,7 +877,14 @@ def main():
         "config": workload_config(world),
         "resampled_steps_end_to_end": f"{resampled} of {args.steps}",
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": DIM * 4,
-                "d2h_bytes_per_step": 80, "timer": "host wall clock around bpf_step"},
+                "d2h_bytes_per_step": 3 * 8, "runs": e2e_runs, "steps_per_run": T_OBS,
+                "timer": "host wall clock around bpf_filter (Filter<BootstrapPF>::filter): observations "
+                         "uploaded from pinned host memory, initial draw, T steps, increments/ESS/log-likelihood "
+                         "read back"},
+        "e2e_step_api": {"value": e2e_step_api, "unit": UNIT, "h2d_bytes_per_step": DIM * 4,
+                         "d2h_bytes_per_step": 80,
+                         "timer": "host wall clock around bpf_step (BootstrapPF::step), one synchronising call "
+                                  "per step"},
         "gpu_launches": LAUNCHES_PER_STEP * args.steps,
         "roofline": {"kernel": "k_l96_transition<float,40>", "bound": "hbm", "achieved": achieved,
                      "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_source": how,
@@ -852,6 +920,7 @@ def main():
         line["pmmh"] = pmmh_chains()
     if extras and not args.no_precision:
         line["precision"] = precision_check(y_host)
+        line["precision_batched"] = batched_precision()
     if extras and not args.no_guided:
         line["guided"] = guided_vs_bootstrap(y_host, seeds=max(2, args.guided_seeds))
     if extras and not args.no_cpu_baseline:
