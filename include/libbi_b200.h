@@ -247,12 +247,19 @@ int bpf_timing_read(bpf_handle* h, int reset, double* resample_ms, double* trans
 
 /* Path output (BootstrapPFCache::writeState + AncestryCache,
  * share/src/bi/cache/BootstrapPFCache.hpp:182-210; BootstrapPF::samplePath,
- * share/src/bi/filter/BootstrapPF.hpp:148-154).  bpf_path_cache reserves
- * room for max_steps steps (0 frees it) and records the current state; every
- * later step (and bpf_init, which restarts the record) appends its state and
- * ancestors.  The whole history is kept in device memory (no pruning):
- * (max_steps + 1) x dim x ld values plus max_steps x ld ancestors. */
+ * share/src/bi/filter/BootstrapPF.hpp:148-154).  bpf_path_cache records up
+ * to max_steps steps (0 stops recording) and starts the record from the
+ * current state; every later step (and bpf_init, which restarts the record)
+ * appends the new particles with their ancestors.  The record is pruned as
+ * AncestryCache prunes it (share/src/bi/cuda/cache/AncestryCacheKernel.cuh:
+ * 29-48): only particles with a line to the current generation keep their
+ * node, so device memory follows the particles' genealogy (about N nodes
+ * plus the distinct ancestors of each past generation), not steps x N.  A
+ * recording step synchronises the stream once. */
 int bpf_path_cache(bpf_handle* h, int max_steps);
+/* Nodes the path record holds and the capacity of its pool (AncestryCache::
+ * report, share/src/bi/cache/AncestryCache.hpp:455-466); synchronises. */
+int bpf_path_cache_nodes(bpf_handle* h, int* nodes, int* capacity);
 /* samplePath: p ~ multinomial(exp(lw)) over the current log-weights
  * (RngHost::multinomial, share/src/bi/host/random/RngHost.hpp:120-139) from
  * one uniform (u: device pointer, or NULL for the handle's own draw), then

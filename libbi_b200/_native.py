@@ -51,7 +51,7 @@ EXPORTS = (
     "bpf_proposal_create", "bpf_proposal_destroy", "bpf_proposal_set_data", "bpf_proposal_train",
     "bpf_proposal_loss_grad", "bpf_proposal_params", "bpf_proposal_set_params", "bpf_set_proposal",
     "bpf_batch_set_proposal",
-    "bpf_path_cache", "bpf_sample_path", "bpf_step_sparse", "bpf_smc2_run", "bpf_debug_set_wait_limit", "bpf_create_model",
+    "bpf_path_cache", "bpf_sample_path", "bpf_step_sparse", "bpf_smc2_run", "bpf_debug_set_wait_limit", "bpf_create_model", "bpf_path_cache_nodes",
 )
 
 
@@ -187,6 +187,7 @@ def _declare(L):
         "bpf_set_proposal": (c_int, [H, H]),
         "bpf_batch_set_proposal": (c_int, [H, H]),
         "bpf_path_cache": (c_int, [H, c_int]),
+        "bpf_path_cache_nodes": (c_int, [H, POINTER(c_int), POINTER(c_int)]),
         "bpf_smc2_run": (c_int, [POINTER(ModelDesc), POINTER(Smc2Config), c_int, c_double, c_double, c_void_p,
                                  c_void_p, c_void_p, c_void_p, c_void_p, POINTER(c_int), POINTER(c_double)]),
         "bpf_step_sparse": (c_int, [H, c_double, c_double, c_void_p, c_void_p, c_int, POINTER(StepOut)]),

@@ -58,13 +58,12 @@ struct bpf_handle {
   bpf::BatchFilter* one_filt = nullptr;
   int* one_order = nullptr;
   int one_threads = 1024;
-  // path cache (bpf_path_cache): pc_len states of dim x ld in the model
-  // precision (slot 0 the state the recording started from, slot t the state
-  // after t more steps) and the ancestors of each recorded step
-  void* pc_x = nullptr;
-  int* pc_a = nullptr;
-  int pc_cap = 0;   // steps that fit
-  int pc_len = 0;   // states recorded
+  // path cache (bpf_path_cache): the pruned ancestry of the particles since
+  // the record started (pc_len generations), at most pc_cap steps
+  bpf::AncestryPool pc;
+  bool pc_on = false;
+  int pc_cap = 0;   // steps that may be recorded
+  int pc_len = 0;   // generations recorded
   bool pc_full = false;
 };
 
@@ -167,28 +166,18 @@ int timing_event(bpf_handle* h, int which) {
   return BPF_OK;
 }
 
-// ancestors of the step just taken, in the previous state's indexing
-__global__ void k_record_ancestors(const bpf::StepStats* st, const int* as, int* out, int n) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p < n) out[p] = st->resampled ? as[p] : p;
-}
-
 // append the handle's current state (and, after a step, its ancestors) to
 // the path cache
 int path_record(bpf_handle* h, bool after_step) {
-  if (!h->pc_x || h->pc_full) return BPF_OK;
+  if (!h->pc_on || h->pc_full) return BPF_OK;
   if (h->pc_len > h->pc_cap) {
     h->pc_full = true;
     return BPF_OK;
   }
-  const size_t slot = (size_t)h->dim * h->ld * h->esz;
-  BPF_TRY(cudaMemcpyAsync((char*)h->pc_x + (size_t)h->pc_len * slot, h->x[h->cur], slot, cudaMemcpyDeviceToDevice,
-                          h->stream));
-  if (after_step && h->pc_len > 0) {
-    k_record_ancestors<<<(h->n + 255) / 256, 256, 0, h->stream>>>(h->rs.stats, h->as,
-                                                                  h->pc_a + (size_t)(h->pc_len - 1) * h->ld, h->n);
-    BPF_TRY(cudaGetLastError());
-  }
+  int rc = after_step && h->pc_len > 0
+               ? bpf::ancestry_append(h->pc, h->x[h->cur], h->ld, h->as, h->rs.stats, h->stream)
+               : bpf::ancestry_reset(h->pc, h->n, h->dim, h->esz, h->x[h->cur], h->ld, h->stream);
+  if (rc) return rc;
   ++h->pc_len;
   return BPF_OK;
 }
@@ -479,7 +468,8 @@ int bpf_destroy(bpf_handle* h) {
   if (h->hist) cudaFree(h->hist);
   for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
   if (h->host_stats) cudaFreeHost(h->host_stats);
-  void* g[] = {h->pc_x, h->pc_a, h->one_filt, h->one_order};
+  bpf::ancestry_free(h->pc);
+  void* g[] = {h->one_filt, h->one_order};
   for (void* p : g)
     if (p) cudaFree(p);
   bpf::scratch_free(h->rs);
@@ -545,19 +535,6 @@ k_sample_index(const double* __restrict__ lw, int n, const double* u_in, uint64_
   if (threadIdx.x == 0) *out = s_best < n ? s_best : n - 1;
 }
 
-// AncestryCache::readPath (share/src/bi/cache/AncestryCache.hpp:294-311):
-// from the final particle back through the recorded ancestors
-template <class T>
-__global__ void k_trace_path(const T* __restrict__ X, const int* __restrict__ A, int len, int dim, int ld,
-                             const int* p_in, T* path) {
-  int a = *p_in;
-  for (int t = len - 1; t >= 0; --t) {
-    for (int i = threadIdx.x; i < dim; i += blockDim.x)
-      path[(size_t)t * dim + i] = X[((size_t)t * dim + i) * ld + a];
-    if (t > 0) a = A[(size_t)(t - 1) * ld + a];
-  }
-}
-
 }  // namespace
 
 extern "C" {
@@ -565,28 +542,24 @@ extern "C" {
 int bpf_path_cache(bpf_handle* h, int max_steps) {
   if (!h || max_steps < 0) return BPF_E_INVALID;
   BPF_TRY(cudaStreamSynchronize(h->stream));
-  if (h->pc_x) cudaFree(h->pc_x);
-  if (h->pc_a) cudaFree(h->pc_a);
-  h->pc_x = nullptr;
-  h->pc_a = nullptr;
+  bpf::ancestry_free(h->pc);
+  h->pc_on = false;
   h->pc_cap = 0;
   h->pc_len = 0;
   h->pc_full = false;
   if (max_steps == 0) return BPF_OK;
-  const size_t slot = (size_t)h->dim * h->ld * h->esz;
-  if (cudaMalloc(&h->pc_x, (size_t)(max_steps + 1) * slot) != cudaSuccess ||
-      cudaMalloc((void**)&h->pc_a, (size_t)max_steps * h->ld * sizeof(int)) != cudaSuccess) {
-    cudaGetLastError();
-    if (h->pc_x) cudaFree(h->pc_x);
-    h->pc_x = nullptr;
-    return BPF_E_NOMEM;
-  }
+  h->pc_on = true;
   h->pc_cap = max_steps;
   return path_record(h, false);  // the current state opens the record
 }
 
+int bpf_path_cache_nodes(bpf_handle* h, int* nodes, int* capacity) {
+  if (!h || !h->pc_on || h->pc_len == 0) return BPF_E_INVALID;
+  return bpf::ancestry_nodes(h->pc, h->stream, nodes, capacity);
+}
+
 int bpf_sample_path(bpf_handle* h, const double* u, void* path, int* particle, int* len) {
-  if (!h || !h->pc_x || h->pc_len == 0) return BPF_E_INVALID;
+  if (!h || !h->pc_on || h->pc_len == 0) return BPF_E_INVALID;
   if (h->pc_full) return BPF_E_TOO_LARGE;
   if (len) *len = h->pc_len;
   int* d_p = nullptr;
@@ -598,19 +571,15 @@ int bpf_sample_path(bpf_handle* h, const double* u, void* path, int* particle, i
     return BPF_E_NOMEM;
   }
   k_sample_index<<<1, kPathThreads, 0, h->stream>>>(h->lw, h->n, u, h->cfg.seed, h->step, d_p);
-  if (h->esz == 4)
-    k_trace_path<float><<<1, 64, 0, h->stream>>>((const float*)h->pc_x, h->pc_a, h->pc_len, h->dim, h->ld, d_p,
-                                                 (float*)d_path);
-  else
-    k_trace_path<double><<<1, 64, 0, h->stream>>>((const double*)h->pc_x, h->pc_a, h->pc_len, h->dim, h->ld, d_p,
-                                                  (double*)d_path);
-  int p = 0;
   cudaError_t e = cudaGetLastError();
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&p, d_p, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
-  if (e == cudaSuccess && path) e = cudaMemcpyAsync(path, d_path, pb, cudaMemcpyDeviceToHost, h->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  int rc = e == cudaSuccess ? bpf::ancestry_trace(h->pc, h->pc_len, d_p, d_path, h->stream) : BPF_E_CUDA;
+  int p = 0;
+  if (!rc) e = cudaMemcpyAsync(&p, d_p, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+  if (!rc && e == cudaSuccess && path) e = cudaMemcpyAsync(path, d_path, pb, cudaMemcpyDeviceToHost, h->stream);
+  if (!rc && e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
   cudaFree(d_p);
   cudaFree(d_path);
+  if (rc) return rc;
   if (e != cudaSuccess) { bpf_set_last_cuda_error(e); return BPF_E_CUDA; }
   if (particle) *particle = p;
   return BPF_OK;

@@ -223,6 +223,30 @@ int autotune_systematic(int n, cudaStream_t st, int* best, double* us);
 // shape holds n particles in one wave
 int autotuned_shape(int n);
 
+// Pruned ancestry store of the path output (ancestry.cu)
+struct AncestryPool {
+  int n = 0, dim = 0, esz = 0;
+  int cap = 0;                       // nodes
+  void* x = nullptr;                 // states: element i of node v at x[i * cap + v]
+  int* par = nullptr;                // parent node (-1: first generation)
+  int* ref = nullptr;                // recorded children
+  int* stack = nullptr;              // free nodes, stack[0 .. *top)
+  int* top = nullptr;                // device counter
+  int* leaf[2] = {nullptr, nullptr};  // node of each particle of the current generation
+  int cur = 0;
+  int* host_top = nullptr;           // pinned copy of *top
+};
+// (re)start the record with the state x as the first generation
+int ancestry_reset(AncestryPool& a, int n, int dim, int esz, const void* x, int ld, cudaStream_t st);
+// the next generation: state x, ancestors as (read when st->resampled);
+// synchronises st once
+int ancestry_append(AncestryPool& a, const void* x, int ld, const int* as, const StepStats* st, cudaStream_t s);
+// the len states of the line ending in particle *p_dev into path_dev (len x dim)
+int ancestry_trace(const AncestryPool& a, int len, const int* p_dev, void* path_dev, cudaStream_t st);
+// nodes in use and pool capacity (synchronises st)
+int ancestry_nodes(AncestryPool& a, cudaStream_t st, int* nodes, int* capacity);
+void ancestry_free(AncestryPool& a);
+
 // limit of the grid-barrier waits of the cooperative resamplers on the
 // current device, in SM clock cycles (negative: give up at once)
 int set_barrier_limit(long long cycles);

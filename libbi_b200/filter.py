@@ -392,6 +392,12 @@ class BootstrapPF:
         N.check(N.lib().bpf_path_cache(self._h, max_steps), "bpf_path_cache")
         self._path_steps = max_steps
 
+    def path_nodes(self):
+        """(nodes held, pool capacity) of the pruned path record."""
+        nodes, cap = ctypes.c_int(), ctypes.c_int()
+        N.check(N.lib().bpf_path_cache_nodes(self._h, ctypes.byref(nodes), ctypes.byref(cap)), "bpf_path_cache_nodes")
+        return nodes.value, cap.value
+
     def sample_path(self, u=None):
         """BootstrapPF::samplePath: (particle, path[len, dim]) with the path of
         a particle drawn from the current weights (u: device tensor with one
