@@ -81,7 +81,7 @@ def test_guided_every_step_against_fp64(cuda, oracle):
     oracle's FP64 guided step (FP64 RK4 mean, the network in FP64 on the same
     BF16 weights and BF16-rounded inputs and activations, FP64 normals of the
     same draws): the step's log-likelihood increments agree to 1e-4
-    relative at the median step."""
+    relative at every step (measured on B200: median 1.4e-7, max 5.2e-7)."""
     from libbi_b200 import BootstrapPF, LearnedProposal, ModelL96
     from oracle.mlp_oracle import forward, guided_step
 
@@ -129,7 +129,7 @@ def test_guided_every_step_against_fp64(cuda, oracle):
     errs = np.array(errs)
     print("guided FP32/BF16 vs FP64, per-step increment relative error: median %.3g max %.3g"
           % (np.median(errs), errs.max()))
-    assert np.median(errs) <= 1e-4, errs
+    assert errs.max() <= 1e-4, errs
 
 
 def test_estimator_means_agree(cuda, oracle):
