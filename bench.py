@@ -330,15 +330,18 @@ def batched_filters(runs=5):
     }
 
 
-def pmmh_chains(iterations=20, nchains=128, nparticles=2048, T=100):
+def pmmh_chains(iterations=2000, nchains=128, n_lo=1024, n_hi=8192, T=100, checks=0.01):
     """Particle-marginal Metropolis-Hastings on the plankton model: 128
     chains over (c, e, m, q) with priors c, e ~ U(0, 1), m, q ~
     LogN(ln 0.1, 0.5^2), Gaussian random walk of 0.02 per coordinate; every
-    iteration filters all chains' proposals (N particles each, systematic
-    resampling every step) over T = 100 daily observations log P + N(0, 0.2^2)
-    of one seeded model run (seed 4).  A bounded number of iterations is
-    timed (host clock around bpf_pmmh_run; each iteration is one graph
-    launch plus the proposal and accept/reject arithmetic on the host)."""
+    iteration filters all chains' proposals as one batch (each chain's
+    filter of N particles, N log-uniform in [1024, 8192] rounded to 32,
+    systematic resampling every step) over T = 100 daily observations
+    log P + N(0, 0.2^2) of one seeded model run (seed 4).  All `iterations`
+    are timed (host clock around bpf_pmmh_run).  Then, on 1% of the
+    iterations, one accepted proposal's log-likelihood is recomputed by an
+    independent single FP64 filter with the chain's particle count, seed and
+    parameters, which must reproduce the batched value."""
     import math
 
     import numpy as np
@@ -354,23 +357,50 @@ def pmmh_chains(iterations=20, nchains=128, nparticles=2048, T=100):
     truth.close()
     rng = np.random.default_rng(4)
     y = (np.log(ps) + model.sigma_y * rng.standard_normal(T)).astype(np.float64)
+    ns = np.floor(np.exp(rng.uniform(np.log(n_lo), np.log(n_hi), nchains))).astype(int)
+    ns = np.clip((ns + 31) // 32 * 32, n_lo, n_hi)
     priors = [Prior(0, "uniform", 0.0, 1.0, 0.02), Prior(1, "uniform", 0.0, 1.0, 0.02),
               Prior(2, "log_normal", math.log(0.1), 0.5, 0.02), Prior(3, "log_normal", math.log(0.1), 0.5, 0.02)]
-    mh = MarginalMH(model, priors, y, 0.0, 1.0, nchains=nchains, nparticles=nparticles, resampler="systematic",
-                    ess_rel=1.0, seed=4)
+    seed = 4
+    mh = MarginalMH(model, priors, y, 0.0, 1.0, nchains=nchains, nparticles=ns, resampler="systematic",
+                    ess_rel=1.0, seed=seed)
     mh.run(2)  # graph capture and warm-up
+    _, _, _, r0 = mh.state()
     t0 = time.perf_counter()
     out = mh.run(iterations)
     wall = time.perf_counter() - t0
     mh.close()
     acc = (out["accepted"] - 1) / (iterations + 2)
+    # FP64 replays of accepted proposals (the sample after an accepted move
+    # is the proposal; the filter of run r, chain c has seed seed + 1 + r C + c)
+    smp, pll = out["samples"], out["proposal_loglik"]
+    step = max(1, int(round(1.0 / checks)))
+    errs = []
+    for i0 in range(0, iterations, step):
+        for i in range(max(i0, 1), min(i0 + step, iterations)):
+            # chains that accepted at iteration i: their state changed
+            hit = [c for c in range(nchains) if np.isfinite(pll[i, c]) and not np.array_equal(smp[i, c], smp[i - 1, c])]
+            if hit:
+                c = hit[0]
+                th = smp[i, c]
+                pf = BootstrapPF(ModelPZ(c=th[0], e=th[1], m=th[2], q=th[3]), int(ns[c]), resampler="systematic",
+                                 ess_rel=1.0, seed=seed + 1 + (r0 + i) * nchains + c)
+                ll, _, _ = pf.filter(y, 0.0, 1.0)
+                pf.close()
+                errs.append(abs(ll - pll[i, c]) / max(abs(pll[i, c]), 1.0))
+                break
+    errs = np.array(errs)
+    particles = int(ns.sum())
     return {
-        "workload": f"pz_pmmh_{nchains}chains_n{nparticles}_t{T}",
-        "chains": nchains, "nparticles": nparticles, "T": T, "iterations_timed": iterations,
-        "iterations_per_s": iterations / wall,
-        "particle_steps_per_s": nchains * nparticles * T * iterations / wall,
-        "seconds_for_2000_iterations": 2000 * wall / iterations,
+        "workload": f"pz_pmmh_{nchains}chains_n{n_lo}_{n_hi}_loguniform_t{T}",
+        "chains": nchains, "nparticles_min": int(ns.min()), "nparticles_max": int(ns.max()),
+        "nparticles_total": particles, "T": T, "iterations_timed": iterations,
+        "seconds": wall, "iterations_per_s": iterations / wall,
+        "particle_steps_per_s": particles * T * iterations / wall,
         "mean_acceptance": float(np.mean(acc)),
+        "fp64_replay_checks": {"count": int(errs.size), "max_rel_err": float(errs.max()) if errs.size else None,
+                               "what": "accepted proposals on 1% of the iterations, refiltered by a single FP64 "
+                                       "filter with the chain's N, seed and parameters"},
         "timer": "host wall clock around bpf_pmmh_run",
     }
 

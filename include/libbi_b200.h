@@ -481,6 +481,8 @@ typedef struct {
   uint64_t seed;         /* proposals, acceptance and filter seeds derive from it */
   int nparams;
   bpf_pmmh_param params[BPF_MAX_THETA];
+  const int* chain_nparticles;  /* optional (host, nchains values, each 1 .. BPF_BATCH_MAX_PARTICLES):
+                                   each chain's filter size; NULL: nparticles for every chain */
 } bpf_pmmh_config;
 
 typedef struct bpf_pmmh bpf_pmmh;

@@ -88,6 +88,7 @@ class PmmhConfig(ctypes.Structure):
     _fields_ = [
         ("nchains", c_int), ("nparticles", c_int), ("resampler", c_int), ("metropolis_steps", c_int),
         ("ess_rel", c_double), ("seed", c_uint64), ("nparams", c_int), ("params", PmmhParam * BPF_MAX_THETA),
+        ("chain_nparticles", c_void_p),
     ]
 
 

@@ -46,6 +46,9 @@ using bpf::sampler::uniform_draw;
 int check_cfg(const bpf_model_desc* m, const bpf_pmmh_config* c) {
   if (!m || !c || c->nchains <= 0 || c->nparams <= 0 || c->nparams > BPF_MAX_THETA) return BPF_E_INVALID;
   if (c->nparticles <= 0 || c->nparticles > BPF_BATCH_MAX_PARTICLES) return BPF_E_INVALID;
+  if (c->chain_nparticles)
+    for (int k = 0; k < c->nchains; ++k)
+      if (c->chain_nparticles[k] <= 0 || c->chain_nparticles[k] > BPF_BATCH_MAX_PARTICLES) return BPF_E_INVALID;
   for (int j = 0; j < c->nparams; ++j) {
     const bpf_pmmh_param& q = c->params[j];
     if (q.index < 0 || q.index >= BPF_MAX_THETA || !(q.step >= 0.0)) return BPF_E_INVALID;
@@ -93,6 +96,7 @@ int bpf_pmmh_create(const bpf_model_desc* model, const bpf_pmmh_config* cfg, int
   if (!s) return BPF_E_NOMEM;
   s->model = *model;
   s->cfg = *cfg;
+  s->cfg.chain_nparticles = nullptr;  // copied into the batch below; the caller's array need not outlive create
   s->T = T;
   s->t0 = t0;
   s->dt = dt;
@@ -126,7 +130,7 @@ int bpf_pmmh_create(const bpf_model_desc* model, const bpf_pmmh_config* cfg, int
   }
   std::vector<bpf_batch_filter> bf((size_t)C);
   for (int c = 0; c < C; ++c) {
-    bf[c].nparticles = cfg->nparticles;
+    bf[c].nparticles = cfg->chain_nparticles ? cfg->chain_nparticles[c] : cfg->nparticles;
     bf[c].resampler = cfg->resampler;
     bf[c].metropolis_steps = cfg->metropolis_steps;
     bf[c].seed = cfg->seed + 1 + (uint64_t)c;

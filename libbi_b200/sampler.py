@@ -40,7 +40,14 @@ class MarginalMH:
         self.nchains = nchains
         self.nparams = len(self.priors)
         cfg = N.PmmhConfig()
-        cfg.nchains, cfg.nparticles = nchains, nparticles
+        # nparticles: one count for every chain, or one per chain
+        counts = np.atleast_1d(np.asarray(nparticles, dtype=np.int32))
+        if counts.size not in (1, nchains):
+            raise ValueError("nparticles: one value, or one per chain")
+        self.nparticles = counts if counts.size == nchains else np.full(nchains, int(counts[0]), np.int32)
+        self._counts = np.ascontiguousarray(self.nparticles, dtype=np.int32)
+        cfg.nchains, cfg.nparticles = nchains, int(self.nparticles.max())
+        cfg.chain_nparticles = self._counts.ctypes.data_as(ctypes.c_void_p).value
         cfg.resampler, cfg.metropolis_steps = RESAMPLERS[resampler], metropolis_steps
         cfg.ess_rel, cfg.seed, cfg.nparams = ess_rel, seed, self.nparams
         for j, q in enumerate(self.priors):

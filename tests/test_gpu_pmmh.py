@@ -86,3 +86,47 @@ def test_pmmh_chains_follow_the_mh_rule_and_oracle_filters(cuda, oracle):
     acc_rate = (out["accepted"] - 1) / iters
     assert (acc_rate > 0).any() and (acc_rate < 1).any()
     mh.close()
+
+
+def test_pmmh_chains_with_their_own_particle_counts(cuda, oracle):
+    """Chains with different filter sizes (N log-uniform in [1024, 8192]):
+    each chain's initial log-likelihood and its accepted proposals'
+    log-likelihoods equal the oracle's FP64 filter with that chain's N and
+    seed."""
+    from libbi_b200 import MarginalMH, ModelPZ, Prior
+    from libbi_b200 import _native as N
+
+    T, dt = 15, 1.0
+    truth = ModelPZ()
+    y, _ = oracle.simulate(truth.desc(), 4, T, 0.0, dt)
+    priors = [Prior(0, "uniform", 0.0, 1.0, 0.02), Prior(1, "uniform", 0.0, 1.0, 0.02),
+              Prior(2, "log_normal", math.log(0.1), 0.5, 0.02), Prior(3, "log_normal", math.log(0.1), 0.5, 0.02)]
+    C, seed, iters = 6, 21, 4
+    ns = [1024, 8192, 2048, 4000, 1500, 6144]
+    th0 = np.array([[0.25, 0.3, 0.1, 0.1]] * C)
+    mh = MarginalMH(truth, priors, y[:, 0], 0.0, dt, nchains=C, nparticles=ns, resampler="systematic",
+                    ess_rel=1.0, seed=seed, theta0=th0)
+
+    def oracle_ll(theta, n, fseed):
+        m = ModelPZ(c=theta[0], e=theta[1], m=theta[2], q=theta[3])
+        cfg = N.Config()
+        cfg.nparticles, cfg.resampler, cfg.ess_rel, cfg.seed = n, 0, 1.0, fseed
+        out = oracle.filter(m.desc(), cfg, y, T, 0.0, dt)
+        return out["ll"] if out["rc"] == 0 else -math.inf
+
+    _, cll, _, _ = mh.state()
+    for c in range(C):
+        np.testing.assert_allclose(cll[c], oracle_ll(th0[c], ns[c], seed + 1 + c), rtol=1e-10)
+    out = mh.run(iters)
+    checked = 0
+    prev = th0
+    for i in range(iters):
+        r = i + 1
+        for c in range(C):
+            if not np.array_equal(out["samples"][i, c], prev[c]):
+                np.testing.assert_allclose(out["proposal_loglik"][i, c],
+                                           oracle_ll(out["samples"][i, c], ns[c], seed + 1 + r * C + c), rtol=1e-10)
+                checked += 1
+        prev = out["samples"][i]
+    assert checked >= 2
+    mh.close()
