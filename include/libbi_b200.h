@@ -506,6 +506,12 @@ int bpf_pmmh_run(bpf_pmmh* s, int iterations, double* samples, double* log_likel
 /* Current state: theta[c*nparams + j], logLikelihood and logPrior per chain,
  * and the number of filter runs so far (the next run index). */
 int bpf_pmmh_state(bpf_pmmh* s, double* theta, double* log_likelihoods, double* log_priors, int* runs);
+typedef struct bpf_proposal bpf_proposal;
+/* Run every later filter of the chains as a guided filter with the learned
+ * proposal p (NULL: back to the bootstrap filter); the proposal is owned by
+ * the caller and must outlive its use.  No counterpart in the reference,
+ * whose MarginalMH filters with the bootstrap filter. */
+int bpf_pmmh_set_proposal(bpf_pmmh* s, bpf_proposal* p);
 
 /* ---- SMC^2 over the batched filter -------------------------------------- */
 /* MarginalSIR (share/src/bi/sampler/MarginalSIR.hpp:283-480): ntheta
@@ -565,11 +571,12 @@ int bpf_dense_bf16(const void* A, long long a_rs, long long a_cs, const void* B,
  * log-likelihood of x_{t+1}.  A filter with a proposal attached
  * (bpf_set_proposal) weights each particle by p(y|x') p(x'|x) / q(x'|x, y),
  * so its likelihood estimate stays unbiased. */
-typedef struct bpf_proposal bpf_proposal;
+/* bpf_proposal: declared with the PMMH entry points above */
 
-/* model: L96, dim 40, BPF_F32 (F = theta[0], sigma_eta = theta[1], h); dt: the
- * observation interval; max_batch: the largest training batch (>= 128).
- * The untrained proposal is close to the transition itself. */
+/* model: L96, dim 40, BPF_F32 (F = theta[0], sigma_eta = theta[1], h), or
+ * PZ, BPF_F64, RK4(3) (a proposal over the log-noise: bpf_proposal_set_states);
+ * dt: the observation interval; max_batch: the largest training batch
+ * (>= 128).  The untrained proposal is close to the transition itself. */
 int bpf_proposal_create(const bpf_model_desc* model, double dt, int max_batch, uint64_t seed, void* stream,
                         bpf_proposal** out);
 int bpf_proposal_destroy(bpf_proposal* p);
@@ -577,6 +584,19 @@ int bpf_proposal_destroy(bpf_proposal* p);
  * training): x_t, x_{t+1} simulated from x_t by the model, y_{t+1} observed
  * from x_{t+1}.  Computes the RK4 means and the input standardisation. */
 int bpf_proposal_set_data(bpf_proposal* p, const float* x_t, const float* x_t1, const float* y_t1, int n);
+/* The plankton model's proposal (model: PZ, FP64, RK4(3)): the network
+ * proposes each particle's log-noise, log alpha ~ N(mu + delta, exp(2 s))
+ * with (delta, s) = MLP([log P, log Z, y_{t+1} - log P]) (3 inputs, two
+ * hidden layers of 128, 2 outputs; the untrained proposal is the prior
+ * N(mu, sigma)).  Training rows are simulated from the states x_t (device,
+ * n x 2 row-major FP64, e.g. particles of a run): for each row the
+ * transition's log-noise from its prior, the ODE over dt and an observation
+ * (tag BPF_RNG_DATA of the proposal's seed); the network learns the
+ * log-noise from the state and the observation (bpf_proposal_train).  A
+ * proposal for PZ attaches to batches (bpf_batch_set_proposal,
+ * bpf_pmmh_set_proposal); their guided step weights each particle by
+ * p(y | x') p(log alpha) / q(log alpha). */
+int bpf_proposal_set_states(bpf_proposal* p, const double* x_t, int n);
 /* `steps` Adam steps on minibatches of `batch` rows drawn with replacement
  * (counter-based stream of the seed), learning rate lr after a linear
  * warm-up over 5% of the steps and decaying by a cosine to lr/10;

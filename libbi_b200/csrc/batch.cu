@@ -584,6 +584,9 @@ struct bpf_batch {
   double rs_us[3] = {0.0, 0.0, 0.0};  // its tuning medians for 256, 512, 1024 threads
   bpf_proposal* prop = nullptr;  // learned proposal (bpf_batch_set_proposal), owned by the caller
   int* tile2f = nullptr;       // tile -> filter, allocated with the proposal
+  // the PZ guided step's network rows (ld rows each), allocated with a PZ proposal
+  __nv_bfloat16 *gU = nullptr, *gH1 = nullptr, *gH2 = nullptr;
+  float* gO = nullptr;
   double ess_rel = 0.0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
@@ -661,7 +664,8 @@ void batch_free(bpf_batch* b) {
   for (cudaEvent_t e : b->ev)
     if (e) cudaEventDestroy(e);
   void* ptrs[] = {b->x[0], b->x[1], b->lw, b->as, b->stats, b->partials, b->counters, b->filt_dev,
-                  b->prm_dev, b->blk2f, b->order, b->lu, b->os, b->y_dev, b->hist, b->tile2f};
+                  b->prm_dev, b->blk2f, b->order, b->lu, b->os, b->y_dev, b->hist, b->tile2f,
+                  b->gU, b->gH1, b->gH2, b->gO};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
@@ -689,7 +693,36 @@ int batch_enqueue_step(bpf_batch* b, double t1, double t2, const void* y_dev, do
   int rc = bpf::launch_batch_resample(b->lw, b->as, b->filt_dev, b->order, b->nf, b->max_n, b->stats, b->lu,
                                       b->os, step, b->stream, b->rs_threads);
   if (rc) return rc;
-  if (b->prop && y_dev) {
+  if (b->prop && y_dev && b->model.kind == BPF_MODEL_PZ) {
+    // guided step of the PZ model: the proposal over the log-noise
+    const double dt = bpf::proposal_dt(b->prop);
+    if (std::fabs((t2 - t1) - dt) > 1e-9 * dt) return BPF_E_INVALID;
+    bpf::BatchPZGuidedArgs g;
+    g.x_in = (const double*)b->x[b->cur];
+    g.x_out = (double*)b->x[b->cur ^ 1];
+    g.ld = b->ld;
+    g.as = b->as;
+    g.lw = b->lw;
+    g.y = (const double*)y_dev;
+    g.t1 = t1;
+    g.t2 = t2;
+    g.step = step;
+    g.filt = b->filt_dev;
+    g.prms = (const bpf::PZParams*)b->prm_dev;
+    g.blk2f = b->blk2f;
+    g.blocks = b->blocks;
+    g.stats = b->stats;
+    g.partials = b->partials;
+    g.counters = b->counters;
+    g.hist = hist;
+    g.nf = b->nf;
+    g.k = k;
+    g.U = b->gU;
+    g.H1 = b->gH1;
+    g.H2 = b->gH2;
+    g.O = b->gO;
+    rc = bpf::launch_batch_pz_guided(*bpf::proposal_net(b->prop), g, b->stream);
+  } else if (b->prop && y_dev) {
     // guided step: the learned proposal, trained for one interval
     const double dt = bpf::proposal_dt(b->prop);
     if (std::fabs((t2 - t1) - dt) > 1e-9 * dt) return BPF_E_INVALID;
@@ -904,7 +937,19 @@ static int batch_timing_end(bpf_batch* b, int steps) {
 
 int bpf_batch_set_proposal(bpf_batch* b, bpf_proposal* p) {
   if (!b) return BPF_E_INVALID;
-  if (p) {
+  if (p && b->model.kind == BPF_MODEL_PZ) {
+    // the PZ proposal (one log-noise from three inputs) and its network rows
+    const bpf::ProposalNet& net = *bpf::proposal_net(p);
+    if (net.dim != 1 || net.din != 3 || net.hidden != bpf::kProposalHidden) return BPF_E_INVALID;
+    if (!b->gU) {
+      const size_t rows = (size_t)b->ld;
+      int rc = dalloc(&b->gU, rows * 3 * sizeof(__nv_bfloat16));
+      if (!rc) rc = dalloc(&b->gH1, rows * bpf::kProposalHidden * sizeof(__nv_bfloat16));
+      if (!rc) rc = dalloc(&b->gH2, rows * bpf::kProposalHidden * sizeof(__nv_bfloat16));
+      if (!rc) rc = dalloc(&b->gO, rows * 2 * sizeof(float));
+      if (rc) return rc;
+    }
+  } else if (p) {
     if (b->model.kind != BPF_MODEL_L96 || b->model.dim != 40 || b->model.precision != BPF_F32) return BPF_E_INVALID;
     const bpf::ProposalNet& net = *bpf::proposal_net(p);
     if (net.dim != b->model.dim || net.hidden != bpf::kProposalHidden) return BPF_E_INVALID;

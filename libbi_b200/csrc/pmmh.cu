@@ -225,6 +225,11 @@ int bpf_pmmh_run(bpf_pmmh* s, int iterations, double* samples, double* log_likel
   return BPF_OK;
 }
 
+int bpf_pmmh_set_proposal(bpf_pmmh* s, bpf_proposal* p) {
+  if (!s) return BPF_E_INVALID;
+  return bpf_batch_set_proposal(s->batch, p);
+}
+
 int bpf_pmmh_state(bpf_pmmh* s, double* theta, double* log_likelihoods, double* log_priors, int* runs) {
   if (!s) return BPF_E_INVALID;
   const int C = s->cfg.nchains;

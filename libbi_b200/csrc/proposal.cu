@@ -65,6 +65,43 @@ __global__ void k_gather_batch(const float* __restrict__ xt, const float* __rest
   for (int i = threadIdx.x; i < D; i += blockDim.x) r0[(size_t)b * D + i] = xt1[row * D + i] - mt[row * D + i];
 }
 
+// PZ training rows from states x_t (n x 2, FP64): the transition's log-noise
+// la = mu + sigma z0 from its prior, the RK4(3) step over dt with
+// alpha = exp(la), an observation y = log P' + sigma_y z1 (z0, z1 one
+// Box-Muller pair of the data stream); inputs [log P, log Z, y - log P] and
+// target la - mu
+__global__ void k_pz_make_data(const double* __restrict__ xt, int n, uint64_t seed, PZParams prm, double dt,
+                               float* __restrict__ feat, float* __restrict__ target) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  double P = xt[2 * (size_t)r], Z = xt[2 * (size_t)r + 1];
+  const bpf_u32x4 w = bpf_draw(seed, (uint32_t)r, 1u, 0u, BPF_RNG_DATA);
+  double z0, z1;
+  bpf_normal_pair_d(w.v[0], w.v[1], &z0, &z1);
+  const double la = __fma_rn(prm.sigma, z0, prm.mu);
+  const double lp0 = bpf_log(P), lz0 = bpf_log(Z);
+  pz_advance<double>(P, Z, bpf_exp(la), 0.0, dt, prm);
+  const double y = __fma_rn(prm.sigma_y, z1, bpf_log(P));
+  feat[3 * (size_t)r + 0] = (float)lp0;
+  feat[3 * (size_t)r + 1] = (float)lz0;
+  feat[3 * (size_t)r + 2] = (float)(y - lp0);
+  target[r] = (float)(la - prm.mu);
+}
+
+// minibatch row b <- a precomputed training row (standardised BF16 inputs,
+// FP32 targets)
+__global__ void k_gather_rows(const float* __restrict__ feat, const float* __restrict__ target, int n, int din,
+                              int D, int B, uint64_t seed, int step, const float* __restrict__ shift,
+                              const float* __restrict__ scale, __nv_bfloat16* U, float* r0) {
+  const int b = blockIdx.x;
+  if (b >= B) return;
+  bpf_u32x4 w = bpf_draw(seed, (uint32_t)b, (uint32_t)step, 0u, BPF_RNG_DATA);
+  const size_t row = (size_t)(((uint64_t)w.v[0] << 32 | w.v[1]) % (uint64_t)n);
+  for (int j = threadIdx.x; j < din; j += blockDim.x)
+    U[(size_t)b * din + j] = __float2bfloat16((feat[row * din + j] - shift[j]) * scale[j]);
+  for (int i = threadIdx.x; i < D; i += blockDim.x) r0[(size_t)b * D + i] = target[row * D + i];
+}
+
 __global__ void k_loss_grad(const float* __restrict__ O, const float* __restrict__ r0, int B, int D,
                             __nv_bfloat16* dO, double* loss_part) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
@@ -167,6 +204,10 @@ __global__ void k_pack_weights(const __nv_bfloat16* __restrict__ Ph, int o_w1, i
 }
 
 int pack_weights(ProposalNet& p, cudaStream_t st) {
+  // the images feed the fused L96 guided kernel, whose inputs are whole
+  // 8-element core-matrix rows; a network with another input width (PZ)
+  // runs through the separate dense layers and needs none
+  if (p.din % 8 != 0) return BPF_OK;
   const int total = p.hidden * p.din + p.hidden * p.hidden + p.dout * p.hidden;
   k_pack_weights<<<(total + 255) / 256, 256, 0, st>>>(p.params_h, p.o_w1, p.o_w2, p.o_w3, p.hidden, p.din, p.dout,
                                                       p.packed, p.pk_w1, p.pk_w2, p.pk_w3);
@@ -245,9 +286,9 @@ static int loss_and_grad(ProposalNet& p, int B, cudaStream_t st) {
   return BPF_OK;
 }
 
-int ProposalNet::alloc(int d, int hid, int cap_batch) {
+int ProposalNet::alloc(int d, int hid, int cap_batch, int din_) {
   dim = d;
-  din = 2 * d;
+  din = din_ > 0 ? din_ : 2 * d;
   dout = 2 * d;
   hidden = hid;
   o_w1 = 0;
@@ -292,7 +333,7 @@ int ProposalNet::alloc(int d, int hid, int cap_batch) {
 
 void ProposalNet::release() {
   void* ps[] = {params, params_h, packed, grads, m1, m2, shift, scale, err, loss, U, H1, H2, O, dO, dH, dZ, r0, mt,
-                 colpart, loss_part, ws};
+                 colpart, loss_part, ws, feat, target};
   for (void* q : ps)
     if (q) cudaFree(q);
 }
@@ -331,7 +372,10 @@ void init_params(bpf_proposal* q, std::vector<float>& P) {
   const double a1 = std::sqrt(6.0 / p.din), a2 = std::sqrt(6.0 / p.hidden);
   for (int i = 0; i < p.hidden * p.din; ++i) P[p.o_w1 + i] = (float)(a1 * u((uint32_t)(p.o_w1 + i)));
   for (int i = 0; i < p.hidden * p.hidden; ++i) P[p.o_w2 + i] = (float)(a2 * u((uint32_t)(p.o_w2 + i)));
-  for (int i = 0; i < p.dim; ++i) P[p.o_b3 + p.dim + i] = (float)std::log(q->model.theta[1] > 0.0 ? q->model.theta[1] : 1.0);
+  // the noise scale: sigma_eta of L96 (theta[1]), the log-noise deviation
+  // sigma of PZ (theta[5])
+  const double sn = q->model.kind == BPF_MODEL_PZ ? q->model.theta[5] : q->model.theta[1];
+  for (int i = 0; i < p.dim; ++i) P[p.o_b3 + p.dim + i] = (float)std::log(sn > 0.0 ? sn : 1.0);
 }
 
 int upload_params(bpf_proposal* q, const float* P) {
@@ -360,16 +404,21 @@ int bpf_proposal_create(const bpf_model_desc* model, double dt, int max_batch, u
                         bpf_proposal** out) {
   if (!out) return BPF_E_INVALID;
   *out = nullptr;
-  if (!model || model->kind != BPF_MODEL_L96 || model->dim != 40 || model->precision != BPF_F32 || !(dt > 0.0) ||
-      !(model->h > 0.0) || max_batch < 128 || max_batch > (1 << 20))
-    return BPF_E_INVALID;
+  if (!model || !(dt > 0.0) || !(model->h > 0.0) || max_batch < 128 || max_batch > (1 << 20)) return BPF_E_INVALID;
+  const bool l96 = model->kind == BPF_MODEL_L96 && model->dim == 40 && model->precision == BPF_F32;
+  const bool pz = model->kind == BPF_MODEL_PZ && model->dim == 2 && model->precision == BPF_F64 &&
+                  model->integrator == BPF_ODE_RK43 && model->theta[5] > 0.0;
+  if (!l96 && !pz) return BPF_E_INVALID;
   bpf_proposal* q = new (std::nothrow) bpf_proposal();
   if (!q) return BPF_E_NOMEM;
   q->model = *model;
   q->dt = dt;
   q->seed = seed;
   q->stream = (cudaStream_t)stream;
-  int rc = q->net.alloc(model->dim, bpf::kProposalHidden, max_batch);
+  // L96: the 40 state components from [x_t, y - m(x_t)] (80 inputs); PZ:
+  // the one log-noise from [log P, log Z, y - log P]
+  int rc = pz ? q->net.alloc(1, bpf::kProposalHidden, max_batch, 3)
+              : q->net.alloc(model->dim, bpf::kProposalHidden, max_batch);
   std::vector<float> P;
   if (!rc) {
     init_params(q, P);
@@ -400,8 +449,44 @@ int bpf_proposal_destroy(bpf_proposal* q) {
   return BPF_OK;
 }
 
+int bpf_proposal_set_states(bpf_proposal* q, const double* x_t, int n) {
+  if (!q || !x_t || n <= 0 || q->model.kind != BPF_MODEL_PZ) return BPF_E_INVALID;
+  bpf::ProposalNet& p = q->net;
+  if (p.feat) cudaFree(p.feat);
+  if (p.target) cudaFree(p.target);
+  p.feat = p.target = nullptr;
+  p.rows = 0;
+  if (cudaMalloc((void**)&p.feat, (size_t)n * p.din * 4) != cudaSuccess ||
+      cudaMalloc((void**)&p.target, (size_t)n * p.dim * 4) != cudaSuccess) {
+    cudaGetLastError();
+    return BPF_E_NOMEM;
+  }
+  p.rows = n;
+  q->n = n;
+  const bpf::PZParams prm = bpf::pz_params<double>(q->model.theta, q->model.h, q->model.atoler, q->model.rtoler);
+  bpf::k_pz_make_data<<<(n + 127) / 128, 128, 0, q->stream>>>(x_t, n, q->seed, prm, q->dt, p.feat, p.target);
+  BPF_TRY(cudaGetLastError());
+  // input standardisation from (up to) the first 65536 rows
+  const int ns = n < 65536 ? n : 65536;
+  std::vector<float> h((size_t)ns * p.din);
+  BPF_TRY(cudaMemcpyAsync(h.data(), p.feat, h.size() * 4, cudaMemcpyDeviceToHost, q->stream));
+  BPF_TRY(cudaStreamSynchronize(q->stream));
+  std::vector<float> sh((size_t)p.din), sc((size_t)p.din);
+  for (int j = 0; j < p.din; ++j) {
+    double s = 0.0, s2 = 0.0;
+    for (int r = 0; r < ns; ++r) { const double v = h[(size_t)r * p.din + j]; s += v; s2 += v * v; }
+    const double mean = s / ns, var = s2 / ns - mean * mean;
+    sh[j] = (float)mean;
+    sc[j] = (float)(1.0 / std::sqrt(var > 1e-12 ? var : 1.0));
+  }
+  BPF_TRY(cudaMemcpyAsync(p.shift, sh.data(), sh.size() * 4, cudaMemcpyHostToDevice, q->stream));
+  BPF_TRY(cudaMemcpyAsync(p.scale, sc.data(), sc.size() * 4, cudaMemcpyHostToDevice, q->stream));
+  BPF_TRY(cudaStreamSynchronize(q->stream));
+  return BPF_OK;
+}
+
 int bpf_proposal_set_data(bpf_proposal* q, const float* x_t, const float* x_t1, const float* y_t1, int n) {
-  if (!q || !x_t || !x_t1 || !y_t1 || n <= 0) return BPF_E_INVALID;
+  if (!q || !x_t || !x_t1 || !y_t1 || n <= 0 || q->model.kind != BPF_MODEL_L96) return BPF_E_INVALID;
   bpf::ProposalNet& p = q->net;
   if (p.mt) cudaFree(p.mt);
   p.mt = nullptr;
@@ -445,8 +530,12 @@ int bpf_proposal_train(bpf_proposal* q, int steps, int batch, double lr, float* 
     const double w = s < warm ? (double)(s + 1) / warm : 1.0;
     const double c = 0.1 + 0.9 * 0.5 * (1.0 + std::cos(3.14159265358979323846 * s / (double)steps));
     const double lr_s = lr * w * c;
-    bpf::k_gather_batch<<<batch, 128, 0, q->stream>>>(q->xt, p.mt, q->xt1, q->yt1, q->n, p.dim, batch, q->seed,
-                                                      q->train_step, p.shift, p.scale, p.U, p.r0);
+    if (p.feat)
+      bpf::k_gather_rows<<<batch, 128, 0, q->stream>>>(p.feat, p.target, p.rows, p.din, p.dim, batch, q->seed,
+                                                       q->train_step, p.shift, p.scale, p.U, p.r0);
+    else
+      bpf::k_gather_batch<<<batch, 128, 0, q->stream>>>(q->xt, p.mt, q->xt1, q->yt1, q->n, p.dim, batch, q->seed,
+                                                        q->train_step, p.shift, p.scale, p.U, p.r0);
     int rc = bpf::loss_and_grad(p, batch, q->stream);
     if (rc) return rc;
     ++q->adam_step;

@@ -12,6 +12,8 @@ constexpr int kProposalHidden = 128;
 constexpr float kSMin = -7.0f, kSMax = 3.0f;
 
 struct ProposalNet {
+  // dim: the proposed variables (the L96 state's 40 components; the PZ
+  // model's one log-noise), din: network inputs, dout = 2 dim: (delta, s)
   int dim = 0, din = 0, dout = 0, hidden = 0;
   // parameter vector: W1 [hidden x din], b1, W2 [hidden x hidden], b2,
   // W3 [dout x hidden], b3 (offsets in floats)
@@ -26,7 +28,12 @@ struct ProposalNet {
   int cap = 0;
   __nv_bfloat16 *U = nullptr, *H1 = nullptr, *H2 = nullptr, *dO = nullptr, *dZ = nullptr;
   float *O = nullptr, *dH = nullptr, *r0 = nullptr;
-  float* mt = nullptr;  // RK4 means of the training inputs
+  float* mt = nullptr;  // RK4 means of the training inputs (L96)
+  // precomputed training rows (PZ): inputs [rows x din] and targets
+  // [rows x dim] in FP32
+  float* feat = nullptr;
+  float* target = nullptr;
+  int rows = 0;
   // the BF16 weight matrices as shared-memory images in the canonical
   // K-major layout (tc.cuh): W1 at byte pk_w1, W2 at pk_w2, W3 at pk_w3;
   // rebuilt by pack_weights whenever params_h changes outside training and
@@ -45,7 +52,7 @@ struct ProposalNet {
   const float* b2() const { return params + o_b2; }
   const float* b3() const { return params + o_b3; }
 
-  int alloc(int d, int hid, int cap_batch);
+  int alloc(int d, int hid, int cap_batch, int din_ = 0);  // din_ 0: 2 d
   void release();
 };
 
@@ -99,6 +106,34 @@ struct BatchGuidedArgs {
   int nf, k;
 };
 int launch_batch_guided(ProposalNet& net, const BatchGuidedArgs& a, cudaStream_t st);
+
+// the guided step of every filter of a PZ batch (guided_pz.cu): the proposal
+// over each particle's log-noise, inputs and network as separate launches
+// over all the batch's columns (rows of U, H1, H2, O)
+struct PZParams;
+struct BatchPZGuidedArgs {
+  const double* x_in;
+  double* x_out;
+  int ld;
+  int* as;
+  double* lw;
+  const double* y;  // nf device observations
+  double t1, t2;
+  int step;
+  const BatchFilter* filt;
+  const PZParams* prms;
+  const int* blk2f;  // transition block -> filter
+  int blocks;
+  StepStats* stats;
+  LwPartial* partials;
+  unsigned* counters;
+  double* hist;
+  int nf, k;
+  // network buffers, ld rows each
+  __nv_bfloat16 *U, *H1, *H2;
+  float* O;
+};
+int launch_batch_pz_guided(ProposalNet& net, const BatchPZGuidedArgs& a, cudaStream_t st);
 
 }  // namespace bpf
 

@@ -73,6 +73,13 @@ class MarginalMH:
         except Exception:
             pass
 
+    def set_proposal(self, proposal):
+        """Filter later iterations with the learned proposal (a
+        LearnedProposal of the same model; None: the bootstrap filter)."""
+        N.check(N.lib().bpf_pmmh_set_proposal(self._h, None if proposal is None else proposal.handle),
+                "bpf_pmmh_set_proposal")
+        self._proposal = proposal
+
     def run(self, iterations: int):
         """Returns dict(samples[it, C, P], loglik[it, C], logprior[it, C],
         proposal_loglik[it, C], accepted[C])."""

@@ -371,14 +371,12 @@ static double l96_particle_d(const bpf_model_desc* m, double* x, const double* y
 }
 
 /* PZ transition of one particle in FP64 (RK4(3) adaptive) */
-static double pz_particle_d(const bpf_model_desc* m, double* x, const double* y, double t1d, double t2d,
-                            uint64_t seed, int step, uint32_t p, double base, uint64_t mask) {
+/* the RK4(3) day of one particle with a given alpha, then the observation
+ * term */
+static double pz_particle_alpha(const bpf_model_desc* m, double* x, const double* y, double t1d, double t2d,
+                                double alpha, double base, uint64_t mask) {
   const double c = m->theta[0], e = m->theta[1], mm = m->theta[2], q = m->theta[3];
-  const double mu = m->theta[4], sigma = m->theta[5], sy = m->theta[6];
-  bpf_u32x4 r = bpf_draw(seed, p, (uint32_t)step, 0u, BPF_RNG_NOISE);
-  double z0, z1;
-  bpf_normal_pair_d(r.v[0], r.v[1], &z0, &z1);
-  const double alpha = bpf_exp(fma(sigma, z0, mu));
+  const double sy = m->theta[6];
   const double atol = m->atoler, rtol = m->rtoler;
   const double facl = 0.2, facr = 10.0, beta = 0.04;
   const double logsafe = log(0.9), expo = 0.5 * fma(-0.04, 0.75, 0.2);
@@ -461,6 +459,41 @@ static double pz_particle_d(const bpf_model_desc* m, double* x, const double* y,
     l += term;
   }
   return l;
+}
+
+static double pz_particle_d(const bpf_model_desc* m, double* x, const double* y, double t1d, double t2d,
+                            uint64_t seed, int step, uint32_t p, double base, uint64_t mask) {
+  const double mu = m->theta[4], sigma = m->theta[5];
+  bpf_u32x4 r = bpf_draw(seed, p, (uint32_t)step, 0u, BPF_RNG_NOISE);
+  double z0, z1;
+  bpf_normal_pair_d(r.v[0], r.v[1], &z0, &z1);
+  return pz_particle_alpha(m, x, y, t1d, t2d, bpf_exp(fma(sigma, z0, mu)), base, mask);
+}
+
+/* The guided step of the PZ model (libbi_b200/csrc/guided_pz.cu) for n
+ * particles given the proposal's outputs delta[p], s[p] (s already clamped):
+ * log alpha = mu + delta + exp(s) z, z the particle's transition normal;
+ * the ODE with alpha = exp(log alpha); lw[p] = base + the observation term
+ * - ((log alpha - mu)/sigma)^2 / 2 - log sigma + z^2 / 2 + s.  x_in/x_out:
+ * SoA (2 x ld); the gather through as when resampled, base ll then. */
+void orc_pz_guided_step(const bpf_model_desc* m, const double* x_in, double* x_out, int ld, int n, const int* as,
+                        int resampled, double* lw, double y, double t1, double t2, uint64_t seed, int step,
+                        double ll, const double* delta, const double* s) {
+  const double mu = m->theta[4], sigma = m->theta[5];
+  for (int p = 0; p < n; ++p) {
+    const int src = resampled ? as[p] : p;
+    double x[2] = {x_in[src], x_in[(size_t)ld + src]};
+    bpf_u32x4 r = bpf_draw(seed, (uint32_t)p, (uint32_t)step, 0u, BPF_RNG_NOISE);
+    double z0, z1;
+    bpf_normal_pair_d(r.v[0], r.v[1], &z0, &z1);
+    const double la = fma(bpf_exp(s[p]), z0, mu + delta[p]);
+    double l = pz_particle_alpha(m, x, &y, t1, t2, bpf_exp(la), resampled ? ll : lw[p], ~(uint64_t)0);
+    const double u = (la - mu) / sigma;
+    l += fma(-0.5, u * u, -bpf_log(sigma)) + fma(0.5, z0 * z0, s[p]);
+    lw[p] = l;
+    x_out[p] = x[0];
+    x_out[(size_t)ld + p] = x[1];
+  }
 }
 
 /* ------------------------------------------- models in the generated form

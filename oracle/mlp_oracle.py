@@ -18,8 +18,9 @@ def bf16(x):
     return r.view(np.float32)
 
 
-def unpack(params, d=40, hidden=128):
-    din = dout = 2 * d
+def unpack(params, d=40, hidden=128, din=None):
+    din = 2 * d if din is None else din
+    dout = 2 * d
     o = 0
     out = {}
     for name, shape in (("W1", (hidden, din)), ("b1", (hidden,)), ("W2", (hidden, hidden)), ("b2", (hidden,)),
@@ -32,10 +33,11 @@ def unpack(params, d=40, hidden=128):
 
 def loss_grad(params, U, r0, d=40, hidden=128):
     """Mean Gaussian NLL and its gradient (flat, the parameter layout) for a
-    minibatch: U [B x 2d] (BF16 values), r0 [B x d] = x_{t+1} - m(x_t)."""
-    P = unpack(params, d, hidden)
-    W1h, W2h, W3h = bf16(P["W1"]), bf16(P["W2"]), bf16(P["W3"])
+    minibatch: U [B x din] (BF16 values; din = 2d for Lorenz '96, 3 for
+    PZ), r0 [B x d] = x_{t+1} - m(x_t) (Lorenz '96) or log alpha - mu (PZ)."""
     U = np.asarray(U, np.float64)
+    P = unpack(params, d, hidden, U.shape[1])
+    W1h, W2h, W3h = bf16(P["W1"]), bf16(P["W2"]), bf16(P["W3"])
     B = U.shape[0]
     H1 = bf16(np.maximum((U @ W1h.T.astype(np.float64)) + P["b1"], 0.0).astype(np.float32))
     H2 = bf16(np.maximum((H1.astype(np.float64) @ W2h.T) + P["b2"], 0.0).astype(np.float32))
@@ -83,3 +85,17 @@ def guided_step(delta, s, m, z, y, sigma_eta, sigma_y, lw0):
     obs = np.sum(-0.5 * ((y - x) / sigma_y) ** 2 - c2 - np.log(sigma_y), axis=1)
     corr = np.sum(-0.5 * (dx / sigma_eta) ** 2 - np.log(sigma_eta), axis=1) - np.sum(-0.5 * z * z - s, axis=1)
     return x, lw0 + obs + corr
+
+
+def forward_rows(params, shift, scale, feats, d, hidden=128):
+    """(delta, s) of the proposal for raw input rows feats [B x din] (the
+    PZ proposal: [log P, log Z, y - log P], d = 1), with the tensor-core
+    path's BF16 roundings."""
+    din = feats.shape[1]
+    P = unpack(params, d, hidden, din)
+    W1h, W2h, W3h = bf16(P["W1"]), bf16(P["W2"]), bf16(P["W3"])
+    U = bf16((np.asarray(feats, np.float32) - shift) * scale).astype(np.float64)
+    H1 = bf16(np.maximum(U @ W1h.T + P["b1"], 0.0).astype(np.float32)).astype(np.float64)
+    H2 = bf16(np.maximum(H1 @ W2h.T + P["b2"], 0.0).astype(np.float32)).astype(np.float64)
+    O = (H2 @ W3h.T + P["b3"]).astype(np.float32)
+    return O[:, :d], np.clip(O[:, d:], S_MIN, S_MAX)

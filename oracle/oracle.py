@@ -57,6 +57,8 @@ class Oracle:
         L.orc_noise_normals.argtypes = [c_uint64, ctypes.c_uint32, c_int, c_int, c_int, c_void_p]
         L.orc_pmmh_draws.argtypes = [c_uint64, c_int, c_int, c_int, c_void_p, POINTER(c_double)]
         L.orc_simulate.argtypes = [c_void_p, c_uint64, c_int, c_double, c_double, c_void_p, c_void_p]
+        L.orc_pz_guided_step.argtypes = [c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p, c_int, c_void_p,
+                                         c_double, c_double, c_double, c_uint64, c_int, c_double, c_void_p, c_void_p]
         self.L = L
 
     # reductions
@@ -155,6 +157,19 @@ class Oracle:
         rc = self.L.orc_filter(ctypes.byref(desc), ctypes.byref(cfg), T, t0, dt, _p(y), _p(inc), _p(ess), _p(res),
                                ctypes.byref(ll), _p(x), _p(lw))
         return dict(rc=rc, ll=ll.value, inc=inc, ess=ess, resampled=res, x=x, lw=lw)
+
+    def pz_guided_step(self, desc, x_in, n, as_, resampled, lw, y, t1, t2, seed, step, ll, delta, s):
+        """The PZ guided step given the proposal's outputs (delta[n], s[n],
+        s clamped): returns (x_out, lw_out)."""
+        x_in = np.ascontiguousarray(x_in, np.float64)
+        x_out = np.zeros_like(x_in)
+        lw = np.ascontiguousarray(lw, np.float64).copy()
+        as_ = None if as_ is None else np.ascontiguousarray(as_, np.int32)
+        d = np.ascontiguousarray(delta, np.float64)
+        s = np.ascontiguousarray(s, np.float64)
+        self.L.orc_pz_guided_step(ctypes.byref(desc), _p(x_in), _p(x_out), x_in.shape[1], n, _p(as_), int(resampled),
+                                  _p(lw), float(y), t1, t2, seed, step, ll, _p(d), _p(s))
+        return x_out, lw
 
     def noise_normals(self, seed, p, step, n, f32):
         """The n standard normals of particle p's process noise at step, in
