@@ -584,9 +584,8 @@ struct bpf_batch {
   double rs_us[3] = {0.0, 0.0, 0.0};  // its tuning medians for 256, 512, 1024 threads
   bpf_proposal* prop = nullptr;  // learned proposal (bpf_batch_set_proposal), owned by the caller
   int* tile2f = nullptr;       // tile -> filter, allocated with the proposal
-  // the PZ guided step's network rows (ld rows each), allocated with a PZ proposal
-  __nv_bfloat16 *gU = nullptr, *gH1 = nullptr, *gH2 = nullptr;
-  float* gO = nullptr;
+  // the PZ guided step's network outputs (ld entries), allocated with a PZ proposal
+  float2* gO = nullptr;
   double ess_rel = 0.0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
@@ -665,7 +664,7 @@ void batch_free(bpf_batch* b) {
     if (e) cudaEventDestroy(e);
   void* ptrs[] = {b->x[0], b->x[1], b->lw, b->as, b->stats, b->partials, b->counters, b->filt_dev,
                   b->prm_dev, b->blk2f, b->order, b->lu, b->os, b->y_dev, b->hist, b->tile2f,
-                  b->gU, b->gH1, b->gH2, b->gO};
+                  b->gO};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
@@ -717,9 +716,6 @@ int batch_enqueue_step(bpf_batch* b, double t1, double t2, const void* y_dev, do
     g.hist = hist;
     g.nf = b->nf;
     g.k = k;
-    g.U = b->gU;
-    g.H1 = b->gH1;
-    g.H2 = b->gH2;
     g.O = b->gO;
     rc = bpf::launch_batch_pz_guided(*bpf::proposal_net(b->prop), g, b->stream);
   } else if (b->prop && y_dev) {
@@ -938,15 +934,11 @@ static int batch_timing_end(bpf_batch* b, int steps) {
 int bpf_batch_set_proposal(bpf_batch* b, bpf_proposal* p) {
   if (!b) return BPF_E_INVALID;
   if (p && b->model.kind == BPF_MODEL_PZ) {
-    // the PZ proposal (one log-noise from three inputs) and its network rows
+    // the PZ proposal (one log-noise from three inputs) and its outputs
     const bpf::ProposalNet& net = *bpf::proposal_net(p);
     if (net.dim != 1 || net.din != 3 || net.hidden != bpf::kProposalHidden) return BPF_E_INVALID;
-    if (!b->gU) {
-      const size_t rows = (size_t)b->ld;
-      int rc = dalloc(&b->gU, rows * 3 * sizeof(__nv_bfloat16));
-      if (!rc) rc = dalloc(&b->gH1, rows * bpf::kProposalHidden * sizeof(__nv_bfloat16));
-      if (!rc) rc = dalloc(&b->gH2, rows * bpf::kProposalHidden * sizeof(__nv_bfloat16));
-      if (!rc) rc = dalloc(&b->gO, rows * 2 * sizeof(float));
+    if (!b->gO) {
+      int rc = dalloc(&b->gO, (size_t)b->ld * sizeof(float2));
       if (rc) return rc;
     }
   } else if (p) {

@@ -188,12 +188,14 @@ __global__ void k_adam(float* __restrict__ P, const float* __restrict__ G, float
 }
 
 // the three weight matrices into their shared-memory images
+// (W1's image has k1 >= din columns, the ones past din zero from allocation)
 __global__ void k_pack_weights(const __nv_bfloat16* __restrict__ Ph, int o_w1, int o_w2, int o_w3, int hidden,
-                               int din, int dout, unsigned char* __restrict__ out, int pk_w1, int pk_w2, int pk_w3) {
+                               int din, int k1, int dout, unsigned char* __restrict__ out, int pk_w1, int pk_w2,
+                               int pk_w3) {
   const int n1 = hidden * din, n2 = hidden * hidden, n3 = dout * hidden;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n1) {
-    *reinterpret_cast<__nv_bfloat16*>(out + pk_w1 + tc::kmajor_off(i / din, i % din, din)) = Ph[o_w1 + i];
+    *reinterpret_cast<__nv_bfloat16*>(out + pk_w1 + tc::kmajor_off(i / din, i % din, k1)) = Ph[o_w1 + i];
   } else if (i < n1 + n2) {
     const int j = i - n1;
     *reinterpret_cast<__nv_bfloat16*>(out + pk_w2 + tc::kmajor_off(j / hidden, j % hidden, hidden)) = Ph[o_w2 + j];
@@ -204,13 +206,9 @@ __global__ void k_pack_weights(const __nv_bfloat16* __restrict__ Ph, int o_w1, i
 }
 
 int pack_weights(ProposalNet& p, cudaStream_t st) {
-  // the images feed the fused L96 guided kernel, whose inputs are whole
-  // 8-element core-matrix rows; a network with another input width (PZ)
-  // runs through the separate dense layers and needs none
-  if (p.din % 8 != 0) return BPF_OK;
   const int total = p.hidden * p.din + p.hidden * p.hidden + p.dout * p.hidden;
-  k_pack_weights<<<(total + 255) / 256, 256, 0, st>>>(p.params_h, p.o_w1, p.o_w2, p.o_w3, p.hidden, p.din, p.dout,
-                                                      p.packed, p.pk_w1, p.pk_w2, p.pk_w3);
+  k_pack_weights<<<(total + 255) / 256, 256, 0, st>>>(p.params_h, p.o_w1, p.o_w2, p.o_w3, p.hidden, p.din, p.k1,
+                                                      p.dout, p.packed, p.pk_w1, p.pk_w2, p.pk_w3);
   BPF_TRY(cudaGetLastError());
   return BPF_OK;
 }
@@ -298,15 +296,18 @@ int ProposalNet::alloc(int d, int hid, int cap_batch, int din_) {
   o_w3 = o_b2 + hidden;
   o_b3 = o_w3 + dout * hidden;
   nparams = o_b3 + dout;
+  k1 = (din + 15) / 16 * 16;
   pk_w1 = 0;
-  pk_w2 = pk_w1 + hidden * din * 2;
+  pk_w2 = pk_w1 + hidden * k1 * 2;
   pk_w3 = pk_w2 + hidden * hidden * 2;
-  pk_bytes = pk_w3 + dout * hidden * 2;
+  // W3's image holds whole 8-row core-matrix groups: dout rounded up to 16
+  pk_bytes = pk_w3 + (dout + 15) / 16 * 16 * hidden * 2;
   cap = cap_batch;
   auto A = [](void** p, size_t b) { return cudaMalloc(p, b) == cudaSuccess ? BPF_OK : BPF_E_NOMEM; };
   int rc = A((void**)&params, (size_t)nparams * 4);
   if (!rc) rc = A((void**)&params_h, (size_t)nparams * 2);
   if (!rc) rc = A((void**)&packed, (size_t)pk_bytes);
+  if (!rc && cudaMemset(packed, 0, (size_t)pk_bytes) != cudaSuccess) rc = BPF_E_CUDA;  // W1's padding columns
   if (!rc) rc = A((void**)&grads, (size_t)nparams * 4);
   if (!rc) rc = A((void**)&m1, (size_t)nparams * 4);
   if (!rc) rc = A((void**)&m2, (size_t)nparams * 4);

@@ -15,6 +15,7 @@ struct ProposalNet {
   // dim: the proposed variables (the L96 state's 40 components; the PZ
   // model's one log-noise), din: network inputs, dout = 2 dim: (delta, s)
   int dim = 0, din = 0, dout = 0, hidden = 0;
+  int k1 = 0;  // columns of W1's shared-memory image: din rounded up to a multiple of 16 (one MMA K step)
   // parameter vector: W1 [hidden x din], b1, W2 [hidden x hidden], b2,
   // W3 [dout x hidden], b3 (offsets in floats)
   int o_w1 = 0, o_b1 = 0, o_w2 = 0, o_b2 = 0, o_w3 = 0, o_b3 = 0, nparams = 0;
@@ -108,8 +109,8 @@ struct BatchGuidedArgs {
 int launch_batch_guided(ProposalNet& net, const BatchGuidedArgs& a, cudaStream_t st);
 
 // the guided step of every filter of a PZ batch (guided_pz.cu): the proposal
-// over each particle's log-noise, inputs and network as separate launches
-// over all the batch's columns (rows of U, H1, H2, O)
+// over each particle's log-noise; the network of every particle in one
+// launch, then the step
 struct PZParams;
 struct BatchPZGuidedArgs {
   const double* x_in;
@@ -129,9 +130,7 @@ struct BatchPZGuidedArgs {
   unsigned* counters;
   double* hist;
   int nf, k;
-  // network buffers, ld rows each
-  __nv_bfloat16 *U, *H1, *H2;
-  float* O;
+  float2* O;  // the network's (delta, raw s) per column, ld entries
 };
 int launch_batch_pz_guided(ProposalNet& net, const BatchPZGuidedArgs& a, cudaStream_t st);
 

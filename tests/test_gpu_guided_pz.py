@@ -17,17 +17,14 @@ pytestmark = pytest.mark.gpu
 def _states(model, n, steps=20, seed=9):
     """Particle states (n x 2, FP64, row-major) after `steps` unobserved days
     of the library's own PZ transition."""
-    import torch
-    from libbi_b200 import BatchedBootstrapPF
+    from libbi_b200 import BootstrapPF
 
-    b = BatchedBootstrapPF([model], [n], "systematic", [seed], ess_rel=0.5)
-    b.init()
+    pf = BootstrapPF(model, n, seed=seed)
     for k in range(steps):
-        b.step_device(float(k), float(k + 1), None)
-    x, _, _, offs = b.state()
-    xt = x[:, offs[0]:offs[0] + n].T.contiguous().clone()
-    torch.cuda.synchronize()
-    b.close()
+        pf.step(float(k), float(k + 1), None)
+    x, _, _ = pf.state()
+    xt = x[:, :n].T.contiguous().clone()
+    pf.close()
     return xt
 
 
