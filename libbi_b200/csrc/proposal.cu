@@ -205,7 +205,47 @@ __global__ void k_pack_weights(const __nv_bfloat16* __restrict__ Ph, int o_w1, i
   }
 }
 
+// the FP32 value b as three BF16 pieces: piece j of hi + mid + lo
+__device__ __forceinline__ __nv_bfloat16 bias_piece(float b, int j) {
+  const __nv_bfloat16 hi = __float2bfloat16(b);
+  if (j == 0) return hi;
+  const float r1 = b - __bfloat162float(hi);
+  const __nv_bfloat16 mid = __float2bfloat16(r1);
+  if (j == 1) return mid;
+  return __float2bfloat16(r1 - __bfloat162float(mid));
+}
+
+// the PZ network's images W1', W2', W3' (kPZNetK1 / kPZNetK2 columns)
+__global__ void k_pack_pz(const __nv_bfloat16* __restrict__ Ph, const float* __restrict__ P, int o_w1, int o_b1,
+                          int o_w2, int o_b2, int o_w3, unsigned char* __restrict__ out, int pk_w1, int pk_w2,
+                          int pk_w3) {
+  constexpr int H = kProposalHidden;
+  constexpr int n1 = H * kPZNetK1, n2 = H * kPZNetK2, n3 = kPZNetN3 * kPZNetK2;
+  const __nv_bfloat16 zero = __float2bfloat16(0.0f);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n1) {
+    const int n = i / kPZNetK1, k = i % kPZNetK1;
+    const __nv_bfloat16 v = k < 3 ? Ph[o_w1 + n * 3 + k] : k < 6 ? bias_piece(P[o_b1 + n], k - 3) : zero;
+    *reinterpret_cast<__nv_bfloat16*>(out + pk_w1 + tc::kmajor_off(n, k, kPZNetK1)) = v;
+  } else if (i < n1 + n2) {
+    const int j = i - n1, n = j / kPZNetK2, k = j % kPZNetK2;
+    const __nv_bfloat16 v = k < H ? Ph[o_w2 + n * H + k] : k < H + 3 ? bias_piece(P[o_b2 + n], k - H) : zero;
+    *reinterpret_cast<__nv_bfloat16*>(out + pk_w2 + tc::kmajor_off(n, k, kPZNetK2)) = v;
+  } else if (i < n1 + n2 + n3) {
+    const int j = i - n1 - n2, n = j / kPZNetK2, k = j % kPZNetK2;
+    const __nv_bfloat16 v = n < 2 && k < H ? Ph[o_w3 + n * H + k] : zero;
+    *reinterpret_cast<__nv_bfloat16*>(out + pk_w3 + tc::kmajor_off(n, k, kPZNetK2)) = v;
+  }
+}
+
 int pack_weights(ProposalNet& p, cudaStream_t st) {
+  if (p.pz) {
+    const int total = kProposalHidden * kPZNetK1 + kProposalHidden * kPZNetK2 + kPZNetN3 * kPZNetK2;
+    k_pack_pz<<<(total + 255) / 256, 256, 0, st>>>(p.params_h, p.params, p.o_w1, p.o_b1, p.o_w2, p.o_b2, p.o_w3,
+                                                   p.packed, p.pk_w1, p.pk_w2, p.pk_w3);
+    BPF_TRY(cudaGetLastError());
+    return BPF_OK;
+  }
   const int total = p.hidden * p.din + p.hidden * p.hidden + p.dout * p.hidden;
   k_pack_weights<<<(total + 255) / 256, 256, 0, st>>>(p.params_h, p.o_w1, p.o_w2, p.o_w3, p.hidden, p.din, p.k1,
                                                       p.dout, p.packed, p.pk_w1, p.pk_w2, p.pk_w3);
@@ -297,11 +337,18 @@ int ProposalNet::alloc(int d, int hid, int cap_batch, int din_) {
   o_b3 = o_w3 + dout * hidden;
   nparams = o_b3 + dout;
   k1 = (din + 15) / 16 * 16;
+  pz = din == 3 && dout == 2 && hidden == kProposalHidden;
   pk_w1 = 0;
-  pk_w2 = pk_w1 + hidden * k1 * 2;
-  pk_w3 = pk_w2 + hidden * hidden * 2;
-  // W3's image holds whole 8-row core-matrix groups: dout rounded up to 16
-  pk_bytes = pk_w3 + (dout + 15) / 16 * 16 * hidden * 2;
+  if (pz) {
+    pk_w2 = pk_w1 + hidden * kPZNetK1 * 2;
+    pk_w3 = pk_w2 + hidden * kPZNetK2 * 2;
+    pk_bytes = pk_w3 + kPZNetN3 * kPZNetK2 * 2;
+  } else {
+    pk_w2 = pk_w1 + hidden * k1 * 2;
+    pk_w3 = pk_w2 + hidden * hidden * 2;
+    // W3's image holds whole 8-row core-matrix groups: dout rounded up to 16
+    pk_bytes = pk_w3 + (dout + 15) / 16 * 16 * hidden * 2;
+  }
   cap = cap_batch;
   auto A = [](void** p, size_t b) { return cudaMalloc(p, b) == cudaSuccess ? BPF_OK : BPF_E_NOMEM; };
   int rc = A((void**)&params, (size_t)nparams * 4);

@@ -10,12 +10,21 @@ namespace bpf {
 constexpr int kProposalHidden = 128;
 // clamp of the proposal's log-scale s
 constexpr float kSMin = -7.0f, kSMax = 3.0f;
+// the PZ network's shared-memory images (guided_pz.cu): W1' = [W1 | b1 | 0]
+// (128 x 16), W2' = [W2 | b2 | 0] (128 x 144), W3' = [W3 | 0] (16 x 144);
+// each bias as three BF16 pieces hi + mid + lo (24 significant bits, the
+// FP32 value) in columns din .. din + 2, multiplied by constant-1 columns of
+// the activations
+constexpr int kPZNetK1 = 16, kPZNetK2 = kProposalHidden + 16, kPZNetN3 = 16;
 
 struct ProposalNet {
   // dim: the proposed variables (the L96 state's 40 components; the PZ
   // model's one log-noise), din: network inputs, dout = 2 dim: (delta, s)
   int dim = 0, din = 0, dout = 0, hidden = 0;
   int k1 = 0;  // columns of W1's shared-memory image: din rounded up to a multiple of 16 (one MMA K step)
+  // PZ network (din 3, dout 2): the images hold the biases of layers 1 and 2
+  // as extra K columns (kPZNetK1, kPZNetK2) and W3 padded to 16 rows
+  bool pz = false;
   // parameter vector: W1 [hidden x din], b1, W2 [hidden x hidden], b2,
   // W3 [dout x hidden], b3 (offsets in floats)
   int o_w1 = 0, o_b1 = 0, o_w2 = 0, o_b2 = 0, o_w3 = 0, o_b3 = 0, nparams = 0;
