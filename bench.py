@@ -1020,11 +1020,11 @@ def main():
         # the resampler's tile shape for this N (bpf_create tuned it; timed
         # again here so the line shows each shape's median)
         from libbi_b200 import autotune_resampler
-        from libbi_b200.filter import RESAMPLE_SHAPES
+        from libbi_b200.filter import RESAMPLE_SHAPES, shape_name
 
         best, us = autotune_resampler(N_PARTICLES)
-        line["autotune"] = {"systematic_resampler_n": N_PARTICLES, "shape": list(RESAMPLE_SHAPES[best]),
-                            "median_us": {f"{a}x{b}": v for (a, b), v in us.items()}}
+        line["autotune"] = {"systematic_resampler_n": N_PARTICLES, "shape": shape_name(RESAMPLE_SHAPES[best]),
+                            "median_us": {shape_name(k): v for k, v in us.items()}}
     if extras and not args.no_large_n:
         line["kernels_large_n"] = large_n_kernels()
     if extras and not args.no_batched:

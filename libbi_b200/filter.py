@@ -282,7 +282,16 @@ class StepResult:
     resampled: bool
 
 
-RESAMPLE_SHAPES = ((256, 2), (128, 4), (512, 1), (512, 2), (256, 4), (1024, 1))
+# (threads per block, particles per thread[, "cluster"]): the cooperative-
+# grid shapes, then the thread-block-cluster shapes (one cluster of at most
+# 16 CTAs)
+RESAMPLE_SHAPES = ((256, 2), (128, 4), (512, 1), (512, 2), (256, 4), (1024, 1),
+                   (1024, 4, "cluster"), (512, 8, "cluster"), (1024, 8, "cluster"))
+
+
+def shape_name(shape) -> str:
+    """'256x2', or 'cluster1024x4' for a cluster shape."""
+    return ("cluster" if len(shape) > 2 else "") + f"{shape[0]}x{shape[1]}"
 
 
 def autotune_resampler(n: int, stream=None):
