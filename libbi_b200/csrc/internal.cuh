@@ -183,12 +183,20 @@ struct ResampleScratch {
   int* o = nullptr;             // offspring counts (Metropolis)
   double* Ws = nullptr;         // FP64 cumulative weights (multinomial search)
   double* lu = nullptr;         // log sorted uniforms (multinomial)
-  unsigned* counters = nullptr; // last-block tickets
+  unsigned* counters = nullptr; // last-block tickets; word kEpochWord: the one-launch kernel's epoch
+  // block results the one-launch systematic kernel publishes (tagged words,
+  // kPubWords per tile; every tag 0xFFFFFFFF when allocated)
+  unsigned long long* pub = nullptr;
   StepStats* stats = nullptr;   // reduction results
   LwPartial* partials = nullptr;
   int max_partials = 0;
 };
 
+// the one-launch systematic kernel's epoch (a counters word) and the
+// published words per tile: three for the weight total, one for the
+// childless count, one for "phase 3 written"
+constexpr int kEpochWord = 10;
+constexpr int kPubWords = 5;
 int scratch_alloc(ResampleScratch& s, int max_n);
 void scratch_free(ResampleScratch& s);
 

@@ -17,9 +17,11 @@
 //   permute            survivors in place; copies fill childless slots by a
 //                      search over the cumulative extra-copy counts
 // Permuted systematic resampling runs all of these as phases of one
-// cooperative launch separated by bounded grid barriers (k_systematic_coop1
-// with one tile per block in one of six autotuned tile shapes, or
-// k_systematic_coop with several tiles per block); the passes above are the
+// cooperative launch: k_systematic_coop1 with one tile per block in one of
+// six autotuned tile shapes, its phases handing over through tagged words
+// that every block polls; k_systematic_cluster, one thread-block cluster
+// (three more shapes); or k_systematic_coop with several tiles per block
+// and bounded grid barriers.  The passes above are the
 // path for multinomial and Metropolis offspring.  The FP64 cumulative weight
 // of element i is the exact sum rounded once, so ancestors are independent
 // of tile order, tile shape, thread count and timing.
@@ -687,65 +689,93 @@ k_systematic_coop(const double* __restrict__ lw, int n, StepStats* st, const dou
 }
 
 // One tile per block (n <= G * NT * IT): each thread keeps its fixed-point
-// weights and cumulative offspring in registers across the grid barriers, so
-// after the log-weights are read the only global traffic is the G block
-// totals, the extra-copy index for the fill, and the ancestors.  NT threads
-// of IT particles each: the tile shapes in kCoopShapes, all computing the
-// same integers (the shape is chosen by the autotuner below).
-// *below = sum a[0..split), *all = sum a[0..count) (exact), computed by
-// warp 0 and shared with the block through one block barrier; once per
-// kernel (the result slots are this function's own)
-__device__ __forceinline__ void warp0_sum_pair_u128(const u128* a, int count, int split, u128* below, u128* all) {
-  __shared__ u128 s_res[2];
-  if (threadIdx.x < 32) {
-    u128 lo = u128_zero(), tot = u128_zero();
-    for (int i = threadIdx.x; i < count; i += 32) {
-      const u128 v = ldcg_u128(&a[i]);
-      tot = u128_add(tot, v);
-      if (i < split) lo = u128_add(lo, v);
-    }
-#pragma unroll
-    for (int d = 16; d > 0; d >>= 1) {
-      u128 o1, o2;
-      o1.lo = __shfl_xor_sync(0xffffffffu, lo.lo, d);
-      o1.hi = __shfl_xor_sync(0xffffffffu, lo.hi, d);
-      o2.lo = __shfl_xor_sync(0xffffffffu, tot.lo, d);
-      o2.hi = __shfl_xor_sync(0xffffffffu, tot.hi, d);
-      lo = u128_add(lo, o1);
-      tot = u128_add(tot, o2);
-    }
-    if (threadIdx.x == 0) {
-      s_res[0] = lo;
-      s_res[1] = tot;
-    }
-  }
-  __syncthreads();
-  *below = s_res[0];
-  *all = s_res[1];
+// weights and cumulative offspring in registers across the phases, so after
+// the log-weights are read the only global traffic is the G blocks'
+// published words, the extra-copy index for the fill, and the ancestors.
+// The phases hand over through tagged words (warp_poll_tagged) instead of
+// grid barriers: a block publishes its weight total, then its childless
+// count, then "E written", and each block's warp 0 polls every block's word
+// of the phase, which carries the data it waits for.  NT threads of IT
+// particles each: the tile shapes in kCoopShapes, all computing the same
+// integers (the shape is chosen by the autotuner below).
+// ---------------------------------------------------------------------------
+// Block results published as tagged words.  A word holds the launch's epoch
+// in its high half and 32 bits of payload in its low half, written by one
+// store, so a reader that finds the epoch has the payload with it.  The
+// readers of one transition poll all G blocks' words at once (every load of
+// a round in flight together) until each carries the epoch: no atomics, no
+// barrier, and the data arrives with the wait.  The epoch is a scratch word
+// every block reads at its start; block 0 advances it once it has seen every
+// block's first publication (so every block has read it), and the next
+// launch on the scratch publishes under the next value.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long tagged(unsigned epoch, unsigned payload) {
+  return ((unsigned long long)epoch << 32) | payload;
 }
 
-__device__ __forceinline__ void warp0_sum_pair_int(const int* a, int count, int split, int* below, int* all) {
-  __shared__ int s_res[2];
-  if (threadIdx.x < 32) {
-    int lo = 0, tot = 0;
-    for (int i = threadIdx.x; i < count; i += 32) {
-      const int v = __ldcg(&a[i]);
-      tot += v;
-      if (i < split) lo += v;
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ unsigned ld_relaxed_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Warp 0 polls words p[i * stride + k] (i < G, k < W) until every one
+// carries the epoch, W words of each of up to 128 entries in flight per
+// round; fn(i, words) then consumes entry i's payloads.  Bounded by the
+// barrier limit: returns false (warp-uniform) when it gave up.  Ends with an
+// acquire fence, so that what the publishers released before their words is
+// visible to this warp afterwards.
+template <int W, class F>
+__device__ __forceinline__ bool warp_poll_tagged(const unsigned long long* p, int stride, int G, unsigned epoch,
+                                                 F fn) {
+  const int lane = threadIdx.x & 31;
+  const long long lim = g_barrier_limit;
+  const long long t0 = clock64();
+  for (int base = 0; base < G; base += 128) {
+    unsigned long long w[4][W];
+    while (true) {
+      bool mine = true;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int i = base + 32 * u + lane;
+#pragma unroll
+        for (int k = 0; k < W; ++k) w[u][k] = i < G ? ld_relaxed_u64(p + (size_t)i * stride + k) : tagged(epoch, 0u);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int k = 0; k < W; ++k) mine &= (unsigned)(w[u][k] >> 32) == epoch;
+      if (__all_sync(0xffffffffu, mine)) break;
+      const int give_up = lane == 0 && (lim < 0 || clock64() - t0 > lim);
+      if (__shfl_sync(0xffffffffu, give_up, 0)) return false;
     }
 #pragma unroll
-    for (int d = 16; d > 0; d >>= 1) {
-      lo += __shfl_xor_sync(0xffffffffu, lo, d);
-      tot += __shfl_xor_sync(0xffffffffu, tot, d);
-    }
-    if (threadIdx.x == 0) {
-      s_res[0] = lo;
-      s_res[1] = tot;
+    for (int u = 0; u < 4; ++u) {
+      const int i = base + 32 * u + lane;
+      if (i < G) {
+        unsigned pl[W];
+#pragma unroll
+        for (int k = 0; k < W; ++k) pl[k] = (unsigned)w[u][k];
+        fn(i, pl);
+      }
     }
   }
-  __syncthreads();
-  *below = s_res[0];
-  *all = s_res[1];
+  __threadfence();
+  return true;
 }
 
 // IT log-weights of one thread (16-byte loads when IT is even and aligned)
@@ -771,13 +801,22 @@ template <int NT, int IT>
 __global__ void __launch_bounds__(NT)
 k_systematic_coop1(const double* __restrict__ lw, int n, StepStats* st, const double* a_in, uint64_t seed,
                    int step, int* Os_out, int* as, int* E, int* ecoarse, int coarse_shift, int* slot,
-                   u128* block_w, int* block_z, unsigned* bar_counter, unsigned* bar_gen, const int* gate) {
+                   unsigned long long* pub, int pub_stride, unsigned* epoch_word, const int* gate) {
   // the next kernel (the transition, a programmatic dependent) may be
-  // scheduled now; it waits for this kernel's completion before it reads
+  // scheduled now; it waits for this kernel's completion before it reads.
+  // This kernel is itself a programmatic dependent of the kernel before it
+  // (the transition that wrote the log-weights and the statistics): its
+  // blocks may be resident before that kernel has finished, and wait here.
   pdl_trigger();
+  pdl_wait();
   if (gate_closed(gate, st)) return;
+  // the epoch of this launch, read before this block publishes anything
+  const unsigned epoch = ld_relaxed_u32(epoch_word);
   extern __shared__ int s_coarse[];
   __shared__ int s_last[NT];
+  __shared__ u128 s_u128[2];
+  __shared__ int s_int[2];
+  __shared__ int s_ok;
   const int G = gridDim.x, b = blockIdx.x;
   const int i0 = b * (NT * IT) + threadIdx.x * IT;
   const double mx = st->mx;
@@ -802,12 +841,48 @@ k_systematic_coop1(const double* __restrict__ lw, int n, StepStats* st, const do
   }
   u128 btot;
   const u128 texcl = block_exclusive_scan_u128_nt<NT>(loc, &btot);
-  if (threadIdx.x == 0) block_w[b] = btot;
-  if (!grid_barrier(bar_counter, bar_gen, st)) return;
+  if (threadIdx.x == 0) {
+    // the total (< 2^80) as three 32-bit payloads
+    unsigned long long* mine = pub + (size_t)b * pub_stride;
+    st_relaxed_u64(mine + 0, tagged(epoch, (unsigned)btot.lo));
+    st_relaxed_u64(mine + 1, tagged(epoch, (unsigned)(btot.lo >> 32)));
+    st_relaxed_u64(mine + 2, tagged(epoch, (unsigned)btot.hi));
+  }
 
-  // phase 2: block prefix and total W; cumulative offspring (registers)
-  u128 prefix, total;
-  warp0_sum_pair_u128(block_w, G, b, &prefix, &total);
+  // phase 2: block prefix and total W from every block's published total;
+  // cumulative offspring (registers)
+  if (threadIdx.x < 32) {
+    u128 lo = u128_zero(), tot = u128_zero();
+    const bool ok = warp_poll_tagged<3>(pub, pub_stride, G, epoch, [&](int i, const unsigned* pl) {
+      u128 v;
+      v.lo = (unsigned long long)pl[0] | ((unsigned long long)pl[1] << 32);
+      v.hi = pl[2];
+      tot = u128_add(tot, v);
+      if (i < b) lo = u128_add(lo, v);
+    });
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+      u128 o1, o2;
+      o1.lo = __shfl_xor_sync(0xffffffffu, lo.lo, d);
+      o1.hi = __shfl_xor_sync(0xffffffffu, lo.hi, d);
+      o2.lo = __shfl_xor_sync(0xffffffffu, tot.lo, d);
+      o2.hi = __shfl_xor_sync(0xffffffffu, tot.hi, d);
+      lo = u128_add(lo, o1);
+      tot = u128_add(tot, o2);
+    }
+    if (threadIdx.x == 0) {
+      s_u128[0] = lo;
+      s_u128[1] = tot;
+      s_ok = ok;
+      // every block has published under this epoch, so every block has
+      // read it: the next launch may use the next one
+      if (ok && b == 0) *epoch_word = epoch + 1u;
+      if (!ok) st->status = BPF_E_TIMEOUT;
+    }
+  }
+  __syncthreads();
+  if (!s_ok) return;
+  const u128 prefix = s_u128[0], total = s_u128[1];
   const double W = u128_to_weight(total);
   if (!(W > 0.0)) {  // every block sees the same W and leaves here
     if (b == 0 && threadIdx.x == 0) st->status = BPF_E_DEGENERATE;
@@ -843,12 +918,30 @@ k_systematic_coop1(const double* __restrict__ lw, int n, StepStats* st, const do
   }
   int ztot;
   const int zexcl = block_exclusive_scan_int_nt<NT>(zl, &ztot);
-  if (threadIdx.x == 0) block_z[b] = ztot;
-  if (!grid_barrier(bar_counter, bar_gen, st)) return;
+  if (threadIdx.x == 0) st_relaxed_u64(pub + (size_t)b * pub_stride + 3, tagged(epoch, (unsigned)ztot));
 
   // phase 3: ranks of childless slots, E, survivors in place
-  int zprefix, R;
-  warp0_sum_pair_int(block_z, G, b, &zprefix, &R);
+  if (threadIdx.x < 32) {
+    int lo = 0, tot = 0;
+    const bool ok = warp_poll_tagged<1>(pub + 3, pub_stride, G, epoch, [&](int i, const unsigned* pl) {
+      tot += (int)pl[0];
+      if (i < b) lo += (int)pl[0];
+    });
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+      lo += __shfl_xor_sync(0xffffffffu, lo, d);
+      tot += __shfl_xor_sync(0xffffffffu, tot, d);
+    }
+    if (threadIdx.x == 0) {
+      s_int[0] = lo;
+      s_int[1] = tot;
+      s_ok = ok;
+      if (!ok) st->status = BPF_E_TIMEOUT;
+    }
+  }
+  __syncthreads();
+  if (!s_ok) return;
+  const int zprefix = s_int[0], R = s_int[1];
   {
     int Z = zprefix + zexcl;
     int prev = before0;
@@ -867,7 +960,20 @@ k_systematic_coop1(const double* __restrict__ lw, int n, StepStats* st, const do
       prev = os[k];
     }
   }
-  if (!grid_barrier(bar_counter, bar_gen, st)) return;
+  // this block's E, coarse entries, slots and survivors are written: publish
+  // that (a release, ordered after every thread's writes by the block
+  // barrier), then wait for every block's
+  __syncthreads();
+  if (threadIdx.x == 0) st_release_u64(pub + (size_t)b * pub_stride + 4, tagged(epoch, 1u));
+  if (threadIdx.x < 32) {
+    const bool ok = warp_poll_tagged<1>(pub + 4, pub_stride, G, epoch, [](int, const unsigned*) {});
+    if (threadIdx.x == 0) {
+      s_ok = ok;
+      if (!ok) st->status = BPF_E_TIMEOUT;
+    }
+  }
+  __syncthreads();
+  if (!s_ok) return;
 
   // phase 4: childless slot of rank r <- ancestor a with E_a <= r < E_{a+1}.
   // The coarse index (every 2^coarse_shift-th E) comes into shared memory
@@ -957,10 +1063,12 @@ __device__ __forceinline__ void warp_sum_split_int(int v, int b, int* below, int
 }
 
 // dynamic shared memory of a CTA: E of its TILE particles, its childless
-// slots in rank order, and the coarse index (every 16th E) of the cluster
+// slots in rank order, its own coarse entries (every 16th E, compact, for
+// the other CTAs to copy as 16-byte vectors) and the coarse index of the
+// cluster
 template <int NT, int IT>
 constexpr size_t cluster_smem(int C) {
-  return (size_t)(2 * NT * IT + C * (NT * IT / 16)) * sizeof(int);
+  return (size_t)(2 * NT * IT + (C + 1) * (NT * IT / 16)) * sizeof(int);
 }
 
 template <int NT, int IT>
@@ -979,11 +1087,13 @@ k_systematic_cluster(const double* __restrict__ lw, int n, StepStats* st, const 
   cg::cluster_group cl = cg::this_cluster();
   const int C = (int)cl.num_blocks(), b = (int)cl.block_rank();
   extern __shared__ __align__(16) int smem_cl[];
-  int* sE = smem_cl;        // TILE
-  int* sSlot = sE + TILE;   // TILE
-  int* sCoarse = sSlot + TILE;  // C * TC
-  __shared__ u128 s_btot, s_pt[2];
-  __shared__ int s_bz, s_zt[2];
+  int* sE = smem_cl;             // TILE
+  int* sSlot = sE + TILE;        // TILE
+  int* sMine = sSlot + TILE;     // TC: this CTA's coarse entries
+  int* sCoarse = sMine + TC;     // C * TC
+  // every CTA's total and childless count, pushed here by its owner
+  __shared__ u128 s_tot_all[kClusterMax], s_pt[2];
+  __shared__ int s_z_all[kClusterMax], s_zt[2];
   __shared__ int s_last[NT];
   const int tid = threadIdx.x;
   const int i0 = b * TILE + tid * IT;
@@ -1009,14 +1119,16 @@ k_systematic_cluster(const double* __restrict__ lw, int n, StepStats* st, const 
   }
   u128 btot;
   const u128 texcl = block_exclusive_scan_u128_nt<NT>(loc, &btot);
-  if (tid == 0) s_btot = btot;
+  // the total into every CTA's shared memory (stores, which the cluster
+  // barrier completes: nothing waits on a remote load)
+  if (tid < C) *cl.map_shared_rank(&s_tot_all[b], tid) = btot;
   cl.sync();
 
   // phase 2: the CTA's prefix and the total W from the CTAs' totals;
   // cumulative offspring (registers) and childless counts
   if (tid < 32) {
     u128 mine = u128_zero();
-    if (tid < C) mine = *cl.map_shared_rank(&s_btot, tid);
+    if (tid < C) mine = s_tot_all[tid];
     u128 below, all;
     warp_sum_split_u128(mine, b, &below, &all);
     if (tid == 0) {
@@ -1055,7 +1167,7 @@ k_systematic_cluster(const double* __restrict__ lw, int n, StepStats* st, const 
   }
   int ztot;
   const int zexcl = block_exclusive_scan_int_nt<NT>(zl, &ztot);
-  if (tid == 0) s_bz = ztot;
+  if (tid < C) *cl.map_shared_rank(&s_z_all[b], tid) = ztot;
   // SystematicResampler::cumulativeOffspring throws
   // ParticleFilterDegeneratedException unless W > 0
   // (share/src/bi/resampler/SystematicResampler.hpp:118-129)
@@ -1066,7 +1178,7 @@ k_systematic_cluster(const double* __restrict__ lw, int n, StepStats* st, const 
   // phase 3: ranks of the childless slots, E, survivors in place
   if (tid < 32) {
     int mine = 0;
-    if (tid < C) mine = *cl.map_shared_rank(&s_bz, tid);
+    if (tid < C) mine = s_z_all[tid];
     int below, all;
     warp_sum_split_int(mine, b, &below, &all);
     if (tid == 0) {
@@ -1085,6 +1197,7 @@ k_systematic_cluster(const double* __restrict__ lw, int n, StepStats* st, const 
       if (i < n) {
         const bool zero = os[k] == prev;
         sE[tid * IT + k] = prev - i + Z;  // E_i: extra copies of the particles before i
+        if (((tid * IT + k) & 15) == 0) sMine[(tid * IT + k) >> 4] = prev - i + Z;
         if (zero) sSlot[Z - zprefix] = i;
         else as[i] = i;
         if (Os_out) Os_out[i] = os[k];
@@ -1092,18 +1205,25 @@ k_systematic_cluster(const double* __restrict__ lw, int n, StepStats* st, const 
         prev = os[k];
       } else {
         sE[tid * IT + k] = INT_MAX;  // past the end: never an ancestor
+        if (((tid * IT + k) & 15) == 0) sMine[(tid * IT + k) >> 4] = INT_MAX;
       }
     }
   }
-  cl.sync();  // every CTA's E is in place
+  // this CTA's coarse entries into every CTA's coarse index (16-byte
+  // stores), completed by the cluster barrier with every CTA's E
+  __syncthreads();
+  {
+    constexpr int TC4 = TC / 4;  // 16-byte vectors of one CTA's coarse entries
+    const int4* src = reinterpret_cast<const int4*>(sMine);
+    for (int e = tid; e < C * TC4; e += NT)
+      reinterpret_cast<int4*>(cl.map_shared_rank(sCoarse, e / TC4))[b * TC4 + e % TC4] = src[e % TC4];
+  }
+  cl.sync();
 
   // phase 4: childless slot of rank r <- ancestor a with E_a <= r < E_{a+1}:
-  // the coarse index of the whole cluster into this CTA's shared memory,
-  // then per slot a search there and one 16-wide window of E read from the
-  // owning CTA as four 16-byte loads
+  // a search in the coarse index of the whole cluster, then one 16-wide
+  // window of E read from the owning CTA as four 16-byte loads
   const int nco = C * TC;
-  for (int e = tid; e < nco; e += NT) sCoarse[e] = cl.map_shared_rank(sE, e / TC)[16 * (e % TC)];
-  __syncthreads();
   for (int j = tid; j < ztot; j += NT) {
     const int r = zprefix + j;
     int lo = 0, hi = nco;
@@ -1428,8 +1548,14 @@ int scratch_alloc(ResampleScratch& s, int max_n) {
   ALLOC(s.counters, 16 * sizeof(unsigned));
   ALLOC(s.stats, sizeof(StepStats));
   ALLOC(s.partials, (size_t)s.max_partials * sizeof(LwPartial));
+  ALLOC(s.pub, T1 * kPubWords * sizeof(unsigned long long));
 #undef ALLOC
   if (cudaMemset(s.counters, 0, 16 * sizeof(unsigned)) != cudaSuccess) { scratch_free(s); return BPF_E_CUDA; }
+  // tags no epoch carries (the epoch starts at zero)
+  if (cudaMemset(s.pub, 0xFF, T1 * kPubWords * sizeof(unsigned long long)) != cudaSuccess) {
+    scratch_free(s);
+    return BPF_E_CUDA;
+  }
   StepStats z{};
   z.status = BPF_OK;
   if (cudaMemcpy(s.stats, &z, sizeof(z), cudaMemcpyHostToDevice) != cudaSuccess) { scratch_free(s); return BPF_E_CUDA; }
@@ -1438,7 +1564,8 @@ int scratch_alloc(ResampleScratch& s, int max_n) {
 
 void scratch_free(ResampleScratch& s) {
   void* ptrs[] = {s.tile_sum, s.tile_prefix, s.vtile_sum, s.vtile_prefix, s.zcount, s.zprefix,
-                  s.icount, s.iprefix, s.Os, s.E, s.slot, s.etile, s.o, s.Ws, s.lu, s.counters, s.stats, s.partials};
+                  s.icount, s.iprefix, s.Os, s.E, s.slot, s.etile, s.o, s.Ws, s.lu, s.counters, s.stats, s.partials,
+                  s.pub};
   for (void* p : ptrs) if (p) cudaFree(p);
   s = ResampleScratch();
 }
@@ -1733,17 +1860,31 @@ static int launch_coop1_shape(int k, const ResampleArgs& a, ResampleScratch& s, 
   int* E = s.E;
   int* ec = s.etile;
   int* slot = s.slot;
-  u128* bw = s.tile_sum;  // G block totals
-  int* bz = s.zcount;
-  unsigned* bc = s.counters + 8;
-  unsigned* bg = s.counters + 9;
+  unsigned long long* pub = s.pub;  // G blocks' published words
+  int pstride = kPubWords;
+  unsigned* ew = s.counters + kEpochWord;
   const int* gate = a.gate;
   int nn = n;
   int* Oo = Os_out;
+  if (!pub || G > s.max_tiles) return BPF_E_INVALID;
   void* args[] = {(void*)&lw, (void*)&nn, (void*)&stats, (void*)&a_in, (void*)&seed, (void*)&step, (void*)&Oo,
-                  (void*)&as, (void*)&E, (void*)&ec, (void*)&sh, (void*)&slot, (void*)&bw, (void*)&bz,
-                  (void*)&bc, (void*)&bg, (void*)&gate};
-  BPF_TRY(cudaLaunchCooperativeKernel(kCoopShapes[k].fn, dim3(G), dim3(kCoopShapes[k].nt), args, smem, st));
+                  (void*)&as, (void*)&E, (void*)&ec, (void*)&sh, (void*)&slot, (void*)&pub, (void*)&pstride,
+                  (void*)&ew, (void*)&gate};
+  // cooperative (every block resident: the blocks poll each other's
+  // words) and a programmatic dependent of the kernel before it
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute at[2];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[1].val.programmaticStreamSerializationAllowed = 1;
+  cfg.gridDim = dim3((unsigned)G);
+  cfg.blockDim = dim3((unsigned)kCoopShapes[k].nt);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cfg.attrs = at;
+  cfg.numAttrs = 2;
+  BPF_TRY(cudaLaunchKernelExC(&cfg, kCoopShapes[k].fn, args));
   return BPF_OK;
 }
 

@@ -39,9 +39,11 @@ constexpr size_t kOffEtile = kOffSlot + align256(kStaticMaxN * sizeof(int));
 constexpr size_t kOffCounters = kOffEtile + align256((kStaticMaxN / 16 + 2) * sizeof(int));
 constexpr size_t kOffStats = kOffCounters + align256(16 * sizeof(unsigned));
 constexpr size_t kOffPartials = kOffStats + align256(sizeof(StepStats));
-constexpr size_t kScratchBytes = kOffPartials + align256(kStaticPartials * sizeof(LwPartial));
+constexpr size_t kOffPub = kOffPartials + align256(kStaticPartials * sizeof(LwPartial));
+constexpr size_t kPubBytes = (size_t)(kStaticTiles + 1) * kPubWords * sizeof(unsigned long long);
+constexpr size_t kScratchBytes = kOffPub + align256(kPubBytes);
 
-// the scratch itself: zero at module load, under 1 MiB per device
+// the scratch itself: zero at module load, about 1 MiB per device
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;
@@ -90,10 +92,14 @@ extern "C" int bpf_systematic_ancestors_static(const double* lw, int n, const do
   s.stats = reinterpret_cast<StepStats*>(base + kOffStats);
   s.partials = reinterpret_cast<LwPartial*>(base + kOffPartials);
   s.max_partials = kStaticPartials;
+  s.pub = reinterpret_cast<unsigned long long*>(base + kOffPub);
   // the array keeps the previous call's contents: clear the last-block
-  // counters and the statistics (status = BPF_OK) before this call's kernels
+  // counters (the one-launch kernel's epoch among them) and the statistics
+  // (status = BPF_OK) before this call's kernels, and give the published
+  // words tags no epoch of this call carries
   BPF_TRY(cudaMemsetAsync(s.counters, 0, 16 * sizeof(unsigned), st));
   BPF_TRY(cudaMemsetAsync(s.stats, 0, sizeof(StepStats), st));
+  BPF_TRY(cudaMemsetAsync(s.pub, 0xFF, kPubBytes, st));
   ResampleArgs ra;
   ra.kind = BPF_RESAMPLER_SYSTEMATIC;
   ra.n = n;
