@@ -216,6 +216,14 @@ class ModelL96 {
 #include "bi/host/updater/StaticSamplerHost.hpp"
 #include "bi/host/updater/StaticUpdaterHost.hpp"
 #include "bi/host/updater/SparseStaticLogDensityHost.hpp"
+#include "bi/traits/resampler_traits.hpp"
+#include "bi/resampler/Resampler.hpp"
+#include "bi/resampler/SystematicResampler.hpp"
+#include "bi/host/resampler/ResamplerHost.hpp"
+#include "bi/primitive/vector_primitive.hpp"
+
+#include <chrono>
+#include <vector>
 
 namespace {
 void ensure_init_l96() {
@@ -263,6 +271,69 @@ int ref_l96_transition(double* x, int P, const double* z, double t1, double t2, 
   for (int p = 0; p < P; ++p)
     for (int i = 0; i < N; ++i) x[(size_t)p * N + i] = s.get(bi::D_VAR)(p, i);
   return 0;
+}
+
+/* The reference's filter loop on this model, timed (the CPU baseline of
+ * the benchmark): T steps of Filter<BootstrapPF>::filter
+ * (share/src/bi/filter/Filter.hpp:58-70), each BootstrapPF::step
+ * (share/src/bi/filter/BootstrapPF.hpp:158-181) run as
+ *   resample  Resampler<R>::resample's test s.ess < essRel * P, then
+ *             R::precompute and R::ancestorsPermute of the reference's
+ *             SystematicResampler, State::gather and set_elements(lws, ll)
+ *             (share/src/bi/resampler/Resampler.hpp:167-182)
+ *   predict   the transition block: StaticSamplerHost (noise),
+ *             RK4IntegratorHost (ode), StaticUpdaterHost (x <- x + eta)
+ *   correct   the observation block through SparseStaticLogDensityHost,
+ *             then ess_reduce for s.ess, lW and the log-likelihood
+ * on `threads` OpenMP threads (the reference's own parallel loops).  Draws
+ * come from the tape shim's cycling tables (nrm, uni: n values each), a
+ * load per draw, so the reference's generator cost is not counted.
+ *   x0  P x N initial states, particle-major;  y  T x N observations
+ * Returns the wall-clock seconds of the T steps; *ll the log-likelihood. */
+double ref_l96_filter_timed(const double* x0, int P, int T, const double* y, double dt, double ess_rel,
+                            int threads, const double* nrm, const double* uni, int n, double* ll) {
+  using namespace l96;
+  ensure_init_l96();
+  bi_omp_init(threads);
+  boost::random_tape::set(nullptr, 0);  // this thread draws from the tables too
+  boost::random_tape::cycle().nrm = nrm;
+  boost::random_tape::cycle().uni = uni;
+  boost::random_tape::cycle().n = (std::size_t)n;
+  bi::State<ModelL96, bi::ON_HOST> s(P);
+  for (int p = 0; p < P; ++p)
+    for (int i = 0; i < N; ++i) s.get(bi::D_VAR)(p, i) = x0[(size_t)p * N + i];
+  bi::host_vector<real> lws(P);
+  bi::set_elements(lws, real(0));
+  bi::Mask<bi::ON_HOST> mask(3);
+  mask.addDenseMask(Var2::ID, N);
+  static bi::Random rng(0);
+  bi::SystematicResampler R;
+  bi_ode_set(BI_REAL(0.01), BI_REAL(1.0e-3), BI_REAL(1.0e-3));
+  double ess = P, logLik = 0.0;
+  const auto t0 = std::chrono::steady_clock::now();
+  for (int k = 0; k < T; ++k) {
+    if (ess < ess_rel * P) {
+      bi::ScanResamplerPrecompute<bi::ON_HOST> pre;
+      bi::host_vector<int> as(P);
+      R.precompute(lws, pre);
+      R.ancestorsPermute(rng, lws, as, pre);
+      s.gather(as);
+      bi::set_elements(lws, real(logLik));
+    }
+    bi::StaticSamplerHost<ModelL96, noise_typelist>::samples(rng, s);
+    bi::RK4IntegratorHost<ModelL96, ode_typelist, real>::update(k * dt, (k + 1) * dt, s);
+    bi::StaticUpdaterHost<ModelL96, eval_typelist>::update(s);
+    for (int i = 0; i < N; ++i) s.get(bi::OY_VAR)(0, i) = y[(size_t)k * N + i];
+    bi::SparseStaticLogDensityHost<ModelL96, obs_typelist>::logDensities(s, mask, lws);
+    double lW;
+    ess = bi::ess_reduce(lws, &lW);
+    logLik = lW;
+  }
+  const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  boost::random_tape::cycle() = boost::random_tape::Cycle();
+  bi_omp_init(1);  // the parity entry points run on one thread
+  if (ll) *ll = logLik;
+  return secs;
 }
 
 }  // extern "C"

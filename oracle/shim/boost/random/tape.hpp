@@ -21,4 +21,26 @@ inline double next() {
   if (t.pos >= t.n) throw std::runtime_error("random tape exhausted");
   return t.data[t.pos++];
 }
+// Timing mode (no tape on this thread): draws cycle through process-wide
+// tables of standard normals and of uniforms filled by the timing harness,
+// each thread from its own position, at the cost of a load per draw.  Used
+// only to time the reference's filter loop on many threads, never for parity.
+struct Cycle { const double* nrm = nullptr; const double* uni = nullptr; std::size_t n = 0; };
+inline Cycle& cycle() { static Cycle c; return c; }
+inline std::size_t& cycle_pos() {
+  static thread_local std::size_t p = reinterpret_cast<std::size_t>(&p) / 64 * 2654435761u;
+  return p;
+}
+inline double next_normal() {
+  if (tape().data) return next();
+  const Cycle& c = cycle();
+  if (!c.nrm) throw std::runtime_error("random tape unset");
+  return c.nrm[cycle_pos()++ % c.n];
+}
+inline double next_uniform() {
+  if (tape().data) return next();
+  const Cycle& c = cycle();
+  if (!c.uni) throw std::runtime_error("random tape unset");
+  return c.uni[cycle_pos()++ % c.n];
+}
 }}
