@@ -698,6 +698,132 @@ def equal_mean_time(boot, ll_target):
     return pts[-1]["ms_per_run"], float(pts[-1]["n"]), False
 
 
+def strip_lls(x):
+    """The per-seed log-likelihoods (kept for the standard errors) left out
+    of the printed line."""
+    if isinstance(x, list):
+        return [strip_lls(v) for v in x]
+    if isinstance(x, dict):
+        return {k: strip_lls(v) for k, v in x.items() if k != "_lls"}
+    return x
+
+
+def equal_sd_ratios(boot, guided, reps=400):
+    """Batched against batched, equal deviation: the bootstrap rows
+    (N_i, sd_i, t_i) give log sd = a + b log N (least squares) and a device
+    time per particle (their mean of t_i / N_i); the bootstrap N that reaches
+    a guided row's sd is exp((log sd_g - a) / b), its time that N times the
+    per-particle time, and the ratio that time over the guided row's time.
+    Standard errors by resampling the seeds (the per-seed log-likelihoods of
+    every row, with replacement, `reps` times)."""
+    import numpy as np
+
+    rng = np.random.default_rng(17)
+    ln_n = np.log([b["n"] for b in boot])
+    per_particle = float(np.mean([b["ms_per_run"] / b["n"] for b in boot]))
+
+    def ratios(bsd, gsd):
+        slope, icpt = np.polyfit(ln_n, np.log(bsd), 1)
+        out = []
+        for gd, sd in zip(guided, gsd):
+            if slope >= 0:
+                out.append((float("nan"), float("nan")))
+                continue
+            n_eq = float(np.exp((np.log(sd) - icpt) / slope))
+            out.append((n_eq, n_eq * per_particle / gd["ms_per_run"]))
+        return slope, out
+
+    bsd = [b["ll_sd"] for b in boot]
+    gsd = [g["ll_sd"] for g in guided]
+    slope, point = ratios(bsd, gsd)
+    reps_r = []
+    for _ in range(reps):
+        rb = [np.std(rng.choice(b["_lls"], b["_lls"].size), ddof=1) for b in boot]
+        rg = [np.std(rng.choice(g["_lls"], g["_lls"].size), ddof=1) for g in guided]
+        reps_r.append([r for _, r in ratios(rb, rg)[1]])
+    reps_r = np.array(reps_r)
+    rows = []
+    lo_n, hi_n = min(b["n"] for b in boot), max(b["n"] for b in boot)
+    for k, gd in enumerate(guided):
+        n_eq, r = point[k]
+        col = reps_r[:, k]
+        col = col[np.isfinite(col)]
+        rows.append({"guided_n": gd["n"], "guided_ll_sd": gd["ll_sd"], "guided_ms_per_run": gd["ms_per_run"],
+                     "bootstrap_n_at_equal_sd": n_eq,
+                     "gpu_time_ratio_bootstrap_over_guided": r,
+                     "ratio_se": float(col.std(ddof=1)) if col.size > 1 else None,
+                     "bootstrap_n_is": "interpolated" if lo_n <= n_eq <= hi_n else "extrapolated"})
+    best = max(rows, key=lambda x: x["gpu_time_ratio_bootstrap_over_guided"]
+               if np.isfinite(x["gpu_time_ratio_bootstrap_over_guided"]) else -1.0)
+    return {"bootstrap_sd_exponent_in_n": float(slope), "bootstrap_ms_per_particle": per_particle, "rows": rows,
+            "best_ratio": best["gpu_time_ratio_bootstrap_over_guided"], "best_ratio_se": best["ratio_se"],
+            "best_guided_n": best["guided_n"],
+            "meets_10x": bool(np.isfinite(best["gpu_time_ratio_bootstrap_over_guided"])
+                              and best["gpu_time_ratio_bootstrap_over_guided"] >= 10.0)}
+
+
+def guided_informative(seeds=64, T=10, train_steps=1500, n_data=1 << 18):
+    """Both arms batched on Lorenz-96 d=40 with informative observations
+    (sigma_eta = 0.5 against sigma_y = 0.1, so that the transition scatters
+    the particles far wider than the observation pins the state): a
+    proposal trained for this model on 2^18 simulated triples, T = 10
+    observations of one seeded run, 64 seeds per row, equal-deviation device
+    time ratios with standard errors (equal_sd_ratios)."""
+    import numpy as np
+    import torch
+    from dataclasses import replace
+    from libbi_b200 import BatchedBootstrapPF, BootstrapPF, LearnedProposal, configs
+
+    model = replace(configs.L96_D40_N65536["model"], sigma_eta=0.5, sigma_y=0.1)
+    sim = BootstrapPF(model, n_data, seed=5)
+    for k in range(40):
+        sim.step_device(k * DT, (k + 1) * DT, None, sync=False)
+    x, _, _ = sim.state()
+    xt = x[:, :n_data].T.contiguous().clone()
+    sim.step_device(40 * DT, 41 * DT, None, sync=False)
+    x, _, _ = sim.state()
+    xt1 = x[:, :n_data].T.contiguous().clone()
+    g = torch.Generator(device="cuda")
+    g.manual_seed(5)
+    yt1 = (xt1 + model.sigma_y * torch.randn(xt1.shape, generator=g, device="cuda")).contiguous()
+    sim.close()
+    prop = LearnedProposal(model, DT, max_batch=8192, seed=5)
+    prop.set_data(xt, xt1, yt1)
+    trace = prop.train(train_steps, 8192, 2e-3)
+    del xt, xt1, yt1
+    truth = BootstrapPF(model, 1, seed=77)
+    xs = np.zeros((T, DIM), np.float32)
+    for k in range(T):
+        truth.step(k * DT, (k + 1) * DT, None)
+        x, _, _ = truth.state()
+        xs[k] = x[:, 0].cpu().numpy()
+    truth.close()
+    y = (xs + model.sigma_y * np.random.default_rng(78).standard_normal(xs.shape)).astype(np.float32)
+
+    def run_batched(n, use_prop):
+        b = BatchedBootstrapPF([model] * seeds, [n] * seeds, "systematic", [20_000 + s for s in range(seeds)],
+                               ess_rel=ESS_REL)
+        if use_prop:
+            b.set_proposal(prop)
+        yb = np.ascontiguousarray(np.repeat(y[:, None, :], seeds, axis=1))
+        b.filter(yb, 0.0, DT)  # capture
+        b.timing(True)
+        b.timing_read(reset=True)
+        lls, _, _, st = b.filter(yb, 0.0, DT)
+        ms, _ = b.timing_read(reset=True)
+        b.close()
+        return {"n": n, "filters": seeds, "ll_mean": float(lls.mean()), "ll_sd": float(lls.std(ddof=1)),
+                "ms_per_run": ms / seeds, "failed": int((st != 0).sum()), "_lls": lls}
+
+    boot = [run_batched(n, False) for n in (4096, 16384, 32768)]
+    guided = [run_batched(n, True) for n in (256, 1024, 4096)]
+    prop.close()
+    return {"model": {"sigma_eta": model.sigma_eta, "sigma_y": model.sigma_y, "T": T},
+            "train": {"triples": n_data, "steps": train_steps, "loss_first": float(trace[:10].mean()),
+                      "loss_last": float(trace[-50:].mean())},
+            "bootstrap": strip_lls(boot), "guided": strip_lls(guided), "equal_sd": equal_sd_ratios(boot, guided)}
+
+
 def guided_vs_bootstrap(y_host, seeds=64, n_guided=(4096, 16384, 65536),
                         n_boot=(16384, 65536, 262144, 1 << 20, 1 << 22), n_ref=65536, n_data=1 << 20,
                         train_steps=3000, n_guided_batched=(1024, 4096, 16384), n_boot_batched=(16384, 32768)):
@@ -778,7 +904,7 @@ def guided_vs_bootstrap(y_host, seeds=64, n_guided=(4096, 16384, 65536),
         ms, _ = b.timing_read(reset=True)
         b.close()
         return {"n": n, "filters": seeds, "ll_mean": float(lls.mean()), "ll_sd": float(lls.std(ddof=1)),
-                "ms_per_run": ms / seeds, "batch_ms": ms, "failed": int((st != 0).sum())}
+                "ms_per_run": ms / seeds, "batch_ms": ms, "failed": int((st != 0).sum()), "_lls": lls}
 
     boot = [run(n, False) for n in n_boot]
     guided = [run(n, True) for n in n_guided]
@@ -789,7 +915,9 @@ def guided_vs_bootstrap(y_host, seeds=64, n_guided=(4096, 16384, 65536),
     short = {"T": 10,
              "bootstrap": [run_batched(n, False, 10) for n in (4096, 16384, 32768)],
              "guided": [run_batched(n, True, 10) for n in (1024, 4096, 16384)]}
+    short["equal_sd"] = equal_sd_ratios(short["bootstrap"], short["guided"])
     prop.close()
+    informative = guided_informative(seeds=seeds)
     # the bootstrap filter's best measured cost per particle-step (single or
     # batched): the conservative price of a bootstrap filter of any size
     T = len(y_host)
@@ -835,7 +963,17 @@ def guided_vs_bootstrap(y_host, seeds=64, n_guided=(4096, 16384, 65536),
                  # near 0: the deviation does not fall with N, so matching
                  # it says little about the estimator (the mean
                  # log-likelihood comparisons do)
-                 "bootstrap_sd_exponent_in_n": slope}
+                 "bootstrap_sd_exponent_in_n": slope,
+                 # equal footing (both batched, the deviation falling with N):
+                 # the C4 model over its first 10 observations, and a model
+                 # whose observations are informative
+                 "equal_footing_batched": {
+                     "c4_model_T10": {k: short["equal_sd"][k] for k in
+                                      ("best_ratio", "best_ratio_se", "best_guided_n", "meets_10x",
+                                       "bootstrap_sd_exponent_in_n")},
+                     "informative_T10": {k: informative["equal_sd"][k] for k in
+                                         ("best_ratio", "best_ratio_se", "best_guided_n", "meets_10x",
+                                          "bootstrap_sd_exponent_in_n")}}}
     best_m = max(guided, key=lambda gd: gd["gpu_time_ratio_bootstrap_over_guided_at_equal_mean_ll"])
     best_b = max(guided_b, key=lambda gd: gd["gpu_time_ratio_bootstrap_over_guided_at_equal_mean_ll"])
     return {
@@ -847,8 +985,9 @@ def guided_vs_bootstrap(y_host, seeds=64, n_guided=(4096, 16384, 65536),
                                                          + 0.5))},
         "bootstrap": boot,
         "guided": guided,
-        "batched": {"guided": guided_b, "bootstrap": boot_b},
-        "short_horizon_batched": short,
+        "batched": {"guided": strip_lls(guided_b), "bootstrap": strip_lls(boot_b)},
+        "short_horizon_batched": strip_lls(short),
+        "informative_observations_batched": informative,
         "named_comparison": named,
         "bootstrap_sd_exponent_in_n": slope,
         "best": {"equal_sd": {"guided_n": best["n"], "gpu_time_ratio_bootstrap_over_guided":
