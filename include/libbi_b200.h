@@ -319,19 +319,16 @@ int bpf_resampler_timing_enable(bpf_resampler* r, int enable);
 int bpf_resampler_timing_read(bpf_resampler* r, int reset, double* ms, int* calls);
 
 /* Autotuner of the one-launch systematic resampler (no counterpart in the
- * reference): tile shapes of threads per block x particles per thread of
- * the cooperative-grid kernel (0: 256 x 2, 1: 128 x 4, 2: 512 x 1,
- * 3: 512 x 2, 4: 256 x 4, 5: 1024 x 1) and of the thread-block-cluster
- * kernel, one cluster of at most 16 CTAs (6: 1024 x 4, 7: 512 x 8,
- * 8: 1024 x 8; n up to 16 tiles), all computing the same ancestors.
- * bpf_autotune_resampler times every shape that fits the GPU in one wave on
- * seeded synthetic
+ * reference): tile shapes of threads per block x particles per thread
+ * (0: 256 x 2, 1: 128 x 4, 2: 512 x 1, 3: 512 x 2, 4: 256 x 4,
+ * 5: 1024 x 1), all computing the same ancestors.  bpf_autotune_resampler
+ * times every shape that fits the GPU in one wave on seeded synthetic
  * log-weights of n particles (on `stream`, which it synchronises; not
  * while the stream is being captured) and keeps the fastest for n's size
  * class (the next power of two) on the current device for the rest of the
  * process; bpf_create runs it for its N.  out (may be NULL) receives the
  * chosen shape and each shape's median microseconds (0: does not fit). */
-#define BPF_RESAMPLE_SHAPES 9
+#define BPF_RESAMPLE_SHAPES 6
 typedef struct {
   int shape;
   double us[BPF_RESAMPLE_SHAPES];

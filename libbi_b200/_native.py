@@ -101,7 +101,7 @@ class Smc2Config(ctypes.Structure):
     ]
 
 
-RESAMPLE_SHAPES = 9  # BPF_RESAMPLE_SHAPES
+RESAMPLE_SHAPES = 6  # BPF_RESAMPLE_SHAPES
 
 
 class TuneResult(ctypes.Structure):

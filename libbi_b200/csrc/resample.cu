@@ -19,18 +19,14 @@
 // Permuted systematic resampling runs all of these as phases of one
 // cooperative launch: k_systematic_coop1 with one tile per block in one of
 // six autotuned tile shapes, its phases handing over through tagged words
-// that every block polls; k_systematic_cluster, one thread-block cluster
-// (three more shapes); or k_systematic_coop with several tiles per block
+// that every block polls, or k_systematic_coop with several tiles per block
 // and bounded grid barriers.  The passes above are the
 // path for multinomial and Metropolis offspring.  The FP64 cumulative weight
 // of element i is the exact sum rounded once, so ancestors are independent
 // of tile order, tile shape, thread count and timing.
 #include "internal.cuh"
 
-#include <cooperative_groups.h>
-
 #include <algorithm>
-#include <climits>
 #include <mutex>
 #include <vector>
 #include "resample_common.cuh"
@@ -1020,232 +1016,6 @@ k_systematic_coop1(const double* __restrict__ lw, int n, StepStats* st, const do
 }
 
 // ---------------------------------------------------------------------------
-// One thread-block cluster (at most 16 CTAs of NT threads x IT particles):
-// the same four phases as k_systematic_coop1, with the hardware cluster
-// barrier in place of the grid barriers and distributed shared memory in
-// place of global scratch.  Each CTA keeps its fixed-point weights and
-// cumulative offspring in registers and its E values and childless slots in
-// its own shared memory; the block totals, childless counts and the E
-// windows of the fill are read from the other CTAs' shared memory.  Global
-// memory sees the log-weights read once and the ancestors written once.
-// ---------------------------------------------------------------------------
-constexpr int kClusterMax = 16;
-
-// sum over the lanes c < C of warp 0 of v_c: *below = sum over c < b, *all =
-// sum over every c (exact, 128-bit); called by every lane of warp 0
-__device__ __forceinline__ void warp_sum_split_u128(u128 v, int b, u128* below, u128* all) {
-  const int lane = threadIdx.x & 31;
-  u128 lo = lane < b ? v : u128_zero(), tot = v;
-#pragma unroll
-  for (int d = 16; d > 0; d >>= 1) {
-    u128 o1, o2;
-    o1.lo = __shfl_xor_sync(0xffffffffu, lo.lo, d);
-    o1.hi = __shfl_xor_sync(0xffffffffu, lo.hi, d);
-    o2.lo = __shfl_xor_sync(0xffffffffu, tot.lo, d);
-    o2.hi = __shfl_xor_sync(0xffffffffu, tot.hi, d);
-    lo = u128_add(lo, o1);
-    tot = u128_add(tot, o2);
-  }
-  *below = lo;
-  *all = tot;
-}
-
-__device__ __forceinline__ void warp_sum_split_int(int v, int b, int* below, int* all) {
-  const int lane = threadIdx.x & 31;
-  int lo = lane < b ? v : 0, tot = v;
-#pragma unroll
-  for (int d = 16; d > 0; d >>= 1) {
-    lo += __shfl_xor_sync(0xffffffffu, lo, d);
-    tot += __shfl_xor_sync(0xffffffffu, tot, d);
-  }
-  *below = lo;
-  *all = tot;
-}
-
-// dynamic shared memory of a CTA: E of its TILE particles, its childless
-// slots in rank order, its own coarse entries (every 16th E, compact, for
-// the other CTAs to copy as 16-byte vectors) and the coarse index of the
-// cluster
-template <int NT, int IT>
-constexpr size_t cluster_smem(int C) {
-  return (size_t)(2 * NT * IT + (C + 1) * (NT * IT / 16)) * sizeof(int);
-}
-
-template <int NT, int IT>
-__global__ void __launch_bounds__(NT, 1)
-k_systematic_cluster(const double* __restrict__ lw, int n, StepStats* st, const double* a_in, uint64_t seed,
-                     int step, int* Os_out, int* as, const int* gate) {
-  namespace cg = cooperative_groups;
-  constexpr int TILE = NT * IT, TC = TILE / 16;
-  static_assert(TILE % 64 == 0, "whole 16-particle windows per CTA");
-  // the transition, a programmatic dependent, may be scheduled now; it waits
-  // for this kernel's completion before it reads
-  pdl_trigger();
-  // one word read by every CTA before any of them can change it (the
-  // degenerate status is written after the first cluster barrier)
-  if (gate_closed(gate, st)) return;
-  cg::cluster_group cl = cg::this_cluster();
-  const int C = (int)cl.num_blocks(), b = (int)cl.block_rank();
-  extern __shared__ __align__(16) int smem_cl[];
-  int* sE = smem_cl;             // TILE
-  int* sSlot = sE + TILE;        // TILE
-  int* sMine = sSlot + TILE;     // TC: this CTA's coarse entries
-  int* sCoarse = sMine + TC;     // C * TC
-  // every CTA's total and childless count, pushed here by its owner
-  __shared__ u128 s_tot_all[kClusterMax], s_pt[2];
-  __shared__ int s_z_all[kClusterMax], s_zt[2];
-  __shared__ int s_last[NT];
-  const int tid = threadIdx.x;
-  const int i0 = b * TILE + tid * IT;
-  const double mx = st->mx;
-  double a;
-  if (a_in) {
-    a = *a_in;
-  } else {
-    bpf_u32x4 r = bpf_draw(seed, 0u, (uint32_t)step, 0u, BPF_RNG_SYSTEMATIC);
-    a = bpf_u01d(r.v[0], r.v[1]);
-  }
-
-  // phase 1: fixed-point weights (registers) and the CTA total
-  double v[IT];
-  load_items<IT>(lw, i0, n, v);
-  unsigned long long q[IT];
-  u128 loc = u128_zero();
-#pragma unroll
-  for (int k = 0; k < IT; ++k) {
-    q[k] = (i0 + k < n) ? weight_to_fixed(nanexp(__dsub_rn(v[k], mx))) : 0ull;
-    u128 qq; qq.lo = q[k]; qq.hi = 0;
-    loc = u128_add(loc, qq);
-  }
-  u128 btot;
-  const u128 texcl = block_exclusive_scan_u128_nt<NT>(loc, &btot);
-  // the total into every CTA's shared memory (stores, which the cluster
-  // barrier completes: nothing waits on a remote load)
-  if (tid < C) *cl.map_shared_rank(&s_tot_all[b], tid) = btot;
-  cl.sync();
-
-  // phase 2: the CTA's prefix and the total W from the CTAs' totals;
-  // cumulative offspring (registers) and childless counts
-  if (tid < 32) {
-    u128 mine = u128_zero();
-    if (tid < C) mine = s_tot_all[tid];
-    u128 below, all;
-    warp_sum_split_u128(mine, b, &below, &all);
-    if (tid == 0) {
-      s_pt[0] = below;
-      s_pt[1] = all;
-    }
-  }
-  __syncthreads();
-  const u128 prefix = s_pt[0];
-  const double W = u128_to_weight(s_pt[1]);
-  // every CTA sees the same W: the branch is uniform over the cluster
-  const bool degenerate = !(W > 0.0);
-  const double nd = (double)n;
-  const double yW = degenerate ? 0.0 : __ddiv_rn(1.0, W);
-  int os[IT];
-  int before0 = 0, zl = 0;
-  if (!degenerate) {
-    u128 Q = u128_add(prefix, texcl);
-#pragma unroll
-    for (int k = 0; k < IT; ++k) {
-      u128 qq; qq.lo = q[k]; qq.hi = 0;
-      Q = u128_add(Q, qq);
-      os[k] = systematic_Os(u128_to_weight(Q), W, yW, nd, a, n);
-    }
-    s_last[tid] = os[IT - 1];
-  }
-  __syncthreads();
-  if (!degenerate) {
-    before0 = tid > 0 ? s_last[tid - 1] : (b == 0 ? 0 : systematic_Os(u128_to_weight(prefix), W, yW, nd, a, n));
-    int prev = before0;
-#pragma unroll
-    for (int k = 0; k < IT; ++k) {
-      if (i0 + k < n) zl += (os[k] == prev);
-      prev = os[k];
-    }
-  }
-  int ztot;
-  const int zexcl = block_exclusive_scan_int_nt<NT>(zl, &ztot);
-  if (tid < C) *cl.map_shared_rank(&s_z_all[b], tid) = ztot;
-  // SystematicResampler::cumulativeOffspring throws
-  // ParticleFilterDegeneratedException unless W > 0
-  // (share/src/bi/resampler/SystematicResampler.hpp:118-129)
-  if (degenerate && b == 0 && tid == 0) st->status = BPF_E_DEGENERATE;
-  cl.sync();  // the totals are read; the childless counts are in place
-  if (degenerate) return;
-
-  // phase 3: ranks of the childless slots, E, survivors in place
-  if (tid < 32) {
-    int mine = 0;
-    if (tid < C) mine = s_z_all[tid];
-    int below, all;
-    warp_sum_split_int(mine, b, &below, &all);
-    if (tid == 0) {
-      s_zt[0] = below;
-      s_zt[1] = all;
-    }
-  }
-  __syncthreads();
-  const int zprefix = s_zt[0];
-  {
-    int Z = zprefix + zexcl;
-    int prev = before0;
-#pragma unroll
-    for (int k = 0; k < IT; ++k) {
-      const int i = i0 + k;
-      if (i < n) {
-        const bool zero = os[k] == prev;
-        sE[tid * IT + k] = prev - i + Z;  // E_i: extra copies of the particles before i
-        if (((tid * IT + k) & 15) == 0) sMine[(tid * IT + k) >> 4] = prev - i + Z;
-        if (zero) sSlot[Z - zprefix] = i;
-        else as[i] = i;
-        if (Os_out) Os_out[i] = os[k];
-        Z += zero;
-        prev = os[k];
-      } else {
-        sE[tid * IT + k] = INT_MAX;  // past the end: never an ancestor
-        if (((tid * IT + k) & 15) == 0) sMine[(tid * IT + k) >> 4] = INT_MAX;
-      }
-    }
-  }
-  // this CTA's coarse entries into every CTA's coarse index (16-byte
-  // stores), completed by the cluster barrier with every CTA's E
-  __syncthreads();
-  {
-    constexpr int TC4 = TC / 4;  // 16-byte vectors of one CTA's coarse entries
-    const int4* src = reinterpret_cast<const int4*>(sMine);
-    for (int e = tid; e < C * TC4; e += NT)
-      reinterpret_cast<int4*>(cl.map_shared_rank(sCoarse, e / TC4))[b * TC4 + e % TC4] = src[e % TC4];
-  }
-  cl.sync();
-
-  // phase 4: childless slot of rank r <- ancestor a with E_a <= r < E_{a+1}:
-  // a search in the coarse index of the whole cluster, then one 16-wide
-  // window of E read from the owning CTA as four 16-byte loads
-  const int nco = C * TC;
-  for (int j = tid; j < ztot; j += NT) {
-    const int r = zprefix + j;
-    int lo = 0, hi = nco;
-    while (lo < hi) {
-      const int mid = (lo + hi) >> 1;
-      if (sCoarse[mid] <= r) lo = mid + 1; else hi = mid;
-    }
-    const int w0 = 16 * (lo - 1);  // sCoarse[0] = E_0 = 0 <= r
-    const int c = w0 / TILE;
-    const int4* win = reinterpret_cast<const int4*>(cl.map_shared_rank(sE, c) + (w0 - c * TILE));
-    int cnt = 0;
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int4 ev = win[u];
-      cnt += (ev.x <= r) + (ev.y <= r) + (ev.z <= r) + (ev.w <= r);
-    }
-    as[sSlot[j]] = w0 + cnt - 1;
-  }
-  cl.sync();  // no CTA leaves while another still reads its shared memory
-}
-
-// ---------------------------------------------------------------------------
 // cumulative offspring from offspring counts o[] (Metropolis) or from sorted
 // ancestors (multinomial), with childless counts per tile
 // ---------------------------------------------------------------------------
@@ -1677,29 +1447,14 @@ int launch_resample(const ResampleArgs& a, ResampleScratch& s, cudaStream_t st) 
 struct CoopShape {
   int nt, it;        // threads per block, particles per thread
   const void* fn;    // the kernel instantiation
-  bool cluster;      // k_systematic_cluster (one cluster of at most 16 CTAs) instead of a cooperative grid
 };
 // every tile holds at least kTile particles, so the block totals fit the
 // scratch sized for kTile tiles
 static const CoopShape kCoopShapes[BPF_RESAMPLE_SHAPES] = {
-    {256, 2, (const void*)k_systematic_coop1<256, 2>, false},
-    {128, 4, (const void*)k_systematic_coop1<128, 4>, false},
-    {512, 1, (const void*)k_systematic_coop1<512, 1>, false},
-    {512, 2, (const void*)k_systematic_coop1<512, 2>, false},
-    {256, 4, (const void*)k_systematic_coop1<256, 4>, false},
-    {1024, 1, (const void*)k_systematic_coop1<1024, 1>, false},
-    {1024, 4, (const void*)k_systematic_cluster<1024, 4>, true},
-    {512, 8, (const void*)k_systematic_cluster<512, 8>, true},
-    {1024, 8, (const void*)k_systematic_cluster<1024, 8>, true},
+    {256, 2, (const void*)k_systematic_coop1<256, 2>}, {128, 4, (const void*)k_systematic_coop1<128, 4>},
+    {512, 1, (const void*)k_systematic_coop1<512, 1>}, {512, 2, (const void*)k_systematic_coop1<512, 2>},
+    {256, 4, (const void*)k_systematic_coop1<256, 4>}, {1024, 1, (const void*)k_systematic_coop1<1024, 1>},
 };
-
-static size_t cluster_smem_of(int k, int C) {
-  switch (k) {
-    case 6: return cluster_smem<1024, 4>(C);
-    case 7: return cluster_smem<512, 8>(C);
-    default: return cluster_smem<1024, 8>(C);
-  }
-}
 
 // process-wide autotuned shape per device and size class (ceil log2 n);
 // -1: not tuned, -2: no shape fits in one wave (the default shape 0, or
@@ -1742,10 +1497,6 @@ struct CoopDevice {
   size_t smem[BPF_RESAMPLE_SHAPES] = {};     // shared memory the cached occupancy is for
   int per[BPF_RESAMPLE_SHAPES] = {};         // resident blocks per SM of each shape
   bool have[BPF_RESAMPLE_SHAPES] = {};
-  // cluster shapes: attributes set, and whether a cluster of C CTAs can be
-  // resident (0: not asked yet, 1: yes, -1: no)
-  bool cl_attr[BPF_RESAMPLE_SHAPES] = {};
-  signed char cl_fits[BPF_RESAMPLE_SHAPES][kClusterMax + 1] = {};
 };
 static std::mutex g_coop_mu;
 static CoopDevice g_coop[kMaxCoopDevices];
@@ -1785,66 +1536,10 @@ static int shape_per_sm(CoopDevice& d, int k, size_t smem) {
   return d.per[k];
 }
 
-// the cluster launch of shape k for n particles: one cluster of
-// C = ceil(n / tile) CTAs; BPF_E_INVALID when C exceeds 16 or the GPU cannot
-// hold such a cluster
-static int launch_cluster_shape(int k, const ResampleArgs& a, ResampleScratch& s, int* Os_out, CoopDevice& d,
-                                cudaStream_t st) {
-  const int n = a.n;
-  const int tile = kCoopShapes[k].nt * kCoopShapes[k].it;
-  const int C = (n + tile - 1) / tile;
-  if (C < 1 || C > kClusterMax) return BPF_E_INVALID;
-  const size_t smem = cluster_smem_of(k, C);
-  cudaLaunchConfig_t cfg = {};
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeClusterDimension;
-  at[0].val.clusterDim.x = (unsigned)C;
-  at[0].val.clusterDim.y = 1;
-  at[0].val.clusterDim.z = 1;
-  cfg.gridDim = dim3((unsigned)C);
-  cfg.blockDim = dim3((unsigned)kCoopShapes[k].nt);
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = st;
-  cfg.attrs = at;
-  cfg.numAttrs = 1;
-  {
-    std::lock_guard<std::mutex> lk(g_coop_mu);
-    if (!d.cl_attr[k]) {
-      BPF_TRY(cudaFuncSetAttribute(kCoopShapes[k].fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-      BPF_TRY(cudaFuncSetAttribute(kCoopShapes[k].fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)cluster_smem_of(k, kClusterMax)));
-      d.cl_attr[k] = true;
-    }
-    if (d.cl_fits[k][C] == 0) {
-      int clusters = 0;
-      if (cudaOccupancyMaxActiveClusters(&clusters, kCoopShapes[k].fn, &cfg) != cudaSuccess) {
-        cudaGetLastError();
-        clusters = 0;
-      }
-      d.cl_fits[k][C] = clusters > 0 ? 1 : -1;
-    }
-    if (d.cl_fits[k][C] < 0) return BPF_E_INVALID;
-  }
-  const double* lw = a.lw;
-  int nn = n;
-  StepStats* stats = s.stats;
-  const double* a_in = a.uniforms;
-  uint64_t seed = a.seed;
-  int step = a.step;
-  int* Oo = Os_out;
-  int* as = a.as;
-  const int* gate = a.gate;
-  void* args[] = {(void*)&lw, (void*)&nn, (void*)&stats, (void*)&a_in, (void*)&seed, (void*)&step,
-                  (void*)&Oo, (void*)&as, (void*)&gate};
-  BPF_TRY(cudaLaunchKernelExC(&cfg, kCoopShapes[k].fn, args));
-  return BPF_OK;
-}
-
 // launch shape k of the one-launch kernel if its tiles fit the GPU in one
 // wave; BPF_E_INVALID when they do not
 static int launch_coop1_shape(int k, const ResampleArgs& a, ResampleScratch& s, int* Os_out, CoopDevice& d,
                               cudaStream_t st) {
-  if (kCoopShapes[k].cluster) return launch_cluster_shape(k, a, s, Os_out, d, st);
   const int n = a.n;
   const int tile = kCoopShapes[k].nt * kCoopShapes[k].it;
   const int G = (n + tile - 1) / tile;
@@ -1969,8 +1664,7 @@ int autotune_systematic(int n, cudaStream_t st, int* best, double* us) {
   bool any = false;
   for (int k = 0; k < BPF_RESAMPLE_SHAPES; ++k) {
     const int tile = kCoopShapes[k].nt * kCoopShapes[k].it;
-    any |= kCoopShapes[k].cluster ? (n + tile - 1) / tile <= kClusterMax
-                                  : (n + tile - 1) / tile <= d->sms * shape_per_sm(*d, k, fill_smem(n, kMaxCoarseCoop));
+    any |= (n + tile - 1) / tile <= d->sms * shape_per_sm(*d, k, fill_smem(n, kMaxCoarseCoop));
   }
   if (!any) {
     set_tuned_shape(dev, n, -2);

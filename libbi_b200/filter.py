@@ -282,16 +282,13 @@ class StepResult:
     resampled: bool
 
 
-# (threads per block, particles per thread[, "cluster"]): the cooperative-
-# grid shapes, then the thread-block-cluster shapes (one cluster of at most
-# 16 CTAs)
-RESAMPLE_SHAPES = ((256, 2), (128, 4), (512, 1), (512, 2), (256, 4), (1024, 1),
-                   (1024, 4, "cluster"), (512, 8, "cluster"), (1024, 8, "cluster"))
+# (threads per block, particles per thread) of the one-launch kernel
+RESAMPLE_SHAPES = ((256, 2), (128, 4), (512, 1), (512, 2), (256, 4), (1024, 1))
 
 
 def shape_name(shape) -> str:
-    """'256x2', or 'cluster1024x4' for a cluster shape."""
-    return ("cluster" if len(shape) > 2 else "") + f"{shape[0]}x{shape[1]}"
+    """'256x2' for (256, 2)."""
+    return f"{shape[0]}x{shape[1]}"
 
 
 def autotune_resampler(n: int, stream=None):
