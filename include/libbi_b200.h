@@ -340,14 +340,18 @@ int bpf_autotune_resampler(int n, void* stream, bpf_tune_result* out);
 int bpf_resampler_set_shape(bpf_resampler* r, int shape);
 
 /* Diagnostic hook, no counterpart in the reference (its resamplers have no
- * device-side waits).  Every grid-wide barrier of the cooperative systematic
- * resampler waits at most `cycles` SM clock cycles on the current device
- * (BPF_WAIT_LIMIT_DEFAULT, about 2 s, unless changed); a block that gives up
- * records BPF_E_TIMEOUT and its kernel returns.  A negative value makes a
- * block that finds a barrier still closed give up at once, so that a test
- * can take the timeout path without a kernel that never arrives.  The next
- * status reset (each stand-alone resampler call, bpf_init, bpf_restore)
- * clears the barrier state the abandoned launch left. */
+ * device-side waits).  Every wait of the cooperative systematic resampler
+ * for the other blocks (a grid-wide barrier, or the poll of the other
+ * blocks' published words) lasts at most `cycles` SM clock cycles on the
+ * current device (BPF_WAIT_LIMIT_DEFAULT, about 2 s, unless changed); a
+ * block that gives up records BPF_E_TIMEOUT and its kernel returns.  A
+ * negative value makes a block give up at the first wait that finds the
+ * others not yet there (a barrier still closed; and every poll, whatever it
+ * finds), so that a test can take the timeout path without a kernel that
+ * never arrives.  The next status reset (each stand-alone resampler call,
+ * bpf_init, bpf_restore) clears the barrier state the abandoned launch left
+ * and moves the resampler's epoch on, so that nothing the abandoned launch
+ * published is taken for a later launch's. */
 #define BPF_WAIT_LIMIT_DEFAULT 4000000000LL
 int bpf_debug_set_wait_limit(long long cycles);
 

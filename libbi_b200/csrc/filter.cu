@@ -291,10 +291,13 @@ __global__ void k_record(const bpf::StepStats* st, double* hist, int k) {
 // the status of a stand-alone call back to BPF_OK, with the grid-barrier
 // counter and generation of the scratch (bar[0], bar[1]): a cooperative
 // launch that timed out can leave the counter above zero
-__global__ void k_set_status_ok(bpf::StepStats* st, unsigned* bar) {
+// the status back to BPF_OK, the grid-barrier word (counters[8..9]) to
+// zero and the resampler's epoch (counters[kEpochWord]) one further
+__global__ void k_set_status_ok(bpf::StepStats* st, unsigned* counters) {
   st->status = BPF_OK;
-  bar[0] = 0u;
-  bar[1] = 0u;
+  counters[8] = 0u;
+  counters[9] = 0u;
+  counters[bpf::kEpochWord] += 1u;
 }
 
 // set_elements(s.logWeights(), s.logLikelihood), Resampler.hpp:177
@@ -611,8 +614,9 @@ int bpf_init(bpf_handle* h) {
   h->step = 0;
   // the last-block tickets and grid-barrier words start from zero (a
   // cooperative resampling that timed out can leave a barrier counter set)
-  BPF_TRY(cudaMemsetAsync(h->rs.counters, 0, 16 * sizeof(unsigned), h->stream));
-  int rc;
+  // and the resampler's epoch moves on
+  int rc = bpf::reset_scratch_words(h->rs, h->stream);
+  if (rc) return rc;
   if (h->custom) {
     bpf_init_args a{};
     a.x = h->x[0];
@@ -888,7 +892,7 @@ int bpf_resampler_destroy(bpf_resampler* r) {
 }
 
 static int reset_status(bpf_resampler* r) {
-  k_set_status_ok<<<1, 1, 0, r->stream>>>(r->rs.stats, r->rs.counters + 8);
+  k_set_status_ok<<<1, 1, 0, r->stream>>>(r->rs.stats, r->rs.counters);
   BPF_TRY(cudaGetLastError());
   return BPF_OK;
 }
@@ -1076,7 +1080,10 @@ int bpf_restore(bpf_handle* h, const void* buf, uint64_t bytes) {
   p += (size_t)h->n * sizeof(double);
   BPF_TRY(cudaMemcpyAsync(h->as, p, (size_t)h->n * sizeof(int), cudaMemcpyHostToDevice, h->stream));
   BPF_TRY(cudaMemcpyAsync(h->rs.stats, &hd.stats, sizeof(hd.stats), cudaMemcpyHostToDevice, h->stream));
-  BPF_TRY(cudaMemsetAsync(h->rs.counters, 0, 16 * sizeof(unsigned), h->stream));
+  {
+    const int rc = bpf::reset_scratch_words(h->rs, h->stream);
+    if (rc) return rc;
+  }
   BPF_TRY(cudaStreamSynchronize(h->stream));
   h->step = hd.step;
   return BPF_OK;

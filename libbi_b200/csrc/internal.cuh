@@ -198,6 +198,9 @@ struct ResampleScratch {
 constexpr int kEpochWord = 10;
 constexpr int kPubWords = 5;
 int scratch_alloc(ResampleScratch& s, int max_n);
+// counters[0 .. kEpochWord) to zero and the epoch advanced (after a timeout,
+// and before a filter starts over)
+int reset_scratch_words(ResampleScratch& s, cudaStream_t st);
 void scratch_free(ResampleScratch& s);
 
 // Reduction of lw[0..n) into s.stats (mx, s1, s2, ess, lW); stats->ll/inc untouched.

@@ -740,6 +740,7 @@ __device__ __forceinline__ bool warp_poll_tagged(const unsigned long long* p, in
                                                  F fn) {
   const int lane = threadIdx.x & 31;
   const long long lim = g_barrier_limit;
+  if (lim < 0) return false;  // the diagnostic limit: every poll gives up
   const long long t0 = clock64();
   for (int base = 0; base < G; base += 128) {
     unsigned long long w[4][W];
@@ -756,7 +757,7 @@ __device__ __forceinline__ bool warp_poll_tagged(const unsigned long long* p, in
 #pragma unroll
         for (int k = 0; k < W; ++k) mine &= (unsigned)(w[u][k] >> 32) == epoch;
       if (__all_sync(0xffffffffu, mine)) break;
-      const int give_up = lane == 0 && (lim < 0 || clock64() - t0 > lim);
+      const int give_up = lane == 0 && clock64() - t0 > lim;
       if (__shfl_sync(0xffffffffu, give_up, 0)) return false;
     }
 #pragma unroll
@@ -1291,6 +1292,22 @@ k_gather(const int* __restrict__ as, const T* __restrict__ X, T* __restrict__ Y,
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
+// the last-block tickets and grid-barrier words back to zero, and the
+// one-launch kernel's epoch one further: the published words of a launch
+// that timed out (or of any earlier launch) then carry an epoch no later
+// launch uses, whatever state that launch left them in
+__global__ void k_reset_scratch_words(unsigned* counters) {
+  const int i = threadIdx.x;
+  if (i < kEpochWord) counters[i] = 0u;
+  if (i == kEpochWord) counters[i] += 1u;
+}
+
+int reset_scratch_words(ResampleScratch& s, cudaStream_t st) {
+  k_reset_scratch_words<<<1, 32, 0, st>>>(s.counters);
+  BPF_TRY(cudaGetLastError());
+  return BPF_OK;
+}
+
 int scratch_alloc(ResampleScratch& s, int max_n) {
   s.max_n = max_n;
   s.max_tiles = ntiles(max_n);

@@ -120,6 +120,33 @@ def test_l96_config_c2_matches_oracle(cuda, oracle):
     pf.close()
 
 
+def test_handle_reused_across_runs_and_restores(cuda, oracle):
+    """One handle, several filter runs on different observations, with a
+    snapshot restored in between: every run equals the oracle's filter.  The
+    one-launch resampler (N = 65536: several blocks handing over through
+    published words) reuses its scratch from run to run; the words of earlier
+    launches must never be taken for the current one's."""
+    from libbi_b200 import ModelL96
+
+    model, n, T, dt = ModelL96(dim=40), 65536, 12, 0.05
+    desc = model.desc()
+    pf = _mk(model, n, "systematic", 1.0, seed=8)
+    snap = None
+    for r, dseed in enumerate((31, 32, 33)):
+        y, _ = oracle.simulate(desc, dseed, T, 0.0, dt)
+        ll, inc, _ = pf.filter(y, 0.0, dt)
+        want = oracle.filter(desc, pf._cfg, y, T, 0.0, dt)
+        assert want["rc"] == 0 and want["resampled"].sum() >= T - 1
+        np.testing.assert_allclose(inc, want["inc"], rtol=1e-10, atol=1e-9)
+        x, _, _ = pf.state()
+        np.testing.assert_array_equal(x.cpu().numpy()[:, :n], want["x"][:, :n])
+        if r == 0:
+            snap = pf.snapshot()
+        elif r == 1:
+            pf.restore(snap)
+    pf.close()
+
+
 def test_step_api_and_snapshot(cuda, oracle):
     from libbi_b200 import ModelL96
 

@@ -7,7 +7,10 @@ timeout path with every block of the kernel running normally: nothing waits
 for a flag that is never set, and the context stays usable.  After the
 default limit is back, the next call on the same scratch (where the
 abandoned launch left a barrier counter above zero) must again return the
-oracle's ancestors bit for bit."""
+oracle's ancestors bit for bit.  The one-tile kernel hands its phases over
+through published words rather than barriers; under a negative limit every
+one of its polls gives up, and the next status reset moves its epoch on.
+"""
 import numpy as np
 import pytest
 
@@ -33,11 +36,14 @@ def test_barrier_timeout_reported_then_next_call_exact(cuda, oracle, n):
     a = rng.random(1)
     lw_d = torch.as_tensor(lw, device="cuda", dtype=torch.float64)
     a_d = torch.as_tensor(a, device="cuda", dtype=torch.float64)
+    # the abandoned launch runs on other log-weights, so that anything it
+    # left behind and a later launch took for its own would show
+    lw_other = torch.as_tensor(rng.standard_normal(n) * 3.0, device="cuda", dtype=torch.float64)
     R = SystematicResampler(max_n=n)
     try:
         _set_limit(-1)
         with pytest.raises(BpfError) as e:
-            R.ancestors(lw_d, a_d, permute=True)
+            R.ancestors(lw_other, a_d, permute=True)
         assert e.value.status == N.BPF_E_TIMEOUT
     finally:
         _set_limit(N.BPF_WAIT_LIMIT_DEFAULT)
