@@ -1072,6 +1072,8 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-guided", action="store_true")
     ap.add_argument("--no-precision", action="store_true")
+    ap.add_argument("--pmmh-iterations", type=int, default=2000,
+                    help="PMMH iterations timed per arm (2000, the workload's; fewer for profiling)")
     ap.add_argument("--guided-seeds", type=int, default=64,
                     help="filter runs per N in the guided/bootstrap comparison (64; fewer for profiling)")
     args = ap.parse_args()
@@ -1254,7 +1256,7 @@ def main():
         line["kernels_large_n"] = large_n_kernels()
     if extras and not args.no_batched:
         line["batched"] = batched_filters()
-        line["pmmh"] = pmmh_chains()
+        line["pmmh"] = pmmh_chains(iterations=max(2, args.pmmh_iterations))
     if extras and not args.no_precision:
         line["precision"] = precision_check(y_host)
         line["precision_batched"] = batched_precision()
