@@ -228,6 +228,19 @@ inline size_t batch_resample_smem(int max_n) {
   return (size_t)max_n * sizeof(int) + (size_t)max_n + (size_t)kBatchThreads * sizeof(double) + 16;
 }
 
+// Batches whose largest filter has at most kBatchOsSmemMax particles keep
+// the cumulative offspring in shared memory too (the SMEM_OS kernels): the
+// CTA's passes over them then cost shared-memory latency instead of L2
+// round trips
+constexpr int kBatchOsSmemMax = 12288;
+inline size_t batch_resample_smem_os(int max_n) { return batch_resample_smem(max_n) + (size_t)max_n * sizeof(int); }
+
+template <bool SMEM_OS>
+__device__ __forceinline__ int ld_os(const int* p) {
+  if constexpr (SMEM_OS) return *p;
+  else return __ldcg(p);
+}
+
 // Permuted ancestors of filter blockIdx.x, the rule of
 // ResamplerHost::cumulativeOffspringToAncestorsPermute
 // (share/src/bi/host/resampler/ResamplerHost.hpp:134-168) in closed form:
@@ -237,7 +250,7 @@ inline size_t batch_resample_smem(int max_n) {
 //   multinomial  MultinomialResamplerHost::ancestors (MultinomialResamplerHost.hpp:29-65)
 //   Metropolis   MetropolisResamplerHost::ancestors (MetropolisResamplerHost.hpp:32-62)
 // computed exactly as the single-filter kernels compute them.
-template <int NT>
+template <int NT, bool SMEM_OS>
 __global__ void __launch_bounds__(NT, 1)
 k_batch_resample(const double* __restrict__ lw, int* __restrict__ as, const BatchFilter* __restrict__ filt,
                  const int* __restrict__ order, StepStats* stats, double* lu_buf, int* os_buf, int step) {
@@ -250,10 +263,12 @@ k_batch_resample(const double* __restrict__ lw, int* __restrict__ as, const Batc
   const int n = fd.n;
   const double* lwf = lw + fd.off;
   int* asf = as + fd.off;
-  int* osf = os_buf + fd.off;
   double* s_coarse = reinterpret_cast<double*>(s_raw);
   int* marks = reinterpret_cast<int*>(s_raw + kBatchThreads * sizeof(double));  // layout for the largest NT
-  unsigned char* flags = reinterpret_cast<unsigned char*>(marks + n);
+  // the cumulative offspring: after the marks in shared memory, or the
+  // filter's columns of the global buffer
+  int* osf = SMEM_OS ? marks + n : os_buf + fd.off;
+  unsigned char* flags = reinterpret_cast<unsigned char*>(SMEM_OS ? osf + n : marks + n);
   const int IT = (n + NT - 1) / NT;
   const int i0 = min(n, threadIdx.x * IT);
   const int i1 = min(n, i0 + IT);
@@ -321,20 +336,20 @@ k_batch_resample(const double* __restrict__ lw, int* __restrict__ as, const Batc
     }
     __syncthreads();
     int loc = 0;
-    for (int i = i0; i < i1; ++i) loc += __ldcg(osf + i);
+    for (int i = i0; i < i1; ++i) loc += ld_os<SMEM_OS>(osf + i);
     int tot;
     int run = block_exclusive_scan_int_nt<NT>(loc, &tot);
-    for (int i = i0; i < i1; ++i) { run += __ldcg(osf + i); osf[i] = run; }
+    for (int i = i0; i < i1; ++i) { run += ld_os<SMEM_OS>(osf + i); osf[i] = run; }
   }
   __syncthreads();
 
   // ---- permutation: childless counts, survivors, extra-copy marks ----
-  const int before0 = i0 == 0 ? 0 : __ldcg(osf + i0 - 1);
+  const int before0 = i0 == 0 ? 0 : ld_os<SMEM_OS>(osf + i0 - 1);
   int zl = 0;
   {
     int prev = before0;
     for (int i = i0; i < i1; ++i) {
-      const int o = __ldcg(osf + i);
+      const int o = ld_os<SMEM_OS>(osf + i);
       zl += (o == prev);
       prev = o;
     }
@@ -346,7 +361,7 @@ k_batch_resample(const double* __restrict__ lw, int* __restrict__ as, const Batc
   {
     int prev = before0, Z = zexcl;
     for (int i = i0; i < i1; ++i) {
-      const int o = __ldcg(osf + i);
+      const int o = ld_os<SMEM_OS>(osf + i);
       const bool zero = o == prev;
       flags[i] = zero;
       if (!zero) {
@@ -444,14 +459,34 @@ int launch_batch_transition(const ModelArgs& m, const void* x_in, void* x_out, i
 int launch_batch_resample(const double* lw, int* as, const BatchFilter* filt, const int* order, int nf,
                           int max_n, StepStats* stats, double* lu_buf, int* os_buf, int step, cudaStream_t st,
                           int threads) {
-  const size_t smem = batch_resample_smem(max_n);
-  switch (threads) {
-    case 256: k_batch_resample<256><<<nf, 256, smem, st>>>(lw, as, filt, order, stats, lu_buf, os_buf, step); break;
-    case 512: k_batch_resample<512><<<nf, 512, smem, st>>>(lw, as, filt, order, stats, lu_buf, os_buf, step); break;
-    case 1024:
-      k_batch_resample<1024><<<nf, 1024, smem, st>>>(lw, as, filt, order, stats, lu_buf, os_buf, step);
-      break;
-    default: return BPF_E_INVALID;
+  if (max_n <= kBatchOsSmemMax) {
+    const size_t smem = batch_resample_smem_os(max_n);
+    switch (threads) {
+      case 256:
+        k_batch_resample<256, true><<<nf, 256, smem, st>>>(lw, as, filt, order, stats, lu_buf, os_buf, step);
+        break;
+      case 512:
+        k_batch_resample<512, true><<<nf, 512, smem, st>>>(lw, as, filt, order, stats, lu_buf, os_buf, step);
+        break;
+      case 1024:
+        k_batch_resample<1024, true><<<nf, 1024, smem, st>>>(lw, as, filt, order, stats, lu_buf, os_buf, step);
+        break;
+      default: return BPF_E_INVALID;
+    }
+  } else {
+    const size_t smem = batch_resample_smem(max_n);
+    switch (threads) {
+      case 256:
+        k_batch_resample<256, false><<<nf, 256, smem, st>>>(lw, as, filt, order, stats, lu_buf, os_buf, step);
+        break;
+      case 512:
+        k_batch_resample<512, false><<<nf, 512, smem, st>>>(lw, as, filt, order, stats, lu_buf, os_buf, step);
+        break;
+      case 1024:
+        k_batch_resample<1024, false><<<nf, 1024, smem, st>>>(lw, as, filt, order, stats, lu_buf, os_buf, step);
+        break;
+      default: return BPF_E_INVALID;
+    }
   }
   BPF_TRY(cudaGetLastError());
   return BPF_OK;
@@ -462,11 +497,15 @@ int launch_batch_resample(const double* lw, int* as, const BatchFilter* filt, co
 // must not lower it under a larger one), once per device.
 int configure_batch_resample(int max_n) {
   if (max_n > BPF_BATCH_MAX_PARTICLES) return BPF_E_INVALID;
-  static unsigned c256 = 0, c512 = 0, c1024 = 0;
+  static unsigned c256 = 0, c512 = 0, c1024 = 0, d256 = 0, d512 = 0, d1024 = 0;
   const int smem = (int)batch_resample_smem(BPF_BATCH_MAX_PARTICLES);
-  BPF_TRY(set_dyn_smem_once(k_batch_resample<256>, smem, c256));
-  BPF_TRY(set_dyn_smem_once(k_batch_resample<512>, smem, c512));
-  BPF_TRY(set_dyn_smem_once(k_batch_resample<1024>, smem, c1024));
+  BPF_TRY(set_dyn_smem_once(k_batch_resample<256, false>, smem, c256));
+  BPF_TRY(set_dyn_smem_once(k_batch_resample<512, false>, smem, c512));
+  BPF_TRY(set_dyn_smem_once(k_batch_resample<1024, false>, smem, c1024));
+  const int smem_os = (int)batch_resample_smem_os(kBatchOsSmemMax);
+  BPF_TRY(set_dyn_smem_once(k_batch_resample<256, true>, smem_os, d256));
+  BPF_TRY(set_dyn_smem_once(k_batch_resample<512, true>, smem_os, d512));
+  BPF_TRY(set_dyn_smem_once(k_batch_resample<1024, true>, smem_os, d1024));
   return BPF_OK;
 }
 
