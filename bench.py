@@ -389,6 +389,79 @@ def batched_filters(runs=5):
     }
 
 
+REF_TIMED_PZ_LIB = os.path.join(ROOT, "oracle", "_ref", "libbiref_time_pz.so")
+
+
+def pz_c1(n=4096, T=100, runs=20):
+    """The plankton configuration (C1): one PZ filter of 4096 FP64 particles,
+    RK4(3) with h0 = 0.1 and tolerances 1e-3, the growth rate's log-normal
+    noise redrawn each day, observations log P + N(0, 0.2^2) daily for
+    T = 100 from one seeded model run (seed 1, P0, Z0 ~ LogN(ln 2, 0.2^2)),
+    systematic resampling at every step (essRel = 1, strict <).  Device time
+    of the filter's kernels per run (the handle's events around each step's
+    kernels) and end to end through bpf_filter (host wall clock: the
+    observations' upload, the initial draw, T steps, the results read
+    back); beside them the reference's own host code on the same workload
+    (ref_pz_filter_timed: its SystematicResampler, StaticSamplerHost,
+    RK43IntegratorHost and SparseStaticLogDensityHost in
+    Filter<BootstrapPF>::filter's loop, real = double, -O3 -funroll-loops,
+    all host threads; draws from pre-generated tables)."""
+    import ctypes
+
+    import numpy as np
+    import torch
+    from libbi_b200 import BootstrapPF, ModelPZ
+
+    model = ModelPZ()
+    truth = BootstrapPF(model, 1, seed=1)
+    ps = np.zeros(T)
+    for k in range(T):
+        truth.step(float(k), float(k + 1), None)
+        x, _, _ = truth.state()
+        ps[k] = float(x[0, 0].item())
+    truth.close()
+    y = (np.log(ps) + model.sigma_y * np.random.default_rng(1).standard_normal(T)).astype(np.float64)
+    pf = BootstrapPF(model, n, resampler="systematic", ess_rel=1.0, seed=1)
+    pf.filter(y, 0.0, 1.0)  # warm-up (graph capture)
+    pf.timing(True)
+    pf.timing_read(reset=True)
+    for _ in range(runs):
+        pf.filter(y, 0.0, 1.0)
+    r_ms, t_ms, steps = pf.timing_read(reset=True)
+    pf.timing(False)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(runs):
+        ll, _, _ = pf.filter(y, 0.0, 1.0)
+    wall = (time.perf_counter() - t0) / runs
+    pf.close()
+    dev_ms = (r_ms + t_ms) / runs
+    out = {"workload": f"pz_n{n}_t{T}_fp64_rk43_systematic_every_step", "nparticles": n, "T": T, "runs": runs,
+           "particle_steps_per_s": n * T / (dev_ms * 1e-3), "ms_per_filter_run": dev_ms,
+           "e2e_particle_steps_per_s": n * T / wall, "e2e_ms_per_filter_run": wall * 1e3,
+           "log_likelihood": ll, "timer": "device: the handle's CUDA events around each step's kernels, summed; "
+                                        "e2e: host wall clock around bpf_filter"}
+    if os.path.exists(REF_TIMED_PZ_LIB):
+        L = ctypes.CDLL(REF_TIMED_PZ_LIB)
+        f = L.ref_pz_filter_timed
+        f.restype = ctypes.c_double
+        f.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_double,
+                      ctypes.c_double, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                      ctypes.POINTER(ctypes.c_double)]
+        rng = np.random.default_rng(1)
+        x0 = np.ascontiguousarray(np.exp(np.log(2.0) + 0.2 * rng.standard_normal((n, 2))))
+        nrm = rng.standard_normal(1 << 20)
+        uni = rng.random(1 << 20)
+        threads = os.cpu_count() or 1
+        rl = ctypes.c_double()
+        p = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+        secs = f(p(x0), n, T, p(y), 1.0, 1.0, threads, p(nrm), p(uni), int(nrm.size), ctypes.byref(rl))
+        out["cpu_reference"] = {"particle_steps_per_s": n * T / secs, "seconds": secs, "cores": threads,
+                                "log_likelihood": rl.value,
+                                "what": "the reference's own host code for this configuration, all T steps"}
+    return out
+
+
 def pmmh_chains(iterations=2000, nchains=128, n_lo=1024, n_hi=8192, T=100, checks=0.01, guided=True):
     """Particle-marginal Metropolis-Hastings on the plankton model: 128
     chains over (c, e, m, q) with priors c, e ~ U(0, 1), m, q ~
@@ -1254,6 +1327,8 @@ def main():
                             "median_us": {shape_name(k): v for k, v in us.items()}}
     if extras and not args.no_large_n:
         line["kernels_large_n"] = large_n_kernels()
+    if extras:
+        line["pz_c1"] = pz_c1()
     if extras and not args.no_batched:
         line["batched"] = batched_filters()
         line["pmmh"] = pmmh_chains(iterations=max(2, args.pmmh_iterations))

@@ -191,6 +191,13 @@ class ModelPZ {
 #include "bi/host/ode/RK43IntegratorHost.hpp"
 #include "bi/host/updater/StaticSamplerHost.hpp"
 #include "bi/host/updater/SparseStaticLogDensityHost.hpp"
+#include "bi/traits/resampler_traits.hpp"
+#include "bi/resampler/Resampler.hpp"
+#include "bi/resampler/SystematicResampler.hpp"
+#include "bi/host/resampler/ResamplerHost.hpp"
+#include "bi/primitive/vector_primitive.hpp"
+
+#include <chrono>
 
 namespace {
 void ensure_init_pz() {
@@ -236,6 +243,64 @@ int ref_pz_transition(double* x, int P, const double* z, double t1, double t2, c
   for (int p = 0; p < P; ++p)
     for (int i = 0; i < 2; ++i) x[(size_t)p * 2 + i] = s.get(bi::D_VAR)(p, i);
   return 0;
+}
+
+/* The reference's filter loop on this model, timed (the CPU baseline of the
+ * plankton configuration): T steps of Filter<BootstrapPF>::filter
+ * (share/src/bi/filter/Filter.hpp:58-70), each BootstrapPF::step
+ * (share/src/bi/filter/BootstrapPF.hpp:158-181) run as Resampler<R>::resample's
+ * test and the reference's SystematicResampler (precompute,
+ * ancestorsPermute, State::gather, set_elements(lws, ll);
+ * share/src/bi/resampler/Resampler.hpp:167-182), the transition block
+ * (StaticSamplerHost for the log-normal growth rate, RK43IntegratorHost for
+ * the ode) and the observation block through SparseStaticLogDensityHost,
+ * then ess_reduce; on `threads` OpenMP threads.  Draws come from the tape
+ * shim's cycling tables (a load each: the generator's cost is not counted).
+ *   x0  P x 2 initial states (P, Z), particle-major;  y  T observations
+ * Returns the wall-clock seconds of the T steps; *ll the log-likelihood. */
+double ref_pz_filter_timed(const double* x0, int P, int T, const double* y, double dt, double ess_rel, int threads,
+                           const double* nrm, const double* uni, int n, double* ll) {
+  using namespace pz;
+  ensure_init_pz();
+  bi_omp_init(threads);
+  boost::random_tape::set(nullptr, 0);  // this thread draws from the tables too
+  boost::random_tape::cycle().nrm = nrm;
+  boost::random_tape::cycle().uni = uni;
+  boost::random_tape::cycle().n = (std::size_t)n;
+  bi::State<ModelPZ, bi::ON_HOST> s(P);
+  for (int p = 0; p < P; ++p)
+    for (int i = 0; i < 2; ++i) s.get(bi::D_VAR)(p, i) = x0[(size_t)p * 2 + i];
+  bi::host_vector<real> lws(P);
+  bi::set_elements(lws, real(0));
+  bi::Mask<bi::ON_HOST> mask(4);
+  mask.addDenseMask(Var3::ID, 1);
+  static bi::Random rng(0);
+  bi::SystematicResampler R;
+  bi_ode_set(BI_REAL(0.1), BI_REAL(1.0e-3), BI_REAL(1.0e-3));
+  double ess = P, logLik = 0.0;
+  const auto t0 = std::chrono::steady_clock::now();
+  for (int k = 0; k < T; ++k) {
+    if (ess < ess_rel * P) {
+      bi::ScanResamplerPrecompute<bi::ON_HOST> pre;
+      bi::host_vector<int> as(P);
+      R.precompute(lws, pre);
+      R.ancestorsPermute(rng, lws, as, pre);
+      s.gather(as);
+      bi::set_elements(lws, real(logLik));
+    }
+    bi::StaticSamplerHost<ModelPZ, noise_typelist>::samples(rng, s);
+    bi::RK43IntegratorHost<ModelPZ, ode_typelist, real>::update(k * dt, (k + 1) * dt, s);
+    s.get(bi::OY_VAR)(0, 0) = y[k];
+    bi::SparseStaticLogDensityHost<ModelPZ, obs_typelist>::logDensities(s, mask, lws);
+    double lW;
+    ess = bi::ess_reduce(lws, &lW);
+    logLik = lW;
+  }
+  const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  boost::random_tape::cycle() = boost::random_tape::Cycle();
+  bi_omp_init(1);  // the parity entry points run on one thread
+  if (ll) *ll = logLik;
+  return secs;
 }
 
 }  // extern "C"
