@@ -38,10 +38,11 @@ ESS_REL = 0.5
 SEED = 2
 DATA_SEED = 102
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
-# our kernels per step with the systematic resampler: the cooperative
-# resample kernel (launched every step, gated on the device) + the fused
-# transition
-LAUNCHES_PER_STEP = 2
+# our kernels per step with the systematic resampler: one (the step kernel,
+# resampling as its prologue when due) in the one-launch form; two (the
+# cooperative resample kernel, launched every step and gated on the device,
+# then the fused transition) in the two-launch form
+LAUNCHES_PER_STEP = {True: 1, False: 2}
 # algorithmic bytes of the fused transition per particle: state read + write
 # (2 * d * 4 B) and FP64 log-weight read + write (16 B); the ancestor index
 # (4 B) is read only on resample steps
@@ -459,6 +460,48 @@ def pz_c1(n=4096, T=100, runs=20):
         out["cpu_reference"] = {"particle_steps_per_s": n * T / secs, "seconds": secs, "cores": threads,
                                 "log_likelihood": rl.value,
                                 "what": "the reference's own host code for this configuration, all T steps"}
+    return out
+
+
+def step_forms(y_dev, steps=300, warmup=5):
+    """The headline workload in both step forms, one after the other on the
+    same observations and seed: one launch per step (the systematic
+    resampling as the step kernel's prologue) and two (the one-launch
+    resampler, then the transition).  CUDA events around each step, L2
+    flushed before each; the filters' numbers are the same bit for bit."""
+    import torch
+    from libbi_b200 import BootstrapPF, configs
+
+    model = configs.L96_D40_N65536["model"]
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    out = {}
+    lls = {}
+    for name, fused in (("one_launch", True), ("two_launch", False)):
+        pf = BootstrapPF(model, N_PARTICLES, resampler="systematic", ess_rel=ESS_REL, seed=SEED)
+        pf.set_step_form(fused)
+        k = 0
+        ms = []
+        for i in range(warmup + steps):
+            if k >= T_OBS:
+                pf.init()
+                k = 0
+            k += 1
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            pf.step_device((k - 1) * DT, k * DT, y_dev[k - 1], sync=False)
+            b.record()
+            if i >= warmup:
+                ms.append((a, b))
+        torch.cuda.synchronize()
+        t = sum(a.elapsed_time(b) for a, b in ms) / steps
+        _, lw, _ = pf.state()
+        lls[name] = lw.cpu().numpy().tobytes()
+        pf.close()
+        out[name] = {"ms_per_step": t, "particle_steps_per_s": N_PARTICLES / (t * 1e-3),
+                     "launches_per_step": LAUNCHES_PER_STEP[fused]}
+    out["same_log_weights"] = lls["one_launch"] == lls["two_launch"]
+    out["timer"] = f"CUDA events around each of {steps} steps after {warmup} warm-up, L2 flushed before each"
     return out
 
 
@@ -1179,6 +1222,7 @@ def main():
     from libbi_b200.replicas import max_over_ranks, replica_seed, whole_job_rate
 
     pf = BootstrapPF(model, N_PARTICLES, resampler="systematic", ess_rel=ESS_REL, seed=replica_seed(SEED, rank))
+    fused = pf.step_form_fused
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
     k = 0
 
@@ -1297,8 +1341,11 @@ def main():
                          "d2h_bytes_per_step": 80,
                          "timer": "host wall clock around bpf_step (BootstrapPF::step), one synchronising call "
                                   "per step"},
-        "gpu_launches": LAUNCHES_PER_STEP * args.steps,
-        "roofline": {"kernel": "k_l96_transition<float,40>", "bound": "hbm", "achieved": achieved,
+        "gpu_launches": LAUNCHES_PER_STEP[fused] * args.steps,
+        "step_form": "one launch per step (resampling as the step kernel's prologue)" if fused else
+                     "two launches per step (resampler, then transition)",
+        "roofline": {"kernel": "k_l96_step<float,40>" if fused else "k_l96_transition<float,40>",
+                     "bound": "hbm", "achieved": achieved,
                      "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "peak_source": how,
                      "traffic": TRANSITION_DRAM_BYTES_PER_LAUNCH,
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch",
@@ -1308,7 +1355,9 @@ def main():
                               "frac": fp32_ach / fp32_peak,
                               "peak_source": "148 SM x 128 FP32 lanes x 2 x sampled SM clock"}},
         "kernel_ms_per_step": {"resample": res_ms / max(nst, 1), "transition": tr_ms / max(nst, 1),
-                               "timer": "a second pass of K steps with events between the kernels"},
+                               "timer": "a second pass of K steps with events between the kernels" +
+                                        ("; in the one-launch form 'transition' is the whole step kernel, "
+                                         "resampling prologue included" if fused else "")},
         "wall_s": wall,
         "clocks": clocks,
     }
@@ -1328,6 +1377,7 @@ def main():
     if extras and not args.no_large_n:
         line["kernels_large_n"] = large_n_kernels()
     if extras:
+        line["step_forms"] = step_forms(y_dev)
         line["pz_c1"] = pz_c1()
     if extras and not args.no_batched:
         line["batched"] = batched_filters()

@@ -52,7 +52,7 @@ EXPORTS = (
     "bpf_proposal_loss_grad", "bpf_proposal_params", "bpf_proposal_set_params", "bpf_set_proposal",
     "bpf_batch_set_proposal",
     "bpf_path_cache", "bpf_sample_path", "bpf_step_sparse", "bpf_smc2_run", "bpf_debug_set_wait_limit", "bpf_create_model", "bpf_path_cache_nodes", "bpf_proposal_set_states",
-    "bpf_pmmh_set_proposal",
+    "bpf_pmmh_set_proposal", "bpf_set_step_form", "bpf_step_form",
 )
 
 
@@ -184,6 +184,8 @@ def _declare(L):
         "bpf_proposal_set_data": (c_int, [H, c_void_p, c_void_p, c_void_p, c_int]),
         "bpf_proposal_set_states": (c_int, [H, c_void_p, c_int]),
         "bpf_pmmh_set_proposal": (c_int, [H, H]),
+        "bpf_set_step_form": (c_int, [H, c_int]),
+        "bpf_step_form": (c_int, [H, POINTER(c_int)]),
         "bpf_proposal_train": (c_int, [H, c_int, c_int, c_double, c_void_p]),
         "bpf_proposal_loss_grad": (c_int, [H, c_void_p, c_void_p, c_int, POINTER(c_double), c_void_p]),
         "bpf_proposal_params": (c_int, [H, c_void_p, c_void_p, c_void_p, POINTER(c_int)]),

@@ -65,6 +65,10 @@ struct bpf_handle {
   int pc_cap = 0;   // steps that may be recorded
   int pc_len = 0;   // generations recorded
   bool pc_full = false;
+  // the Lorenz-96 step in one launch (resampling as its prologue), selected
+  // by bpf_set_step_form: built-in L96 with the systematic resampler, every
+  // block of the step resident at once
+  bool fused = false;
 };
 
 struct bpf_resampler {
@@ -195,6 +199,49 @@ int enqueue_step(bpf_handle* h, double t1, double t2, const void* y_dev, uint64_
     int rc = timing_event(h, 0);
     if (rc) return rc;
   }
+  const bool guided = h->prop && y_dev && (mask | ~((h->dim >= 64 ? 0ull : (1ull << h->dim)) - 1ull)) == ~0ull;
+  if (h->fused && !guided) {
+    // the whole step in one launch: the resampling (when due) as the
+    // transition kernel's prologue
+    if (y_host && y_dev)
+      BPF_TRY(cudaMemcpyAsync(const_cast<void*>(y_dev), y_host, y_bytes, cudaMemcpyHostToDevice, h->stream));
+    if (h->timing) {
+      int rc = timing_event(h, 1);
+      if (rc) return rc;
+    }
+    bpf::FusedStepArgs fa;
+    fa.t.x_in = h->x[h->cur];
+    fa.t.x_out = h->x[h->cur ^ 1];
+    fa.t.ld = h->ld;
+    fa.t.n = h->n;
+    fa.t.as = h->as;
+    fa.t.lw = h->lw;
+    fa.t.y = y_dev;
+    fa.t.t1 = t1;
+    fa.t.t2 = t2;
+    fa.t.seed = h->cfg.seed;
+    fa.t.step = k;
+    fa.t.stats = h->rs.stats;
+    fa.t.partials = h->rs.partials;
+    fa.t.max_partials = h->rs.max_partials;
+    fa.t.counter = h->rs.counters + 4;
+    fa.t.obs_mask = mask;
+    fa.E = h->rs.E;
+    fa.ecoarse = h->rs.etile;
+    fa.pub = h->rs.pub;
+    fa.max_pub = h->rs.pub_entries;
+    fa.epoch_word = h->rs.counters + bpf::kEpochWord;
+    int rc = bpf::launch_fused_step(h->model, fa, h->stream);
+    if (rc) return rc;
+    if (h->timing) {
+      rc = timing_event(h, 2);
+      if (rc) return rc;
+      h->ev_steps += 1;
+    }
+    h->cur ^= 1;
+    h->step = k;
+    return path_record(h, true);
+  }
   const int* gate = &h->rs.stats->resample;
   bpf::ResampleArgs ra;
   ra.kind = h->cfg.resampler;
@@ -219,7 +266,7 @@ int enqueue_step(bpf_handle* h, double t1, double t2, const void* y_dev, uint64_
     rc = timing_event(h, 1);
     if (rc) return rc;
   }
-  if (h->prop && y_dev && (mask | ~((h->dim >= 64 ? 0ull : (1ull << h->dim)) - 1ull)) == ~0ull) {
+  if (guided) {
     // guided step (every component observed): the learned proposal instead
     // of the transition
     const double dt = bpf::proposal_dt(h->prop);
@@ -288,11 +335,10 @@ __global__ void k_record(const bpf::StepStats* st, double* hist, int k) {
   hist[3 * k + 2] = (double)st->resampled;
 }
 
-// the status of a stand-alone call back to BPF_OK, with the grid-barrier
-// counter and generation of the scratch (bar[0], bar[1]): a cooperative
-// launch that timed out can leave the counter above zero
 // the status back to BPF_OK, the grid-barrier word (counters[8..9]) to
-// zero and the resampler's epoch (counters[kEpochWord]) one further
+// zero and the resampler's epoch (counters[kEpochWord]) one further: a
+// cooperative launch that timed out can leave the barrier word part-counted
+// and tagged words of the abandoned epoch behind
 __global__ void k_set_status_ok(bpf::StepStats* st, unsigned* counters) {
   st->status = BPF_OK;
   counters[8] = 0u;
@@ -438,6 +484,24 @@ int bpf_create(const bpf_model_desc* model, const bpf_config* config, bpf_handle
   h->model.rtoler = model->rtoler;
   for (int i = 0; i < BPF_MAX_THETA; ++i) h->model.theta[i] = model->theta[i];
   return create_common(h, config, model->dim, model->precision, out);
+}
+
+int bpf_set_step_form(bpf_handle* h, int fused) {
+  if (!h) return BPF_E_INVALID;
+  if (!fused) {
+    h->fused = false;
+    return BPF_OK;
+  }
+  if (h->custom || h->cfg.resampler != BPF_RESAMPLER_SYSTEMATIC || !bpf::fused_step_available(h->model, h->n))
+    return BPF_E_INVALID;
+  h->fused = true;
+  return BPF_OK;
+}
+
+int bpf_step_form(bpf_handle* h, int* fused) {
+  if (!h || !fused) return BPF_E_INVALID;
+  *fused = h->fused ? 1 : 0;
+  return BPF_OK;
 }
 
 int bpf_create_model(const bpf_model_ops* ops, const double* params, const bpf_config* config, bpf_handle** out) {

@@ -184,9 +184,11 @@ struct ResampleScratch {
   double* Ws = nullptr;         // FP64 cumulative weights (multinomial search)
   double* lu = nullptr;         // log sorted uniforms (multinomial)
   unsigned* counters = nullptr; // last-block tickets; word kEpochWord: the one-launch kernel's epoch
-  // block results the one-launch systematic kernel publishes (tagged words,
-  // kPubWords per tile; every tag 0xFFFFFFFF when allocated)
+  // block results the one-launch systematic kernel and the fused step
+  // publish (tagged words, kPubWords per block, pub_entries blocks at most;
+  // every tag 0xFFFFFFFF when allocated)
   unsigned long long* pub = nullptr;
+  int pub_entries = 0;
   StepStats* stats = nullptr;   // reduction results
   LwPartial* partials = nullptr;
   int max_partials = 0;
@@ -197,6 +199,8 @@ struct ResampleScratch {
 // childless count, one for "phase 3 written"
 constexpr int kEpochWord = 10;
 constexpr int kPubWords = 5;
+// blocks that may publish for n particles: tiles of at least 128 particles
+inline int pub_entries_for(int n) { return n / 128 + 2; }
 int scratch_alloc(ResampleScratch& s, int max_n);
 // counters[0 .. kEpochWord) to zero and the epoch advanced (after a timeout,
 // and before a filter starts over)
@@ -261,6 +265,8 @@ void ancestry_free(AncestryPool& a);
 // limit of the grid-barrier waits of the cooperative resamplers on the
 // current device, in SM clock cycles (negative: give up at once)
 int set_barrier_limit(long long cycles);
+// the current device's wait limit (what set_barrier_limit last set there)
+long long barrier_limit();
 
 int launch_gather(const int* as, const void* X, void* Y, int n, int d, int ld, int esz,
                   const int* gate, cudaStream_t st);
@@ -304,6 +310,20 @@ struct TransitionArgs {
   uint64_t obs_mask = ~0ull;  // bit i: component i observed (when y is given)
 };
 int launch_transition(const ModelArgs& m, const TransitionArgs& a, cudaStream_t st);
+// The Lorenz-96 step in one cooperative launch with the permuted systematic
+// resampling as its prologue (step_fused.cu); BPF_E_INVALID when the model
+// is not the built-in Lorenz-96 or the blocks cannot all be resident
+struct FusedStepArgs {
+  TransitionArgs t;
+  int* E;                    // n: extra-copy counts (scratch)
+  int* ecoarse;              // n/16 + 1: every 16th of them (scratch)
+  unsigned long long* pub;   // kPubWords per block (scratch)
+  int max_pub;               // blocks the published words have room for
+  unsigned* epoch_word;      // the scratch's epoch
+};
+int launch_fused_step(const ModelArgs& m, const FusedStepArgs& a, cudaStream_t st);
+// 1 when the fused step can run n particles of model m on the current device
+int fused_step_available(const ModelArgs& m, int n);
 // the step statistics of a freshly initialised filter
 int launch_stats_init(StepStats* stats, int n, double ess_rel, cudaStream_t st);
 int launch_init(const ModelArgs& m, void* x, int ld, int n, double* lw, uint64_t seed,

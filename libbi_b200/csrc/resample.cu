@@ -30,6 +30,7 @@
 #include <mutex>
 #include <vector>
 #include "resample_common.cuh"
+#include "handover.cuh"
 #include "reduce.cuh"
 #include "../../include/bpf_math.h"
 
@@ -694,87 +695,6 @@ k_systematic_coop(const double* __restrict__ lw, int n, StepStats* st, const dou
 // of the phase, which carries the data it waits for.  NT threads of IT
 // particles each: the tile shapes in kCoopShapes, all computing the same
 // integers (the shape is chosen by the autotuner below).
-// ---------------------------------------------------------------------------
-// Block results published as tagged words.  A word holds the launch's epoch
-// in its high half and 32 bits of payload in its low half, written by one
-// store, so a reader that finds the epoch has the payload with it.  The
-// readers of one transition poll all G blocks' words at once (every load of
-// a round in flight together) until each carries the epoch: no atomics, no
-// barrier, and the data arrives with the wait.  The epoch is a scratch word
-// every block reads at its start; block 0 advances it once it has seen every
-// block's first publication (so every block has read it), and the next
-// launch on the scratch publishes under the next value.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ unsigned long long tagged(unsigned epoch, unsigned payload) {
-  return ((unsigned long long)epoch << 32) | payload;
-}
-
-__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
-  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-
-__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
-  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
-
-__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
-  unsigned long long v;
-  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-  return v;
-}
-
-__device__ __forceinline__ unsigned ld_relaxed_u32(const unsigned* p) {
-  unsigned v;
-  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-
-// Warp 0 polls words p[i * stride + k] (i < G, k < W) until every one
-// carries the epoch, W words of each of up to 128 entries in flight per
-// round; fn(i, words) then consumes entry i's payloads.  Bounded by the
-// barrier limit: returns false (warp-uniform) when it gave up.  Ends with an
-// acquire fence, so that what the publishers released before their words is
-// visible to this warp afterwards.
-template <int W, class F>
-__device__ __forceinline__ bool warp_poll_tagged(const unsigned long long* p, int stride, int G, unsigned epoch,
-                                                 F fn) {
-  const int lane = threadIdx.x & 31;
-  const long long lim = g_barrier_limit;
-  if (lim < 0) return false;  // the diagnostic limit: every poll gives up
-  const long long t0 = clock64();
-  for (int base = 0; base < G; base += 128) {
-    unsigned long long w[4][W];
-    while (true) {
-      bool mine = true;
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int i = base + 32 * u + lane;
-#pragma unroll
-        for (int k = 0; k < W; ++k) w[u][k] = i < G ? ld_relaxed_u64(p + (size_t)i * stride + k) : tagged(epoch, 0u);
-      }
-#pragma unroll
-      for (int u = 0; u < 4; ++u)
-#pragma unroll
-        for (int k = 0; k < W; ++k) mine &= (unsigned)(w[u][k] >> 32) == epoch;
-      if (__all_sync(0xffffffffu, mine)) break;
-      const int give_up = lane == 0 && clock64() - t0 > lim;
-      if (__shfl_sync(0xffffffffu, give_up, 0)) return false;
-    }
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int i = base + 32 * u + lane;
-      if (i < G) {
-        unsigned pl[W];
-#pragma unroll
-        for (int k = 0; k < W; ++k) pl[k] = (unsigned)w[u][k];
-        fn(i, pl);
-      }
-    }
-  }
-  __threadfence();
-  return true;
-}
-
 // IT log-weights of one thread (16-byte loads when IT is even and aligned)
 template <int IT>
 __device__ __forceinline__ void load_items(const double* __restrict__ lw, int i0, int n, double (&v)[IT]) {
@@ -850,7 +770,7 @@ k_systematic_coop1(const double* __restrict__ lw, int n, StepStats* st, const do
   // cumulative offspring (registers)
   if (threadIdx.x < 32) {
     u128 lo = u128_zero(), tot = u128_zero();
-    const bool ok = warp_poll_tagged<3>(pub, pub_stride, G, epoch, [&](int i, const unsigned* pl) {
+    const bool ok = warp_poll_tagged<3>(pub, pub_stride, G, epoch, g_barrier_limit, [&](int i, const unsigned* pl) {
       u128 v;
       v.lo = (unsigned long long)pl[0] | ((unsigned long long)pl[1] << 32);
       v.hi = pl[2];
@@ -920,7 +840,7 @@ k_systematic_coop1(const double* __restrict__ lw, int n, StepStats* st, const do
   // phase 3: ranks of childless slots, E, survivors in place
   if (threadIdx.x < 32) {
     int lo = 0, tot = 0;
-    const bool ok = warp_poll_tagged<1>(pub + 3, pub_stride, G, epoch, [&](int i, const unsigned* pl) {
+    const bool ok = warp_poll_tagged<1>(pub + 3, pub_stride, G, epoch, g_barrier_limit, [&](int i, const unsigned* pl) {
       tot += (int)pl[0];
       if (i < b) lo += (int)pl[0];
     });
@@ -963,7 +883,7 @@ k_systematic_coop1(const double* __restrict__ lw, int n, StepStats* st, const do
   __syncthreads();
   if (threadIdx.x == 0) st_release_u64(pub + (size_t)b * pub_stride + 4, tagged(epoch, 1u));
   if (threadIdx.x < 32) {
-    const bool ok = warp_poll_tagged<1>(pub + 4, pub_stride, G, epoch, [](int, const unsigned*) {});
+    const bool ok = warp_poll_tagged<1>(pub + 4, pub_stride, G, epoch, g_barrier_limit, [](int, const unsigned*) {});
     if (threadIdx.x == 0) {
       s_ok = ok;
       if (!ok) st->status = BPF_E_TIMEOUT;
@@ -1335,11 +1255,12 @@ int scratch_alloc(ResampleScratch& s, int max_n) {
   ALLOC(s.counters, 16 * sizeof(unsigned));
   ALLOC(s.stats, sizeof(StepStats));
   ALLOC(s.partials, (size_t)s.max_partials * sizeof(LwPartial));
-  ALLOC(s.pub, T1 * kPubWords * sizeof(unsigned long long));
+  s.pub_entries = pub_entries_for(max_n);
+  ALLOC(s.pub, (size_t)s.pub_entries * kPubWords * sizeof(unsigned long long));
 #undef ALLOC
   if (cudaMemset(s.counters, 0, 16 * sizeof(unsigned)) != cudaSuccess) { scratch_free(s); return BPF_E_CUDA; }
   // tags no epoch carries (the epoch starts at zero)
-  if (cudaMemset(s.pub, 0xFF, T1 * kPubWords * sizeof(unsigned long long)) != cudaSuccess) {
+  if (cudaMemset(s.pub, 0xFF, (size_t)s.pub_entries * kPubWords * sizeof(unsigned long long)) != cudaSuccess) {
     scratch_free(s);
     return BPF_E_CUDA;
   }
@@ -1578,7 +1499,7 @@ static int launch_coop1_shape(int k, const ResampleArgs& a, ResampleScratch& s, 
   const int* gate = a.gate;
   int nn = n;
   int* Oo = Os_out;
-  if (!pub || G > s.max_tiles) return BPF_E_INVALID;
+  if (!pub || G > s.pub_entries) return BPF_E_INVALID;
   void* args[] = {(void*)&lw, (void*)&nn, (void*)&stats, (void*)&a_in, (void*)&seed, (void*)&step, (void*)&Oo,
                   (void*)&as, (void*)&E, (void*)&ec, (void*)&sh, (void*)&slot, (void*)&pub, (void*)&pstride,
                   (void*)&ew, (void*)&gate};
@@ -1755,9 +1676,30 @@ int autotune_systematic(int n, cudaStream_t st, int* best, double* us) {
   return rc ? rc : (*best >= 0 ? BPF_OK : BPF_E_INVALID);
 }
 
+// host copy of each device's limit, for kernels that take it as an argument
+static long long g_host_limit[64];
+static bool g_host_limit_init = false;
+static std::mutex g_limit_mu;
+
 int set_barrier_limit(long long cycles) {
+  int dev = 0;
+  BPF_TRY(cudaGetDevice(&dev));
   BPF_TRY(cudaMemcpyToSymbol(g_barrier_limit, &cycles, sizeof(cycles)));
+  barrier_limit();  // initialises the table
+  std::lock_guard<std::mutex> lk(g_limit_mu);
+  if (dev >= 0 && dev < 64) g_host_limit[dev] = cycles;
   return BPF_OK;
+}
+
+long long barrier_limit() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;
+  std::lock_guard<std::mutex> lk(g_limit_mu);
+  if (!g_host_limit_init) {
+    for (long long& v : g_host_limit) v = kBarrierTimeoutCycles;
+    g_host_limit_init = true;
+  }
+  return dev >= 0 && dev < 64 ? g_host_limit[dev] : kBarrierTimeoutCycles;
 }
 
 int autotuned_shape(int n) {

@@ -40,7 +40,8 @@ constexpr size_t kOffCounters = kOffEtile + align256((kStaticMaxN / 16 + 2) * si
 constexpr size_t kOffStats = kOffCounters + align256(16 * sizeof(unsigned));
 constexpr size_t kOffPartials = kOffStats + align256(sizeof(StepStats));
 constexpr size_t kOffPub = kOffPartials + align256(kStaticPartials * sizeof(LwPartial));
-constexpr size_t kPubBytes = (size_t)(kStaticTiles + 1) * kPubWords * sizeof(unsigned long long);
+constexpr int kStaticPubEntries = kStaticMaxN / 128 + 2;
+constexpr size_t kPubBytes = (size_t)kStaticPubEntries * kPubWords * sizeof(unsigned long long);
 constexpr size_t kScratchBytes = kOffPub + align256(kPubBytes);
 
 // the scratch itself: zero at module load, about 1 MiB per device
@@ -93,6 +94,7 @@ extern "C" int bpf_systematic_ancestors_static(const double* lw, int n, const do
   s.partials = reinterpret_cast<LwPartial*>(base + kOffPartials);
   s.max_partials = kStaticPartials;
   s.pub = reinterpret_cast<unsigned long long*>(base + kOffPub);
+  s.pub_entries = kStaticPubEntries;
   // the array keeps the previous call's contents: clear the last-block
   // counters (the one-launch kernel's epoch among them) and the statistics
   // (status = BPF_OK) before this call's kernels, and give the published

@@ -421,6 +421,18 @@ class BootstrapPF:
         N.check(N.lib().bpf_set_proposal(self._h, None if proposal is None else proposal.handle), "bpf_set_proposal")
         self._proposal = proposal
 
+    def set_step_form(self, fused: bool):
+        """One launch per step with the resampling as the transition's
+        prologue (fused), or the resampler and the transition as two
+        launches (the default); both give the same numbers bit for bit."""
+        N.check(N.lib().bpf_set_step_form(self._h, int(bool(fused))), "bpf_set_step_form")
+
+    @property
+    def step_form_fused(self) -> bool:
+        v = ctypes.c_int()
+        N.check(N.lib().bpf_step_form(self._h, ctypes.byref(v)), "bpf_step_form")
+        return bool(v.value)
+
     def reduce(self):
         lW, ess = ctypes.c_double(), ctypes.c_double()
         N.check(N.lib().bpf_reduce(self._h, ctypes.byref(lW), ctypes.byref(ess)), "bpf_reduce")

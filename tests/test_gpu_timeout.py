@@ -55,11 +55,14 @@ def test_barrier_timeout_reported_then_next_call_exact(cuda, oracle, n):
     R.close()
 
 
-def test_filter_step_timeout_is_sticky_until_init(cuda, oracle):
+@pytest.mark.parametrize("one_launch", [True, False])
+def test_filter_step_timeout_is_sticky_until_init(cuda, oracle, one_launch):
     """A filter whose resampling gave up reports BPF_E_TIMEOUT on that step
     and every later one (the status is sticky, so no later launch starts on
     the abandoned barrier state); bpf_init clears it, and the next whole
-    filter equals the oracle's."""
+    filter equals the oracle's.  one_launch: the resampling is the step
+    kernel's prologue (its polls give up); otherwise the one-launch
+    resampler's."""
     from libbi_b200 import BootstrapPF, BpfError, ModelL96
     from libbi_b200 import _native as N
 
@@ -68,6 +71,7 @@ def test_filter_step_timeout_is_sticky_until_init(cuda, oracle):
     n, T, dt = 65536, 6, 0.05
     y, _ = oracle.simulate(desc, 31, T, 0.0, dt)
     pf = BootstrapPF(model, n, resampler="systematic", ess_rel=1.0, seed=12)
+    pf.set_step_form(one_launch)
     pf.step(0.0, dt, y[0])  # observed: the next step resamples (essRel = 1)
     try:
         _set_limit(-1)
