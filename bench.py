@@ -464,19 +464,20 @@ def pz_c1(n=4096, T=100, runs=20):
 
 
 def step_forms(y_dev, steps=300, warmup=5):
-    """The headline workload in both step forms, one after the other on the
-    same observations and seed: one launch per step (the systematic
-    resampling as the step kernel's prologue) and two (the one-launch
-    resampler, then the transition).  CUDA events around each step, L2
-    flushed before each; the filters' numbers are the same bit for bit."""
+    """The headline workload in both forms of the step, one after the other
+    on the same observations and seed: two launches per step (the one-launch
+    resampler, then the transition as its programmatic dependent; the
+    default) and one (the systematic resampling as the prologue of the step
+    kernel).  CUDA events around each step, L2 flushed before each; the two
+    forms compute the same log-weights bit for bit."""
     import torch
     from libbi_b200 import BootstrapPF, configs
 
     model = configs.L96_D40_N65536["model"]
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
     out = {}
-    lls = {}
-    for name, fused in (("one_launch", True), ("two_launch", False)):
+    lws = {}
+    for name, fused in (("two_launch", False), ("one_launch", True)):
         pf = BootstrapPF(model, N_PARTICLES, resampler="systematic", ess_rel=ESS_REL, seed=SEED)
         pf.set_step_form(fused)
         k = 0
@@ -496,11 +497,11 @@ def step_forms(y_dev, steps=300, warmup=5):
         torch.cuda.synchronize()
         t = sum(a.elapsed_time(b) for a, b in ms) / steps
         _, lw, _ = pf.state()
-        lls[name] = lw.cpu().numpy().tobytes()
+        lws[name] = lw.cpu().numpy().tobytes()
         pf.close()
         out[name] = {"ms_per_step": t, "particle_steps_per_s": N_PARTICLES / (t * 1e-3),
                      "launches_per_step": LAUNCHES_PER_STEP[fused]}
-    out["same_log_weights"] = lls["one_launch"] == lls["two_launch"]
+    out["same_log_weights_bitwise"] = lws["one_launch"] == lws["two_launch"]
     out["timer"] = f"CUDA events around each of {steps} steps after {warmup} warm-up, L2 flushed before each"
     return out
 
@@ -1192,6 +1193,8 @@ def main():
                     help="PMMH iterations timed per arm (2000, the workload's; fewer for profiling)")
     ap.add_argument("--guided-seeds", type=int, default=64,
                     help="filter runs per N in the guided/bootstrap comparison (64; fewer for profiling)")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="the headline line alone, none of the single-GPU sections after it (for profiling)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -1364,7 +1367,7 @@ def main():
     # the sections below are single-GPU measurements: under torchrun (N > 1)
     # the line carries the replicas' headline only, so that no rank waits
     # at the final barrier while rank 0 runs them
-    extras = rank == 0 and world == 1
+    extras = rank == 0 and world == 1 and not args.headline_only
     if extras:
         # the resampler's tile shape for this N (bpf_create tuned it; timed
         # again here so the line shows each shape's median)
