@@ -1085,8 +1085,6 @@ int bpf_resampler_ancestors(bpf_resampler* r, const double* lw, int n, const dou
 
 int bpf_debug_set_wait_limit(long long cycles) { return bpf::set_barrier_limit(cycles); }
 
-int bpf_debug_set_l96_lanes(int lanes) { return bpf::set_l96_lanes(lanes); }
-
 int bpf_gather_rows(const int* as, const void* X, void* Y, int n, int d, int ld, int elem_size, void* stream) {
   if (!as || !X || !Y || X == Y) return BPF_E_INVALID;
   return bpf::launch_gather(as, X, Y, n, d, ld, elem_size, nullptr, (cudaStream_t)stream);
