@@ -69,6 +69,26 @@ struct bpf_handle {
   // by bpf_set_step_form: built-in L96 with the systematic resampler, every
   // block of the step resident at once
   bool fused = false;
+  // bpf_filter's T steps as one CUDA graph: captured when a call repeats the
+  // schedule of the call before it, replayed while the schedule stays
+  struct FilterKey {
+    int T = 0;
+    double t0 = 0.0, dt = 0.0;
+    const void* y = nullptr;
+    const double* hist = nullptr;
+    bool fused = false;
+    bool operator==(const FilterKey& o) const {
+      return T == o.T && t0 == o.t0 && dt == o.dt && y == o.y && hist == o.hist && fused == o.fused;
+    }
+  };
+  cudaGraphExec_t fgraph = nullptr;
+  cudaStream_t capture_stream = nullptr;  // the graph is captured here (the
+                                          // legacy default stream cannot
+                                          // capture), launched on `stream`
+  FilterKey fgraph_key;
+  int fgraph_cur = 0;  // the state buffer the replayed steps end in
+  FilterKey last_filter;
+  bool last_filter_set = false;
 };
 
 struct bpf_resampler {
@@ -329,7 +349,10 @@ int enqueue_step(bpf_handle* h, double t1, double t2, const void* y_dev, uint64_
   return path_record(h, true);
 }
 
+// a programmatic dependent of the step's transition; the next step's
+// resampler waits for it
 __global__ void k_record(const bpf::StepStats* st, double* hist, int k) {
+  bpf::pdl_wait();
   hist[3 * k + 0] = st->inc;
   hist[3 * k + 1] = st->ess;
   hist[3 * k + 2] = (double)st->resampled;
@@ -535,6 +558,8 @@ int bpf_destroy(bpf_handle* h) {
   if (h->hist) cudaFree(h->hist);
   for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
   if (h->host_stats) cudaFreeHost(h->host_stats);
+  if (h->fgraph) cudaGraphExecDestroy(h->fgraph);
+  if (h->capture_stream) cudaStreamDestroy(h->capture_stream);
   bpf::ancestry_free(h->pc);
   void* g[] = {h->one_filt, h->one_order};
   for (void* p : g)
@@ -779,6 +804,88 @@ int bpf_step_device(bpf_handle* h, double t1, double t2, const void* y_dev, bpf_
   return BPF_OK;
 }
 
+// the T steps of bpf_filter, each followed by its history record
+static int launch_filter_steps(bpf_handle* h, int T, double t0, double dt) {
+  for (int k = 1; k <= T; ++k) {
+    const double t1 = t0 + (k - 1) * dt, t2 = t0 + k * dt;
+    int rc = enqueue_step(h, t1, t2, (const char*)h->y_dev + (size_t)(k - 1) * nobs(h) * h->esz);
+    if (rc) return rc;
+    BPF_TRY(bpf::launch_pdl(k_record, dim3(1), dim3(1), 0, h->stream, (const bpf::StepStats*)h->rs.stats, h->hist,
+                            k - 1));
+  }
+  BPF_TRY(cudaGetLastError());
+  return BPF_OK;
+}
+
+// Capture the steps into h->fgraph on the handle's capture stream (false:
+// they would not capture; nothing was launched and the handle is as before)
+static bool capture_filter_steps(bpf_handle* h, int T, double t0, double dt, const bpf_handle::FilterKey& key) {
+  if (h->fgraph) {
+    cudaGraphExecDestroy(h->fgraph);
+    h->fgraph = nullptr;
+  }
+  if (!h->capture_stream && cudaStreamCreateWithFlags(&h->capture_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    h->capture_stream = nullptr;
+    cudaGetLastError();
+    return false;
+  }
+  const int cur0 = h->cur, step0 = h->step;
+  if (cudaStreamBeginCapture(h->capture_stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  cudaStream_t launch_stream = h->stream;
+  h->stream = h->capture_stream;
+  const int rc = launch_filter_steps(h, T, t0, dt);
+  h->stream = launch_stream;
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(h->capture_stream, &g);
+  if (e == cudaSuccess && rc == BPF_OK && g) e = cudaGraphInstantiate(&h->fgraph, g, 0);
+  if (g) cudaGraphDestroy(g);
+  if (e != cudaSuccess || rc != BPF_OK || !h->fgraph) {
+    if (h->fgraph) cudaGraphExecDestroy(h->fgraph);
+    h->fgraph = nullptr;
+    cudaGetLastError();
+    h->cur = cur0;
+    h->step = step0;
+    return false;
+  }
+  h->fgraph_key = key;
+  h->fgraph_cur = h->cur;
+  return true;
+}
+
+// The steps of a filter run after bpf_init.  A caller that filters the same
+// schedule again and again (a sampler's Filter::filter per proposal) gets
+// them as one CUDA graph from the second call on: the launches of T steps
+// then cost the host one graph launch.  Timing events, path recording,
+// learned proposals and models compiled outside the library run the steps
+// as separate launches.
+static int enqueue_filter_steps(bpf_handle* h, int T, double t0, double dt) {
+  bpf_handle::FilterKey key;
+  key.T = T;
+  key.t0 = t0;
+  key.dt = dt;
+  key.y = h->y_dev;
+  key.hist = h->hist;
+  key.fused = h->fused;
+  const bool graphable = !h->custom && !h->prop && !h->timing && !h->pc_on && h->cur == 0 && h->step == 0;
+  if (graphable && h->fgraph && h->fgraph_key == key) {
+    BPF_TRY(cudaGraphLaunch(h->fgraph, h->stream));
+    h->cur = h->fgraph_cur;
+    h->step = T;
+    return BPF_OK;
+  }
+  const bool repeat = h->last_filter_set && h->last_filter == key;
+  h->last_filter = key;
+  h->last_filter_set = true;
+  if (graphable && repeat && capture_filter_steps(h, T, t0, dt, key)) {
+    BPF_TRY(cudaGraphLaunch(h->fgraph, h->stream));
+    return BPF_OK;
+  }
+  return launch_filter_steps(h, T, t0, dt);
+}
+
 int bpf_filter(bpf_handle* h, int T, double t0, double dt, const void* y, double* log_increments, double* ess,
                double* log_likelihood) {
   if (!h || T <= 0 || !(dt > 0.0) || !y) return BPF_E_INVALID;
@@ -795,13 +902,8 @@ int bpf_filter(bpf_handle* h, int T, double t0, double dt, const void* y, double
     if (cudaMalloc((void**)&h->hist, (size_t)3 * T * sizeof(double)) != cudaSuccess) return BPF_E_NOMEM;
     h->hist_cap = T;
   }
-  for (int k = 1; k <= T; ++k) {
-    const double t1 = t0 + (k - 1) * dt, t2 = t0 + k * dt;
-    rc = enqueue_step(h, t1, t2, (const char*)h->y_dev + (size_t)(k - 1) * nobs(h) * h->esz);
-    if (rc) return rc;
-    k_record<<<1, 1, 0, h->stream>>>(h->rs.stats, h->hist, k - 1);
-  }
-  BPF_TRY(cudaGetLastError());
+  rc = enqueue_filter_steps(h, T, t0, dt);
+  if (rc) return rc;
   // BootstrapPF::term: logLikelihood = logsumexp(lws) - log P
   // (share/src/bi/filter/BootstrapPF.hpp:192-196); keep the step statistics
   bpf::StepStats s;

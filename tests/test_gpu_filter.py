@@ -177,3 +177,39 @@ def test_unobserved_steps(cuda, oracle):
     assert r.log_likelihood == 0.0 and not r.resampled
     _, lw, _ = pf.state()
     assert float(lw.abs().max()) == 0.0
+
+
+@pytest.mark.parametrize("which", ["pz", "l96_multinomial", "l96_one_launch", "l96_large"])
+def test_repeated_filter_calls_replay_the_same_steps(cuda, oracle, which):
+    """bpf_filter runs a repeated schedule as a CUDA graph from the second
+    call on (captured then, replayed after): every call equals the oracle's
+    filter of its observations, and a call with another schedule in between
+    runs directly and leaves the captured steps in place."""
+    from libbi_b200 import ModelL96, ModelPZ
+
+    if which == "pz":
+        model, n, T, dt, res, ess_rel = ModelPZ(), 1024, 15, 1.0, "systematic", 1.0
+    elif which == "l96_multinomial":
+        model, n, T, dt, res, ess_rel = ModelL96(dim=40), 8192, 8, 0.05, "multinomial", 0.5
+    elif which == "l96_one_launch":
+        model, n, T, dt, res, ess_rel = ModelL96(dim=40), 4096, 8, 0.05, "systematic", 1.0
+    else:
+        model, n, T, dt, res, ess_rel = ModelL96(dim=40), 65536, 6, 0.05, "systematic", 1.0
+    desc = model.desc()
+    pf = _mk(model, n, res, ess_rel, seed=14)
+    if which == "l96_one_launch":
+        pf.set_step_form(True)
+    runs = [oracle.simulate(desc, dseed, T, 0.0, dt)[0] for dseed in (81, 82, 83, 84)]
+    short, _ = oracle.simulate(desc, 85, T - 2, 0.0, dt)
+    for r, y in enumerate(runs):
+        if r == 3:
+            pf.filter(short, 0.0, dt)  # another schedule: run directly
+        ll, inc, ess = pf.filter(y, 0.0, dt)
+        want = oracle.filter(desc, pf._cfg, y, T, 0.0, dt)
+        assert want["rc"] == 0
+        np.testing.assert_allclose(inc, want["inc"], rtol=1e-10, atol=1e-9)
+        np.testing.assert_allclose(ess, want["ess"], rtol=1e-9)
+        np.testing.assert_allclose(ll, want["ll"], rtol=1e-10)
+        x, _, _ = pf.state()
+        np.testing.assert_array_equal(x.cpu().numpy()[:, :n], want["x"][:, :n])
+    pf.close()
