@@ -214,6 +214,19 @@ def cpu_baseline(y, seconds: float = 12.0):
     return ref
 
 
+def omp_threads(n: int):
+    """Set the process's OpenMP thread count.  The reference's host code,
+    loaded into this process for its timed leg, leaves it at one thread on
+    return (its parity entry points run on one thread); the port's parallel
+    loops would then run on one thread too."""
+    import ctypes
+
+    try:
+        ctypes.CDLL("libgomp.so.1").omp_set_num_threads(int(n))
+    except OSError:
+        pass
+
+
 def port_cpu_baseline(y, seconds: float = 12.0):
     """The oracle's port of the reference's CPU filter (OpenMP over particles,
     all host threads), on a bounded sample of the same workload."""
@@ -222,6 +235,7 @@ def port_cpu_baseline(y, seconds: float = 12.0):
     from libbi_b200 import configs
     from libbi_b200 import _native as N
 
+    omp_threads(int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)))
     O = Oracle()
     model = configs.L96_D40_N65536["model"]
     desc = model.desc()

@@ -41,17 +41,31 @@ struct u128 {
 
 __host__ __device__ __forceinline__ u128 u128_zero() { u128 r; r.lo = 0; r.hi = 0; return r; }
 
+// on the device through the carry flag (add.cc / addc), one carry chain
+// instead of a compare and a select per operation
 __host__ __device__ __forceinline__ u128 u128_add(u128 a, u128 b) {
   u128 r;
+#ifdef __CUDA_ARCH__
+  asm("add.cc.u64 %0, %2, %4;\n\taddc.u64 %1, %3, %5;"
+      : "=l"(r.lo), "=l"(r.hi)
+      : "l"(a.lo), "l"(a.hi), "l"(b.lo), "l"(b.hi));
+#else
   r.lo = a.lo + b.lo;
   r.hi = a.hi + b.hi + (r.lo < a.lo ? 1ull : 0ull);
+#endif
   return r;
 }
 
 __host__ __device__ __forceinline__ u128 u128_sub(u128 a, u128 b) {
   u128 r;
+#ifdef __CUDA_ARCH__
+  asm("sub.cc.u64 %0, %2, %4;\n\tsubc.u64 %1, %3, %5;"
+      : "=l"(r.lo), "=l"(r.hi)
+      : "l"(a.lo), "l"(a.hi), "l"(b.lo), "l"(b.hi));
+#else
   r.lo = a.lo - b.lo;
   r.hi = a.hi - b.hi - (a.lo < b.lo ? 1ull : 0ull);
+#endif
   return r;
 }
 
