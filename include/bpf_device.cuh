@@ -56,6 +56,11 @@ struct StepStats {
   double ess_rel;
   int n;
   int pad;
+  // a whole-filter run's per-step record (inc, ess, resampled) at
+  // hist[3 (step - 1)], written by the step's last block; null outside one
+  double* hist;
+  int hist_n;       // steps hist holds
+  int pad2;
 };
 
 
@@ -214,7 +219,16 @@ __device__ __forceinline__ bool transition_reduce_tail(LwPartial part, LwPartial
     __threadfence();
     if (ok) {
       finalize_partials(partials + pbase, np, n, st, kFinalizeStep, observed);
-      if (threadIdx.x == 0) st->resampled = resampled;
+      if (threadIdx.x == 0) {
+        st->resampled = resampled;
+        double* h = st->hist;
+        const int k = st->step;
+        if (h && observed && k >= 1 && k <= st->hist_n) {
+          h[3 * (k - 1) + 0] = st->inc;
+          h[3 * (k - 1) + 1] = st->ess;
+          h[3 * (k - 1) + 2] = (double)resampled;
+        }
+      }
     }
     if (threadIdx.x == 0) *counter = 0;
   }

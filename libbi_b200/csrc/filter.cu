@@ -349,13 +349,11 @@ int enqueue_step(bpf_handle* h, double t1, double t2, const void* y_dev, uint64_
   return path_record(h, true);
 }
 
-// a programmatic dependent of the step's transition; the next step's
-// resampler waits for it
-__global__ void k_record(const bpf::StepStats* st, double* hist, int k) {
-  bpf::pdl_wait();
-  hist[3 * k + 0] = st->inc;
-  hist[3 * k + 1] = st->ess;
-  hist[3 * k + 2] = (double)st->resampled;
+// point the step statistics at a whole-filter run's record (each step's
+// last block then writes its entry), or at nothing
+__global__ void k_set_hist(bpf::StepStats* st, double* hist, int n) {
+  st->hist = hist;
+  st->hist_n = n;
 }
 
 // the status back to BPF_OK, the grid-barrier word (counters[8..9]) to
@@ -804,14 +802,13 @@ int bpf_step_device(bpf_handle* h, double t1, double t2, const void* y_dev, bpf_
   return BPF_OK;
 }
 
-// the T steps of bpf_filter, each followed by its history record
+// the T steps of bpf_filter (each step's last block records its entry in
+// h->hist through the step statistics)
 static int launch_filter_steps(bpf_handle* h, int T, double t0, double dt) {
   for (int k = 1; k <= T; ++k) {
     const double t1 = t0 + (k - 1) * dt, t2 = t0 + k * dt;
     int rc = enqueue_step(h, t1, t2, (const char*)h->y_dev + (size_t)(k - 1) * nobs(h) * h->esz);
     if (rc) return rc;
-    BPF_TRY(bpf::launch_pdl(k_record, dim3(1), dim3(1), 0, h->stream, (const bpf::StepStats*)h->rs.stats, h->hist,
-                            k - 1));
   }
   BPF_TRY(cudaGetLastError());
   return BPF_OK;
@@ -902,7 +899,9 @@ int bpf_filter(bpf_handle* h, int T, double t0, double dt, const void* y, double
     if (cudaMalloc((void**)&h->hist, (size_t)3 * T * sizeof(double)) != cudaSuccess) return BPF_E_NOMEM;
     h->hist_cap = T;
   }
+  k_set_hist<<<1, 1, 0, h->stream>>>(h->rs.stats, h->hist, T);
   rc = enqueue_filter_steps(h, T, t0, dt);
+  k_set_hist<<<1, 1, 0, h->stream>>>(h->rs.stats, nullptr, 0);
   if (rc) return rc;
   // BootstrapPF::term: logLikelihood = logsumexp(lws) - log P
   // (share/src/bi/filter/BootstrapPF.hpp:192-196); keep the step statistics
@@ -1245,6 +1244,10 @@ int bpf_restore(bpf_handle* h, const void* buf, uint64_t bytes) {
   BPF_TRY(cudaMemcpyAsync(h->lw, p, (size_t)h->n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   p += (size_t)h->n * sizeof(double);
   BPF_TRY(cudaMemcpyAsync(h->as, p, (size_t)h->n * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  // no whole-filter run is in progress after a restore (the saved record
+  // pointer may name a buffer freed since)
+  hd.stats.hist = nullptr;
+  hd.stats.hist_n = 0;
   BPF_TRY(cudaMemcpyAsync(h->rs.stats, &hd.stats, sizeof(hd.stats), cudaMemcpyHostToDevice, h->stream));
   {
     const int rc = bpf::reset_scratch_words(h->rs, h->stream);
