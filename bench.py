@@ -1208,6 +1208,9 @@ def main():
                     help="PMMH iterations timed per arm (2000, the workload's; fewer for profiling)")
     ap.add_argument("--guided-seeds", type=int, default=64,
                     help="filter runs per N in the guided/bootstrap comparison (64; fewer for profiling)")
+    ap.add_argument("--large-n-sizes", type=int, nargs="+", default=[1 << 22, 1 << 24, 1 << 26],
+                    help="particle counts of the large-N kernel section (one small size for profiling: the "
+                         "section holds about 330 B per particle on the device)")
     ap.add_argument("--headline-only", action="store_true",
                     help="the headline line alone, none of the single-GPU sections after it (for profiling)")
     args = ap.parse_args()
@@ -1397,7 +1400,7 @@ def main():
         line["autotune"] = {"systematic_resampler_n": N_PARTICLES, "shape": shape_name(RESAMPLE_SHAPES[best]),
                             "median_us": {shape_name(k): v for k, v in us.items()}}
     if extras and not args.no_large_n:
-        line["kernels_large_n"] = large_n_kernels()
+        line["kernels_large_n"] = large_n_kernels(tuple(args.large_n_sizes))
     if extras:
         line["step_forms"] = step_forms(y_dev)
         line["pz_c1"] = pz_c1()
