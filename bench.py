@@ -205,12 +205,13 @@ def reference_cpu_baseline(y, seconds: float = 20.0):
 def cpu_baseline(y, seconds: float = 12.0):
     """The timed CPU baseline: the reference's own host code where it was
     compiled here (reference_cpu_baseline), with the oracle's port of the
-    reference's CPU filter beside it; the port alone otherwise."""
-    port = port_cpu_baseline(y, seconds)
+    reference's CPU filter beside it; the port alone otherwise.  The
+    reference runs first, on host cores that have not just run the port at
+    full load."""
     if not os.path.exists(REF_TIMED_LIB):
-        return port
+        return port_cpu_baseline(y, seconds)
     ref = reference_cpu_baseline(y, seconds=max(seconds, 20.0))
-    ref["port"] = port
+    ref["port"] = port_cpu_baseline(y, seconds)
     return ref
 
 
