@@ -77,8 +77,10 @@ struct bpf_handle {
     const void* y = nullptr;
     const double* hist = nullptr;
     bool fused = false;
+    long long wait_limit = 0;  // the one-launch step takes it as an argument
     bool operator==(const FilterKey& o) const {
-      return T == o.T && t0 == o.t0 && dt == o.dt && y == o.y && hist == o.hist && fused == o.fused;
+      return T == o.T && t0 == o.t0 && dt == o.dt && y == o.y && hist == o.hist && fused == o.fused &&
+             wait_limit == o.wait_limit;
     }
   };
   cudaGraphExec_t fgraph = nullptr;
@@ -866,6 +868,7 @@ static int enqueue_filter_steps(bpf_handle* h, int T, double t0, double dt) {
   key.y = h->y_dev;
   key.hist = h->hist;
   key.fused = h->fused;
+  key.wait_limit = bpf::barrier_limit();
   const bool graphable = !h->custom && !h->prop && !h->timing && !h->pc_on && h->cur == 0 && h->step == 0;
   if (graphable && h->fgraph && h->fgraph_key == key) {
     BPF_TRY(cudaGraphLaunch(h->fgraph, h->stream));

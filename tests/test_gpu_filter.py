@@ -179,7 +179,7 @@ def test_unobserved_steps(cuda, oracle):
     assert float(lw.abs().max()) == 0.0
 
 
-@pytest.mark.parametrize("which", ["pz", "l96_multinomial", "l96_one_launch", "l96_large"])
+@pytest.mark.parametrize("which", ["pz", "pz_metropolis", "l96_multinomial", "l96_one_launch", "l96_large"])
 def test_repeated_filter_calls_replay_the_same_steps(cuda, oracle, which):
     """bpf_filter runs a repeated schedule as a CUDA graph from the second
     call on (captured then, replayed after): every call equals the oracle's
@@ -189,6 +189,8 @@ def test_repeated_filter_calls_replay_the_same_steps(cuda, oracle, which):
 
     if which == "pz":
         model, n, T, dt, res, ess_rel = ModelPZ(), 1024, 15, 1.0, "systematic", 1.0
+    elif which == "pz_metropolis":
+        model, n, T, dt, res, ess_rel = ModelPZ(), 2048, 12, 1.0, "metropolis", 1.0
     elif which == "l96_multinomial":
         model, n, T, dt, res, ess_rel = ModelL96(dim=40), 8192, 8, 0.05, "multinomial", 0.5
     elif which == "l96_one_launch":
@@ -196,7 +198,7 @@ def test_repeated_filter_calls_replay_the_same_steps(cuda, oracle, which):
     else:
         model, n, T, dt, res, ess_rel = ModelL96(dim=40), 65536, 6, 0.05, "systematic", 1.0
     desc = model.desc()
-    pf = _mk(model, n, res, ess_rel, seed=14)
+    pf = _mk(model, n, res, ess_rel, seed=14, B=8 if res == "metropolis" else 0)
     if which == "l96_one_launch":
         pf.set_step_form(True)
     runs = [oracle.simulate(desc, dseed, T, 0.0, dt)[0] for dseed in (81, 82, 83, 84)]
@@ -210,6 +212,40 @@ def test_repeated_filter_calls_replay_the_same_steps(cuda, oracle, which):
         np.testing.assert_allclose(inc, want["inc"], rtol=1e-10, atol=1e-9)
         np.testing.assert_allclose(ess, want["ess"], rtol=1e-9)
         np.testing.assert_allclose(ll, want["ll"], rtol=1e-10)
+        x, _, _ = pf.state()
+        np.testing.assert_array_equal(x.cpu().numpy()[:, :n], want["x"][:, :n])
+    pf.close()
+
+
+@pytest.mark.parametrize("one_launch", [True, False])
+def test_filter_graph_after_a_timed_out_run(cuda, oracle, one_launch):
+    """Whole-filter calls under a wait limit that makes every hand-over give
+    up report BPF_E_TIMEOUT (the second such call captures its steps as a
+    graph); with the default limit back, the next calls of the same
+    schedule run again correctly: the limit a capture was made under is
+    part of what a replay must match."""
+    from libbi_b200 import BpfError, ModelL96
+    from libbi_b200 import _native as N
+
+    model = ModelL96(dim=40)
+    desc = model.desc()
+    n, T, dt = 65536, 5, 0.05
+    y, _ = oracle.simulate(desc, 91, T, 0.0, dt)
+    pf = _mk(model, n, "systematic", 1.0, seed=19)
+    pf.set_step_form(one_launch)
+    try:
+        assert N.lib().bpf_debug_set_wait_limit(-1) == N.BPF_OK
+        for _ in range(2):
+            with pytest.raises(BpfError) as e:
+                pf.filter(y, 0.0, dt)
+            assert e.value.status == N.BPF_E_TIMEOUT
+    finally:
+        N.lib().bpf_debug_set_wait_limit(N.BPF_WAIT_LIMIT_DEFAULT)
+    want = oracle.filter(desc, pf._cfg, y, T, 0.0, dt)
+    assert want["rc"] == 0
+    for _ in range(3):
+        ll, inc, ess = pf.filter(y, 0.0, dt)
+        np.testing.assert_allclose(inc, want["inc"], rtol=1e-10, atol=1e-9)
         x, _, _ = pf.state()
         np.testing.assert_array_equal(x.cpu().numpy()[:, :n], want["x"][:, :n])
     pf.close()
